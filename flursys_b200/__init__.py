@@ -1,0 +1,24 @@
+"""B200 (sm_100a) backend for the FLURSYS structured MAC projection step.
+
+The compute path is libflursys_cuda.so (hand-written CUDA behind the C ABI of
+include/flursys_cuda.h). This package is its host-side mirror of the
+reference's solver and linear-algebra interfaces; it has no CPU fallback.
+"""
+from . import _abi
+from .cases import (BackwardStepCase, Case, CavityCase, ChannelCase, CylinderCase, SolverBoundaryOverride,
+                    SolverBoundaryOverrides)
+from .solver import (BackendOptions, FieldUpdate, IncompressibleSolver, LidDrivenCavity3DConfig,
+                     LidDrivenCavity3DSolver, RunSummary, RunSummary3D, SimulationConfig, SolverError, SolverStep,
+                     TimeStepSettings)
+
+__all__ = [
+    "BackendOptions", "BackwardStepCase", "Case", "CavityCase", "ChannelCase", "CylinderCase", "FieldUpdate",
+    "IncompressibleSolver", "LidDrivenCavity3DConfig", "LidDrivenCavity3DSolver", "RunSummary", "RunSummary3D",
+    "SimulationConfig", "SolverBoundaryOverride", "SolverBoundaryOverrides", "SolverError", "SolverStep",
+    "TimeStepSettings", "load_library",
+]
+
+
+def load_library():
+    """Loads libflursys_cuda.so; raises ImportError when it was not built."""
+    return _abi.load()

@@ -1,0 +1,326 @@
+// capi.cu — the extern "C" boundary of libflursys_cuda.so (include/flursys_cuda.h).
+//
+// Host-side mirror of the reference solver objects: a FlursysCudaHandle plays
+// the role of IncompressibleSolver (src/solver/incompressible.rs:294-317) or
+// LidDrivenCavity3DSolver (src/solver/incompressible_3d.rs:103-115). It owns
+// device memory and one stream; every call validates its arguments, returns
+// a FlursysStatus and keeps a message for flursys_cuda_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "capi_internal.cuh"
+#include "cavity2d.cuh"
+#include "cavity3d.cuh"
+#include "common.cuh"
+#include "csr.cuh"
+#include "flursys_cuda.h"
+#include "pcg2d.cuh"
+#include "pcg3d.cuh"
+
+using namespace flursys;
+
+namespace {
+
+thread_local std::string g_error;
+
+void copy_msg(const std::string &s, char *buf, size_t size) {
+    if (!buf || size == 0) return;
+    size_t n = std::min(size - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+}
+
+// SimulationConfig::validate (incompressible.rs:93-191, thermal checks do not
+// apply: the backend runs flow-only physics) and LidDrivenCavity3DConfig::
+// validate (incompressible_3d.rs:50-84).
+int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
+    auto fin_pos = [](double x) { return std::isfinite(x) && x > 0.0; };
+    if (c.abi_version != FLURSYS_CUDA_ABI_VERSION) { *msg = "config abi_version does not match the library"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.precision != FLURSYS_PRECISION_F64 && c.precision != FLURSYS_PRECISION_MIXED) { *msg = "unknown precision"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.stop_rule < FLURSYS_STOP_ABS_INF || c.stop_rule > FLURSYS_STOP_REFERENCE_RESIDUAL) { *msg = "unknown stop rule"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.pressure_solver < FLURSYS_PRESSURE_PCG || c.pressure_solver > FLURSYS_PRESSURE_FCG) { *msg = "unknown pressure solver"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.stop_rule == FLURSYS_STOP_REL_L2 &&
+        !(std::isfinite(c.pressure_atol) && c.pressure_atol >= 0.0 && std::isfinite(c.pressure_rtol) && c.pressure_rtol >= 0.0)) {
+        *msg = "pressure_atol and pressure_rtol must be finite and non-negative";
+        return FLURSYS_ERR_INVALID_CONFIG;
+    }
+    if (c.precision == FLURSYS_PRECISION_MIXED && c.residual_replacement_every < 1) { *msg = "residual_replacement_every must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.dimension == 3) {
+        if (c.case_params.kind != FLURSYS_CASE_CAVITY) { *msg = "the current 3D backend supports only a lid-driven cavity case"; return FLURSYS_ERR_UNSUPPORTED; }
+        if (c.nx < 4 || c.ny < 4 || c.nz < 4) { *msg = "nx, ny, and nz must all be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0 && c.case_params.depth > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.density)) { *msg = "density must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.reference_velocity)) { *msg = "lid_velocity must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.reynolds)) { *msg = "reynolds must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.dt)) { *msg = "dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.max_steps <= 0 || c.pressure_max_iters <= 0) { *msg = "iteration limits must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.pressure_tolerance)) { *msg = "pressure_tolerance must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!(std::isfinite(c.pressure_omega) && c.pressure_omega > 0.0 && c.pressure_omega < 2.0)) { *msg = "pressure_omega must lie between 0 and 2"; return FLURSYS_ERR_INVALID_CONFIG; }
+        // Indices are 32-bit per dimension and 64-bit overall on the device.
+        if (c.nx > (1 << 20) || c.ny > (1 << 20) || c.nz > (1 << 20)) { *msg = "grid dimension too large"; return FLURSYS_ERR_INVALID_CONFIG; }
+        return FLURSYS_OK;
+    }
+    if (c.dimension != 2) { *msg = "dimension must be 2 or 3"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.case_params.kind < FLURSYS_CASE_CAVITY || c.case_params.kind > FLURSYS_CASE_CHANNEL) { *msg = "unknown case kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    for (int s = 0; s < 4; ++s)
+        if (c.overrides[s].kind < FLURSYS_BOUNDARY_CASE_DEFAULT || c.overrides[s].kind > FLURSYS_BOUNDARY_PRESSURE_OUTLET) { *msg = "unknown boundary override kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.nx < 4 || c.ny < 4) { *msg = "nx and ny must be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.nx > (1 << 20) || c.ny > (1 << 20)) { *msg = "grid dimension too large"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.dt)) { *msg = "dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.t_end) || c.t_end < 0.0) { *msg = "t_end must be finite and non-negative"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.coupling == FLURSYS_COUPLING_PROJECTION && c.t_end == 0.0) { *msg = "t_end must be positive for projection coupling"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.max_steps <= 0) { *msg = "max_steps must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.pressure_max_iters <= 0) { *msg = "pressure_max_iters must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.pressure_omega) || c.pressure_omega <= 0.0 || c.pressure_omega >= 2.0) { *msg = "pressure_omega must lie between 0 and 2"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.velocity_relaxation) || c.velocity_relaxation <= 0.0 || c.velocity_relaxation > 1.0) { *msg = "velocity_relaxation must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.pressure_relaxation) || c.pressure_relaxation <= 0.0 || c.pressure_relaxation > 1.0) { *msg = "pressure_relaxation must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.steady_tolerance)) { *msg = "steady_tolerance must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.case_params.density) || !fin_pos(c.case_params.kinematic_viscosity)) { *msg = "fluid density and kinematic viscosity must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.adaptive) {
+        if (c.coupling != FLURSYS_COUPLING_PROJECTION) { *msg = "adaptive time stepping requires transient projection coupling"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.min_dt)) { *msg = "adaptive min_dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.max_dt)) { *msg = "adaptive max_dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.min_dt > c.max_dt) { *msg = "adaptive min_dt must not exceed max_dt"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.dt < c.min_dt || c.dt > c.max_dt) { *msg = "adaptive initial dt must lie between min_dt and max_dt"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.target_cfl) || c.target_cfl <= 0.0 || c.target_cfl > 1.0) { *msg = "adaptive target_cfl must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.target_diffusion_number) || c.target_diffusion_number <= 0.0 || c.target_diffusion_number > 0.5) { *msg = "adaptive target_diffusion_number must lie between 0 (exclusive) and 0.5"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.max_growth_factor) || c.max_growth_factor < 1.0) { *msg = "adaptive max_growth_factor must be finite and at least 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
+    if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    return FLURSYS_OK;
+}
+
+}  // namespace
+
+namespace flursys {
+
+void set_global_error(const std::string &msg) { g_error = msg; }
+
+int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    *dst = buf;
+    return e == cudaErrorMemoryAllocation ? FLURSYS_ERR_OUT_OF_MEMORY : FLURSYS_ERR_CUDA;
+}
+
+// Enqueues one persistent 3D PCG solve of A x = -rhs on `stream`.
+int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                  const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
+                  long long max_iters, int replace_every, cudaStream_t stream, std::string *err) {
+    Pcg3dArgs a{};
+    a.nx = nx; a.ny = ny; a.nz = nz;
+    a.ix2 = 1.0 / (dx * dx); a.iy2 = 1.0 / (dy * dy); a.iz2 = 1.0 / (dz * dz);
+    a.x = x; a.rhs = rhs;
+    a.r = ws.r; a.d0 = ws.d0; a.d1 = ws.d1; a.q = ws.q; a.dx = ws.dx;
+    a.partials = ws.partials; a.barrier = ws.barrier; a.result = ws.result;
+    a.stop_rule = stop_rule; a.tol = tol; a.atol = atol; a.rtol = rtol;
+    a.max_iters = max_iters; a.replace_every = replace_every > 0 ? replace_every : 50;
+    cudaError_t e = cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream);
+    if (e == cudaSuccess) e = pcg3d_launch(a, ws.grid, precision, stream);
+    if (e != cudaSuccess) return set_cuda_error(err, e, "pcg3d launch");
+    return FLURSYS_OK;
+}
+
+cudaError_t PcgWorkspace::allocate(long long n, int precision, int device, int dim) {
+    free_all();
+    int maxgrid = 0;
+    cudaError_t e = dim == 3 ? pcg3d_max_grid(precision, device, &maxgrid) : pcg2d_max_grid(precision, device, &maxgrid);
+    if (e != cudaSuccess) return e;
+    const int bs = dim == 3 ? pcg3d_block_size() : pcg2d_block_size();
+    long long want = (n + (long long)bs * 4 - 1) / ((long long)bs * 4);  // >= 4 cells per thread
+    grid = (int)std::max(1LL, std::min((long long)maxgrid, want));
+    const size_t vb = precision == FLURSYS_PRECISION_MIXED ? sizeof(float) : sizeof(double);
+    const int np = dim == 3 ? pcg3d_num_partials() : pcg2d_num_partials();
+    if ((e = cudaMalloc(&r, vb * n)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&d0, vb * n)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&d1, vb * n)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&q, vb * n)) != cudaSuccess) return e;
+    if (precision == FLURSYS_PRECISION_MIXED && (e = cudaMalloc(&dx, sizeof(float) * n)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&partials, sizeof(double) * (size_t)np * grid)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&barrier, sizeof(GridBarrier))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&result, sizeof(PcgResultDev))) != cudaSuccess) return e;
+    if ((e = cudaMallocHost(&h_result, sizeof(PcgResultDev))) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+void PcgWorkspace::free_all() {
+    cudaFree(r); cudaFree(d0); cudaFree(d1); cudaFree(q); cudaFree(dx);
+    cudaFree(partials); cudaFree(barrier); cudaFree(result);
+    if (h_result) cudaFreeHost(h_result);
+    r = d0 = d1 = q = nullptr; dx = nullptr; partials = nullptr; barrier = nullptr; result = nullptr;
+    h_result = nullptr;
+}
+
+}  // namespace flursys
+
+extern "C" {
+
+uint32_t flursys_cuda_abi_version(void) { return FLURSYS_CUDA_ABI_VERSION; }
+
+int32_t flursys_cuda_global_error(char *buf, size_t size) {
+    copy_msg(g_error, buf, size);
+    return FLURSYS_OK;
+}
+
+// LidDrivenCavity3DConfig::default() (incompressible_3d.rs:27-47) for
+// dimension 3; the CLI cavity defaults (src/bin/flursys.rs:102-123,236-300)
+// with TimeStepSettings::default() (incompressible.rs:45-56) otherwise.
+int32_t flursys_cuda_default_config(int32_t dimension, FlursysCudaConfig *c) {
+    if (!c) { g_error = "null config"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    std::memset(c, 0, sizeof *c);
+    c->abi_version = FLURSYS_CUDA_ABI_VERSION;
+    c->dimension = dimension == 3 ? 3 : 2;
+    c->case_params.kind = FLURSYS_CASE_CAVITY;
+    c->case_params.length = 1.0;
+    c->case_params.height = 1.0;
+    c->case_params.depth = 1.0;
+    c->case_params.density = 1.0;
+    c->case_params.reference_velocity = 1.0;
+    c->case_params.reynolds = 100.0;
+    c->case_params.kinematic_viscosity = 0.01;
+    c->min_dt = 1.0e-6;
+    c->max_dt = 1.0e-2;
+    c->target_cfl = 0.5;
+    c->target_diffusion_number = 0.25;
+    c->max_growth_factor = 1.1;
+    c->pressure_solver = FLURSYS_PRESSURE_PCG;
+    c->pressure_atol = 0.0;
+    c->pressure_rtol = 1.0e-8;
+    c->precision = FLURSYS_PRECISION_F64;
+    c->residual_replacement_every = 50;
+    if (c->dimension == 3) {
+        c->nx = c->ny = c->nz = 32;
+        c->dt = 5.0e-4;
+        c->max_steps = 10000;
+        c->pressure_max_iters = 2000;
+        c->pressure_tolerance = 1.0e-6;
+        c->pressure_omega = 1.7;
+        c->pressure_solver = FLURSYS_PRESSURE_SOR;
+        c->stop_rule = FLURSYS_STOP_REFERENCE_RESIDUAL;
+        c->convection = FLURSYS_CONVECTION_CENTRAL;
+        c->t_end = 1e300;
+    } else {
+        c->nx = c->ny = 64;
+        c->nz = 1;
+        c->dt = 0.001;
+        c->t_end = 100.0;
+        c->max_steps = 100000;
+        c->convection = FLURSYS_CONVECTION_UPWIND;
+        c->coupling = FLURSYS_COUPLING_PROJECTION;
+        c->stop_rule = FLURSYS_STOP_ABS_INF;
+        c->pressure_max_iters = 1200;
+        c->pressure_tolerance = 1.0e-5;
+        c->pressure_omega = 1.7;
+        c->velocity_relaxation = 0.7;
+        c->pressure_relaxation = 0.3;
+        c->steady_tolerance = 1.0e-7;
+        c->minimum_steps = 2000;
+    }
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_create(const FlursysCudaConfig *cfg, FlursysCudaHandle **out) {
+    if (!cfg || !out) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    std::string msg;
+    int32_t st = validate_config(*cfg, &msg);
+    if (st) { g_error = msg; return st; }
+    auto *h = new FlursysCudaHandle();
+    h->cfg = *cfg;
+    h->cfg.fcg_weights_path = nullptr;  // the path is read during create only
+    st = handle_init(h, cfg);
+    if (st) {
+        g_error = h->err;
+        handle_free(h);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_step(FlursysCudaHandle *h, int64_t nsteps, FlursysStepReport *report) {
+    if (!h) { g_error = "null handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (nsteps < 0) { h->err = "nsteps must be non-negative"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "cudaSetDevice");
+    FlursysStepReport rep;
+    std::memset(&rep, 0, sizeof rep);
+    int32_t st = FLURSYS_OK;
+    for (int64_t s = 0; s < nsteps; ++s) {
+        st = h->cfg.dimension == 3 ? step3d(h, &rep) : step2d(h, &rep);
+        if (st) break;
+        if (h->cfg.dimension == 2 && (rep.converged || rep.reached_end_time)) break;
+    }
+    if (report) *report = rep;
+    return st;
+}
+
+size_t flursys_cuda_field_size(const FlursysCudaHandle *h, int32_t id) {
+    if (!h) return 0;
+    double *p = nullptr;
+    size_t n = 0;
+    field_ptr(const_cast<FlursysCudaHandle *>(h), id, &p, &n);
+    return n;
+}
+
+int32_t flursys_cuda_download(FlursysCudaHandle *h, int32_t id, double *host, size_t n) {
+    if (!h || !host) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    double *p = nullptr;
+    size_t fn = 0;
+    if (!field_ptr(h, id, &p, &fn)) { h->err = "unknown field id for this handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (fn != n) { h->err = "field size mismatch"; return FLURSYS_ERR_DIMENSION_MISMATCH; }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, p, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "download");
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_upload(FlursysCudaHandle *h, int32_t id, const double *host, size_t n) {
+    if (!h || !host) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    double *p = nullptr;
+    size_t fn = 0;
+    if (!field_ptr(h, id, &p, &fn)) { h->err = "unknown field id for this handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (fn != n) { h->err = "field size mismatch"; return FLURSYS_ERR_DIMENSION_MISMATCH; }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "upload");
+    if (h->cfg.dimension == 2) on_upload2d(h, id);
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_state(const FlursysCudaHandle *h, int64_t *step, double *time) {
+    if (!h) { g_error = "null handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (step) *step = h->step;
+    if (time) *time = h->time;
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream) {
+    if (!h) { g_error = "null handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size) {
+    copy_msg(h ? h->err : g_error, buf, size);
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_destroy(FlursysCudaHandle *h) {
+    if (!h) return FLURSYS_OK;
+    cudaSetDevice(h->device);
+    handle_free(h);
+    delete h;
+    return FLURSYS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// capi_internal.cuh — the handle behind FlursysCudaHandle and the helpers
+// shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cavity3d.cuh"
+#include "common.cuh"
+#include "flursys_cuda.h"
+#include "pcg3d.cuh"
+
+namespace flursys {
+
+// Device work vectors of one structured PCG solve (sized for n cells).
+struct PcgWorkspace {
+    int grid = 0;
+    void *r = nullptr, *d0 = nullptr, *d1 = nullptr, *q = nullptr;
+    float *dx = nullptr;
+    double *partials = nullptr;
+    GridBarrier *barrier = nullptr;
+    PcgResultDev *result = nullptr;
+    PcgResultDev *h_result = nullptr;  // pinned host copy
+    cudaError_t allocate(long long n, int precision, int device, int dim);
+    void free_all();
+};
+
+struct Handle2D;
+
+}  // namespace flursys
+
+struct FlursysCudaHandle {
+    FlursysCudaConfig cfg{};
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+    int64_t step = 0;
+    double time = 0.0;
+    // 3D state
+    flursys::Cavity3dState s3{};
+    flursys::Diag3Dev *diag3 = nullptr;
+    flursys::Diag3Dev *h_diag3 = nullptr;
+    flursys::PcgWorkspace pcg;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // 2D state
+    flursys::Handle2D *h2 = nullptr;
+};
+
+namespace flursys {
+
+int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what);
+// Message returned by flursys_cuda_global_error() on this thread.
+void set_global_error(const std::string &msg);
+// Matrix-free 2D pressure PCG for flursys_cuda_stencil_pcg (nz == 1).
+int32_t stencil_pcg2d(int64_t nx, int64_t ny, double dx, double dy, const double *rhs, double *x_inout,
+                      int32_t precision, const FlursysLinearSolverOptions *options,
+                      FlursysLinearSolveReport *report);
+int32_t handle_init(FlursysCudaHandle *h, const FlursysCudaConfig *cfg);
+void handle_free(FlursysCudaHandle *h);
+int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep);
+int32_t step2d(FlursysCudaHandle *h, FlursysStepReport *rep);
+bool field_ptr(FlursysCudaHandle *h, int32_t id, double **p, size_t *n);
+void on_upload2d(FlursysCudaHandle *h, int32_t id);
+int32_t init2d(FlursysCudaHandle *h);
+void free2d(FlursysCudaHandle *h);
+bool field_ptr2d(FlursysCudaHandle *h, int32_t id, double **p, size_t *n);
+int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                  const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
+                  long long max_iters, int replace_every, cudaStream_t stream, std::string *err);
+// Maps a finished PcgResultDev to a status and message.
+int32_t pcg_result_status(const PcgResultDev &r, std::string *err);
+
+}  // namespace flursys

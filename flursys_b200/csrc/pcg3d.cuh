@@ -1,0 +1,46 @@
+// pcg3d.cuh — host interface of the persistent 3D pressure PCG kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "common.cuh"
+
+namespace flursys {
+
+// Written by block 0 at the end of a solve.
+struct PcgResultDev {
+    int error;        // FlursysStatus of a failure, 0 when none
+    int status;       // FlursysLinearStatus
+    long long iterations;
+    double initial;   // initial residual in the stop-rule norm
+    double residual;  // final residual in the stop-rule norm
+    double true_l2;   // FP64 ||b - A x||_2 of the returned solution
+    double initial_l2;
+    unsigned device_error;  // DeviceError bits
+    unsigned pad;
+};
+
+struct Pcg3dArgs {
+    int nx, ny, nz;
+    double ix2, iy2, iz2;
+    double *x;          // pressure, FP64, updated in place
+    const double *rhs;  // Poisson right-hand side; the system is A x = -rhs
+    void *r, *d0, *d1, *q;  // FP64 (F64) or FP32 (MIXED) work vectors, n each
+    float *dx;          // MIXED solution increment, n
+    double *partials;   // grid * pcg3d_num_partials()
+    GridBarrier *barrier;
+    PcgResultDev *result;
+    int stop_rule;      // FlursysStopRule
+    double tol, atol, rtol;
+    long long max_iters;
+    int replace_every;
+};
+
+size_t pcg3d_vector_bytes(int precision);
+cudaError_t pcg3d_max_grid(int precision, int device, int *grid);
+int pcg3d_block_size();
+int pcg3d_num_partials();
+cudaError_t pcg3d_launch(const Pcg3dArgs &args, int grid, int precision, cudaStream_t stream);
+
+}  // namespace flursys

@@ -1,0 +1,410 @@
+"""Host-side mirror of the reference structured solvers, driving the CUDA backend.
+
+Names, fields and error behaviour follow the reference:
+  * ``LidDrivenCavity3DConfig`` / ``LidDrivenCavity3DSolver``
+    (src/solver/incompressible_3d.rs:8-162),
+  * ``SimulationConfig`` / ``IncompressibleSolver`` / ``SolverStep``
+    (src/solver/incompressible.rs:58-90, 211-229, 294-586).
+``new`` validates like the reference and raises ``SolverError`` with the
+reference's message where the reference returns ``Err(String)``. Every call
+goes through the C ABI of libflursys_cuda.so (include/flursys_cuda.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .cases import Case, CavityCase, SolverBoundaryOverrides
+
+
+class SolverError(RuntimeError):
+    """The reference's ``Err(String)``; ``status`` is the FlursysStatus code."""
+
+    def __init__(self, message: str, status: int = _abi.ERR_INVALID_CONFIG):
+        super().__init__(message)
+        self.status = status
+
+
+def _check(lib, handle, status: int) -> None:
+    if status == _abi.OK:
+        return
+    buf = C.create_string_buffer(1024)
+    if handle:
+        lib.flursys_cuda_last_error(handle, buf, len(buf))
+    else:
+        lib.flursys_cuda_global_error(buf, len(buf))
+    raise SolverError(buf.value.decode(errors="replace") or _abi.STATUS_NAMES.get(status, str(status)), status)
+
+
+@dataclass
+class BackendOptions:
+    """Backend knobs with no reference counterpart."""
+    precision: str = "f64"              # "f64" (parity) or "mixed"
+    stop_rule: Optional[str] = None     # "abs-inf" | "rel-l2" | "reference-residual"; None = solver default
+    pressure_atol: float = 0.0          # rel-l2 absolute part
+    pressure_rtol: float = 1.0e-8       # rel-l2 relative part
+    residual_replacement_every: int = 50
+    device: int = 0
+    fcg_weights_path: Optional[str] = None
+
+    def apply(self, cfg: _abi.CudaConfig) -> None:
+        cfg.precision = {"f64": _abi.PRECISION_F64, "mixed": _abi.PRECISION_MIXED}[self.precision]
+        if self.stop_rule is not None:
+            cfg.stop_rule = {"abs-inf": _abi.STOP_ABS_INF, "rel-l2": _abi.STOP_REL_L2,
+                             "reference-residual": _abi.STOP_REFERENCE_RESIDUAL}[self.stop_rule]
+        cfg.pressure_atol = self.pressure_atol
+        cfg.pressure_rtol = self.pressure_rtol
+        cfg.residual_replacement_every = self.residual_replacement_every
+        cfg.device = self.device
+
+
+# --------------------------------------------------------------------------
+# 3D: LidDrivenCavity3DConfig / LidDrivenCavity3DSolver
+# --------------------------------------------------------------------------
+@dataclass
+class LidDrivenCavity3DConfig:
+    """src/solver/incompressible_3d.rs:8-47 (same fields and defaults)."""
+    nx: int = 32
+    ny: int = 32
+    nz: int = 32
+    length: float = 1.0
+    height: float = 1.0
+    depth: float = 1.0
+    density: float = 1.0
+    lid_velocity: float = 1.0
+    reynolds: float = 100.0
+    dt: float = 5.0e-4
+    max_steps: int = 10_000
+    pressure_max_iters: int = 2_000
+    pressure_tolerance: float = 1.0e-6
+    pressure_omega: float = 1.7
+    output_dir: str = "results/cavity-3d"
+    # backend selection: "sor" mirrors the reference; "pcg" / "fcg" are the
+    # Krylov solves of the pinned system.
+    pressure_solver: str = "sor"
+    backend: BackendOptions = field(default_factory=BackendOptions)
+
+    def viscosity(self) -> float:
+        return self.lid_velocity * self.length / self.reynolds
+
+    def to_c(self) -> _abi.CudaConfig:
+        lib = _abi.load()
+        cfg = _abi.CudaConfig()
+        _check(lib, None, lib.flursys_cuda_default_config(3, C.byref(cfg)))
+        cfg.nx, cfg.ny, cfg.nz = self.nx, self.ny, self.nz
+        cp = cfg.case_params
+        cp.length, cp.height, cp.depth = self.length, self.height, self.depth
+        cp.density = self.density
+        cp.reference_velocity = self.lid_velocity
+        cp.reynolds = self.reynolds
+        cp.kinematic_viscosity = self.viscosity()
+        cfg.dt = self.dt
+        cfg.max_steps = self.max_steps
+        cfg.pressure_max_iters = self.pressure_max_iters
+        cfg.pressure_tolerance = self.pressure_tolerance
+        cfg.pressure_omega = self.pressure_omega
+        cfg.pressure_solver = {"pcg": _abi.PRESSURE_PCG, "sor": _abi.PRESSURE_SOR,
+                               "fcg": _abi.PRESSURE_FCG}[self.pressure_solver]
+        cfg.stop_rule = _abi.STOP_REFERENCE_RESIDUAL if self.pressure_solver == "sor" else _abi.STOP_REL_L2
+        self.backend.apply(cfg)
+        return cfg
+
+
+@dataclass
+class RunSummary3D:
+    """src/solver/incompressible_3d.rs:91-99."""
+    steps: int
+    final_time: float
+    max_divergence: float
+    pressure_residual: float
+    max_speed: float
+    elapsed: float
+
+
+class _Handle:
+    """Owns one FlursysCudaHandle."""
+
+    def __init__(self, cfg: _abi.CudaConfig):
+        self.lib = _abi.load()
+        self._weights = cfg.fcg_weights_path  # keep the bytes alive during create
+        h = C.c_void_p()
+        _check(self.lib, None, self.lib.flursys_cuda_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.flursys_cuda_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1) -> _abi.StepReport:
+        rep = _abi.StepReport()
+        _check(self.lib, self.h, self.lib.flursys_cuda_step(self.h, n, C.byref(rep)))
+        return rep
+
+    def field_size(self, fid: int) -> int:
+        return int(self.lib.flursys_cuda_field_size(self.h, fid))
+
+    def download(self, fid: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        n = self.field_size(fid)
+        if out is None:
+            out = np.empty(n, dtype=np.float64)
+        _check(self.lib, self.h, self.lib.flursys_cuda_download(self.h, fid, _abi.dptr(out), n))
+        return out
+
+    def upload(self, fid: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        _check(self.lib, self.h, self.lib.flursys_cuda_upload(self.h, fid, _abi.dptr(a), a.size))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(self.lib, self.h, self.lib.flursys_cuda_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def state(self):
+        s = C.c_int64()
+        t = C.c_double()
+        self.lib.flursys_cuda_state(self.h, C.byref(s), C.byref(t))
+        return s.value, t.value
+
+
+class LidDrivenCavity3DSolver:
+    """src/solver/incompressible_3d.rs:117-172 on the device."""
+
+    def __init__(self, cfg: LidDrivenCavity3DConfig):
+        self.cfg = cfg
+        self._h = _Handle(cfg.to_c())
+        self.last_report: Optional[_abi.StepReport] = None
+
+    @classmethod
+    def new(cls, cfg: LidDrivenCavity3DConfig) -> "LidDrivenCavity3DSolver":
+        return cls(cfg)
+
+    @property
+    def handle(self) -> _Handle:
+        return self._h
+
+    def advance(self, steps: int = 1) -> _abi.StepReport:
+        self.last_report = self._h.step(steps)
+        return self.last_report
+
+    def run(self, write_output: bool = True) -> RunSummary3D:
+        """run() (:136-162): max_steps steps, then field.vtk in output_dir."""
+        started = time.perf_counter()
+        rep = self.advance(self.cfg.max_steps)
+        if write_output:
+            from . import output
+            os.makedirs(self.cfg.output_dir, exist_ok=True)
+            output.write_legacy_vtk_3d(os.path.join(self.cfg.output_dir, "field.vtk"),
+                                       "FLURSYS 3D lid-driven cavity", self)
+        return RunSummary3D(steps=int(rep.iteration), final_time=rep.time,
+                            max_divergence=rep.continuity_residual,
+                            pressure_residual=rep.pressure_residual, max_speed=rep.max_speed,
+                            elapsed=time.perf_counter() - started)
+
+    def field(self, name: str) -> np.ndarray:
+        fid = {"u": _abi.FIELD_U, "v": _abi.FIELD_V, "w": _abi.FIELD_W, "pressure": _abi.FIELD_PRESSURE,
+               "rhs": _abi.FIELD_RHS, "u_star": _abi.FIELD_U_STAR, "v_star": _abi.FIELD_V_STAR,
+               "w_star": _abi.FIELD_W_STAR}[name]
+        return self._h.download(fid)
+
+    def close(self) -> None:
+        self._h.close()
+
+
+# --------------------------------------------------------------------------
+# 2D: SimulationConfig / IncompressibleSolver
+# --------------------------------------------------------------------------
+@dataclass
+class TimeStepSettings:
+    """src/solver/incompressible.rs:35-56."""
+    adaptive: bool = False
+    min_dt: float = 1.0e-6
+    max_dt: float = 1.0e-2
+    target_cfl: float = 0.5
+    target_diffusion_number: float = 0.25
+    max_growth_factor: float = 1.1
+
+
+@dataclass
+class SimulationConfig:
+    """src/solver/incompressible.rs:58-90 (flow-only physics)."""
+    case: Case = field(default_factory=lambda: Case.lid_driven_cavity(CavityCase()))
+    nx: int = 64
+    ny: int = 64
+    dt: float = 1.0e-3
+    time_step: TimeStepSettings = field(default_factory=TimeStepSettings)
+    max_steps: int = 100_000
+    t_end: float = 100.0
+    convection: str = "upwind"          # "upwind" | "central"
+    coupling: str = "projection"        # "projection" | "simple"
+    pressure_solver: str = "pcg"        # "pcg" | "sor"
+    pressure_max_iters: int = 1200
+    pressure_tolerance: float = 1.0e-5
+    pressure_omega: float = 1.7
+    velocity_relaxation: float = 0.7
+    pressure_relaxation: float = 0.3
+    print_every: int = 100
+    output_every: int = 100
+    frame_every: int = 500
+    steady_tolerance: float = 1.0e-7
+    minimum_steps: int = 2000
+    threads: int = 0
+    boundary_overrides: SolverBoundaryOverrides = field(default_factory=SolverBoundaryOverrides)
+    output_dir: str = "results/cavity"
+    backend: BackendOptions = field(default_factory=BackendOptions)
+
+    def to_c(self) -> _abi.CudaConfig:
+        lib = _abi.load()
+        cfg = _abi.CudaConfig()
+        _check(lib, None, lib.flursys_cuda_default_config(2, C.byref(cfg)))
+        self.case.fill(cfg.case_params)
+        self.boundary_overrides.fill(cfg.overrides)
+        cfg.nx, cfg.ny, cfg.nz = self.nx, self.ny, 1
+        cfg.dt = self.dt
+        ts = self.time_step
+        cfg.adaptive = 1 if ts.adaptive else 0
+        cfg.min_dt, cfg.max_dt = ts.min_dt, ts.max_dt
+        cfg.target_cfl, cfg.target_diffusion_number = ts.target_cfl, ts.target_diffusion_number
+        cfg.max_growth_factor = ts.max_growth_factor
+        cfg.max_steps = self.max_steps
+        cfg.t_end = self.t_end
+        cfg.convection = {"upwind": _abi.CONVECTION_UPWIND, "first-order-upwind": _abi.CONVECTION_UPWIND,
+                          "central": _abi.CONVECTION_CENTRAL}[self.convection]
+        cfg.coupling = {"projection": _abi.COUPLING_PROJECTION, "simple": _abi.COUPLING_SIMPLE}[self.coupling]
+        cfg.pressure_solver = {"pcg": _abi.PRESSURE_PCG, "sor": _abi.PRESSURE_SOR,
+                               "fcg": _abi.PRESSURE_FCG}[self.pressure_solver]
+        cfg.stop_rule = _abi.STOP_ABS_INF
+        cfg.pressure_max_iters = self.pressure_max_iters
+        cfg.pressure_tolerance = self.pressure_tolerance
+        cfg.pressure_omega = self.pressure_omega
+        cfg.velocity_relaxation = self.velocity_relaxation
+        cfg.pressure_relaxation = self.pressure_relaxation
+        cfg.steady_tolerance = self.steady_tolerance
+        cfg.minimum_steps = self.minimum_steps
+        self.backend.apply(cfg)
+        return cfg
+
+
+@dataclass
+class SolverStep:
+    """src/solver/incompressible.rs:211-229."""
+    iteration: int
+    time: float
+    time_step: float
+    continuity_residual: float
+    pressure_residual: float
+    pressure_iterations: int
+    momentum_residual: float
+    max_speed: float
+    momentum_cfl: float
+    viscous_diffusion_number: float
+    drag_coefficient: float
+    lift_coefficient: float
+    converged: bool
+    reached_end_time: bool
+
+    @classmethod
+    def from_report(cls, r: _abi.StepReport) -> "SolverStep":
+        return cls(int(r.iteration), r.time, r.time_step, r.continuity_residual, r.pressure_residual,
+                   int(r.pressure_iterations), r.momentum_residual, r.max_speed, r.momentum_cfl,
+                   r.viscous_diffusion_number, r.drag_coefficient, r.lift_coefficient, bool(r.converged),
+                   bool(r.reached_end_time))
+
+
+@dataclass
+class RunSummary:
+    """src/solver/incompressible.rs:200-209."""
+    case_name: str
+    steps: int
+    final_time: float
+    max_divergence: float
+    pressure_residual: float
+    elapsed: float
+    converged: bool
+
+
+@dataclass
+class FieldUpdate:
+    """src/solver/incompressible.rs:231-244 (no temperature)."""
+    nx: int
+    ny: int
+    pressure: np.ndarray
+    speed: np.ndarray
+    velocity_x: np.ndarray
+    velocity_y: np.ndarray
+    vorticity: np.ndarray
+    solid: np.ndarray
+
+
+class IncompressibleSolver:
+    """src/solver/incompressible.rs:319-586 on the device."""
+
+    def __init__(self, cfg: SimulationConfig):
+        self.cfg = cfg
+        self._h = _Handle(cfg.to_c())
+        self.last_report: Optional[_abi.StepReport] = None
+
+    @classmethod
+    def new(cls, cfg: SimulationConfig) -> "IncompressibleSolver":
+        return cls(cfg)
+
+    @property
+    def handle(self) -> _Handle:
+        return self._h
+
+    def advance(self) -> SolverStep:
+        """advance() (:523-555): one step and its SolverStep."""
+        self.last_report = self._h.step(1)
+        return SolverStep.from_report(self.last_report)
+
+    def run(self) -> RunSummary:
+        """run() (:368-499) without file output: steps until max_steps, t_end or steady."""
+        started = time.perf_counter()
+        step, _ = self._h.state()
+        rep = None
+        converged = False
+        while step < self.cfg.max_steps:
+            rep = self._h.step(min(self.cfg.max_steps - step, 1 << 20))
+            step = int(rep.iteration)
+            if rep.converged:
+                converged = True
+                break
+            if rep.reached_end_time:
+                break
+        self.last_report = rep
+        return RunSummary(case_name=self.cfg.case.name(), steps=step, final_time=rep.time if rep else 0.0,
+                          max_divergence=rep.continuity_residual if rep else 0.0,
+                          pressure_residual=rep.pressure_residual if rep else 0.0,
+                          elapsed=time.perf_counter() - started, converged=converged)
+
+    def field(self, name: str) -> np.ndarray:
+        fid = {"u": _abi.FIELD_U, "v": _abi.FIELD_V, "pressure": _abi.FIELD_PRESSURE, "rhs": _abi.FIELD_RHS,
+               "u_star": _abi.FIELD_U_STAR, "v_star": _abi.FIELD_V_STAR, "speed": _abi.FIELD_SPEED,
+               "vorticity": _abi.FIELD_VORTICITY, "u_cell": _abi.FIELD_U_CELL,
+               "v_cell": _abi.FIELD_V_CELL}[name]
+        return self._h.download(fid)
+
+    def field_update(self) -> FieldUpdate:
+        """field_update() (:563-586)."""
+        nx, ny = self.cfg.nx, self.cfg.ny
+        u = self.field("u").reshape(ny, nx + 1)
+        v = self.field("v").reshape(ny + 1, nx)
+        return FieldUpdate(nx=nx, ny=ny, pressure=self.field("pressure"), speed=self.field("speed"),
+                           velocity_x=(0.5 * (u[:, :-1] + u[:, 1:])).ravel(),
+                           velocity_y=(0.5 * (v[:-1, :] + v[1:, :])).ravel(),
+                           vorticity=self.field("vorticity"),
+                           solid=self.cfg.case.solid_mask(nx, ny).ravel())
+
+    def close(self) -> None:
+        self._h.close()

@@ -1,0 +1,306 @@
+/*
+ * flursys_cuda.h — C ABI of the B200 (sm_100a) backend for the FLURSYS
+ * structured MAC projection step and its `src/linear` pressure solvers.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int32 status
+ * (FlursysStatus) and never aborts. Host pointers are borrowed for the
+ * duration of a call only; a handle owns its device memory and one CUDA
+ * stream. A handle is used by one host thread at a time; different handles
+ * may run concurrently. Reference paths below are relative to the FLURSYS
+ * source tree.
+ */
+#ifndef FLURSYS_CUDA_H
+#define FLURSYS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLURSYS_CUDA_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------
+ * Status codes. 1..7 mirror LinearAlgebraError (src/linear/mod.rs:17-26);
+ * the rest carry the solver-level `Err(String)` cases of
+ * src/solver/incompressible.rs and src/solver/incompressible_3d.rs.
+ * ---------------------------------------------------------------------- */
+typedef enum FlursysStatus {
+    FLURSYS_OK = 0,
+    FLURSYS_ERR_DIMENSION_MISMATCH = 1,  /* LinearAlgebraError::DimensionMismatch */
+    FLURSYS_ERR_INVALID_CSR = 2,         /* LinearAlgebraError::InvalidCsr */
+    FLURSYS_ERR_INDEX_OUT_OF_BOUNDS = 3, /* LinearAlgebraError::IndexOutOfBounds */
+    FLURSYS_ERR_NON_FINITE = 4,          /* LinearAlgebraError::NonFiniteValue, ensure_finite() */
+    FLURSYS_ERR_MISSING_DIAGONAL = 5,    /* LinearAlgebraError::MissingDiagonal */
+    FLURSYS_ERR_ZERO_DIAGONAL = 6,       /* LinearAlgebraError::ZeroDiagonal */
+    FLURSYS_ERR_BREAKDOWN = 7,           /* LinearAlgebraError::Breakdown, PCG singular direction */
+    FLURSYS_ERR_INVALID_CONFIG = 8,      /* SimulationConfig::validate, LidDrivenCavity3DConfig::validate */
+    FLURSYS_ERR_REACHED_END_TIME = 9,    /* "projection simulation has already reached t_end" */
+    FLURSYS_ERR_CUDA = 10,               /* a CUDA runtime call failed */
+    FLURSYS_ERR_OUT_OF_MEMORY = 11,
+    FLURSYS_ERR_UNSUPPORTED = 12,        /* a configuration this backend does not implement */
+    FLURSYS_ERR_INVALID_ARGUMENT = 13,   /* null pointer, unknown enum value, wrong buffer size */
+    FLURSYS_ERR_TIMEOUT = 14             /* a bounded device-side wait gave up */
+} FlursysStatus;
+
+/* LinearSolverStatus (src/linear/solver.rs:22-26). */
+typedef enum FlursysLinearStatus {
+    FLURSYS_LINEAR_CONVERGED = 0,
+    FLURSYS_LINEAR_MAX_ITERATIONS = 1
+} FlursysLinearStatus;
+
+/* LinearSolverOptions (src/linear/solver.rs:5-20). Defaults: 1e-10, 1e-8, 1000. */
+typedef struct FlursysLinearSolverOptions {
+    double absolute_tolerance;
+    double relative_tolerance;
+    int64_t max_iterations;
+} FlursysLinearSolverOptions;
+
+/* LinearSolveReport (src/linear/solver.rs:28-35). */
+typedef struct FlursysLinearSolveReport {
+    int32_t status; /* FlursysLinearStatus */
+    int32_t reserved;
+    int64_t iterations;
+    double initial_residual;
+    double final_residual;
+    double relative_residual;
+} FlursysLinearSolveReport;
+
+/* ------------------------------------------------------------------------
+ * Case and solver configuration: a POD mirror of SimulationConfig
+ * (src/solver/incompressible.rs:58-90) and LidDrivenCavity3DConfig
+ * (src/solver/incompressible_3d.rs:8-25), plus backend knobs.
+ * ---------------------------------------------------------------------- */
+typedef enum FlursysCaseKind { /* CaseKind, src/cases/mod.rs:11-17 */
+    FLURSYS_CASE_CAVITY = 0,
+    FLURSYS_CASE_CYLINDER = 1,
+    FLURSYS_CASE_BACKWARD_STEP = 2,
+    FLURSYS_CASE_CHANNEL = 3
+} FlursysCaseKind;
+
+typedef enum FlursysSide { /* Side, src/cases/mod.rs:30-36 */
+    FLURSYS_SIDE_LEFT = 0,
+    FLURSYS_SIDE_RIGHT = 1,
+    FLURSYS_SIDE_BOTTOM = 2,
+    FLURSYS_SIDE_TOP = 3
+} FlursysSide;
+
+typedef enum FlursysBoundaryOverrideKind { /* SolverBoundaryOverride, src/preprocess.rs:1356-1361 */
+    FLURSYS_BOUNDARY_CASE_DEFAULT = 0,
+    FLURSYS_BOUNDARY_VELOCITY = 1,
+    FLURSYS_BOUNDARY_SYMMETRY = 2,
+    FLURSYS_BOUNDARY_PRESSURE_OUTLET = 3
+} FlursysBoundaryOverrideKind;
+
+typedef enum FlursysConvection { /* ConvectionScheme, src/solver/incompressible.rs:14-18 */
+    FLURSYS_CONVECTION_UPWIND = 0,
+    FLURSYS_CONVECTION_CENTRAL = 1
+} FlursysConvection;
+
+typedef enum FlursysCoupling { /* PressureVelocityCoupling, :26-33 */
+    FLURSYS_COUPLING_PROJECTION = 0,
+    FLURSYS_COUPLING_SIMPLE = 1
+} FlursysCoupling;
+
+typedef enum FlursysPressureSolver { /* PressureSolverKind, :20-24, plus the learned FCG */
+    FLURSYS_PRESSURE_PCG = 0,
+    FLURSYS_PRESSURE_SOR = 1, /* GPU: red-black ordering, not iterate-identical to the lexicographic sweep */
+    FLURSYS_PRESSURE_FCG = 2  /* flexible CG with the learned preconditioner, Jacobi-PCG fallback */
+} FlursysPressureSolver;
+
+typedef enum FlursysPrecision {
+    FLURSYS_PRECISION_F64 = 0,  /* every vector and reduction in FP64: parity mode */
+    FLURSYS_PRECISION_MIXED = 1 /* FP32 stencil/SpMV vectors, FP64 dots, FP64 solution,
+                                   FP64 residual replacement and final residual check */
+} FlursysPrecision;
+
+typedef enum FlursysStopRule {
+    /* Reference 2D PCG: stop when max|r| < pressure_tolerance (incompressible.rs:1111-1115,1156-1164). */
+    FLURSYS_STOP_ABS_INF = 0,
+    /* src/linear convention: ||r||_2 <= pressure_atol + pressure_rtol * ||r0||_2 (solver.rs:84-85). */
+    FLURSYS_STOP_REL_L2 = 1,
+    /* Reference 3D SOR test: max|Lap(p) - rhs| over cells other than (0,0,0) < pressure_tolerance
+       (incompressible_3d.rs:476-502). */
+    FLURSYS_STOP_REFERENCE_RESIDUAL = 2
+} FlursysStopRule;
+
+typedef struct FlursysCaseParams { /* Case / CavityCase / ChannelCase / CylinderCase / BackwardStepCase */
+    int32_t kind;                 /* FlursysCaseKind */
+    int32_t reserved;
+    double length, height, depth; /* domain extents; depth is used in 3D only */
+    double density;
+    double kinematic_viscosity;   /* 2D: Case::kinematic_viscosity(); 3D derives U*L/Re (incompressible_3d.rs:86-88) */
+    double reference_velocity;    /* lid velocity, u_inf or u_mean */
+    double reynolds;
+    double cylinder_xc, cylinder_yc, cylinder_diameter, cylinder_perturbation, cylinder_mu;
+    double step_x, step_height;
+} FlursysCaseParams;
+
+typedef struct FlursysBoundaryOverride {
+    int32_t kind; /* FlursysBoundaryOverrideKind */
+    int32_t reserved;
+    double u, v;      /* Velocity override */
+    double pressure;  /* PressureOutlet override */
+} FlursysBoundaryOverride;
+
+typedef struct FlursysCudaConfig {
+    uint32_t abi_version; /* FLURSYS_CUDA_ABI_VERSION */
+    int32_t dimension;    /* 2 or 3 */
+    FlursysCaseParams case_params;
+    FlursysBoundaryOverride overrides[4]; /* indexed by FlursysSide */
+    int64_t nx, ny, nz;                   /* cells; nz ignored in 2D */
+    double dt;
+    /* TimeStepSettings (incompressible.rs:35-56) */
+    int32_t adaptive;
+    int32_t reserved0;
+    double min_dt, max_dt, target_cfl, target_diffusion_number, max_growth_factor;
+    int64_t max_steps;
+    double t_end;
+    int32_t convection;      /* FlursysConvection (3D always uses central advective form) */
+    int32_t coupling;        /* FlursysCoupling (2D only) */
+    int32_t pressure_solver; /* FlursysPressureSolver */
+    int32_t stop_rule;       /* FlursysStopRule */
+    int64_t pressure_max_iters;
+    double pressure_tolerance;  /* ABS_INF and REFERENCE_RESIDUAL threshold */
+    double pressure_atol;       /* REL_L2 absolute part */
+    double pressure_rtol;       /* REL_L2 relative part */
+    double pressure_omega;
+    double velocity_relaxation, pressure_relaxation;
+    double steady_tolerance;
+    int64_t minimum_steps;
+    /* backend knobs */
+    int32_t precision;                  /* FlursysPrecision */
+    int32_t residual_replacement_every; /* MIXED: FP64 true-residual replacement period (default 50) */
+    int32_t device;                     /* CUDA ordinal */
+    int32_t reserved1;
+    const char *fcg_weights_path;       /* learned preconditioner weights (FCG only), may be NULL */
+} FlursysCudaConfig;
+
+/* SolverStep (incompressible.rs:211-229) plus backend diagnostics. */
+typedef struct FlursysStepReport {
+    int64_t iteration;
+    double time;
+    double time_step;
+    double continuity_residual; /* max |div u| */
+    double pressure_residual;   /* residual in the configured stop-rule norm */
+    int64_t pressure_iterations;
+    double momentum_residual;   /* max |u_new - u_old| over faces */
+    double max_speed;
+    double momentum_cfl;
+    double viscous_diffusion_number;
+    double drag_coefficient;
+    double lift_coefficient;
+    int32_t converged;
+    int32_t reached_end_time;
+    /* backend extras */
+    double pressure_initial_residual;      /* ||r0|| in the stop-rule norm */
+    double pressure_true_relative_residual; /* FP64 ||b - A x||_2 / ||r0||_2 after the solve */
+    double pressure_solve_ms;              /* device time of the pressure solve (CUDA events) */
+    double step_ms;                        /* device time of the whole step (CUDA events) */
+    int32_t pressure_status;               /* FlursysLinearStatus */
+    int32_t fcg_fallback;                  /* 1 when FCG stalled and Jacobi-PCG finished the solve */
+} FlursysStepReport;
+
+typedef enum FlursysFieldId {
+    FLURSYS_FIELD_U = 0,        /* 2D (nx+1)*ny, 3D (nx+1)*ny*nz, x fastest */
+    FLURSYS_FIELD_V = 1,        /* 2D nx*(ny+1), 3D nx*(ny+1)*nz */
+    FLURSYS_FIELD_W = 2,        /* 3D nx*ny*(nz+1) */
+    FLURSYS_FIELD_PRESSURE = 3, /* nx*ny(*nz) */
+    FLURSYS_FIELD_RHS = 4,      /* pressure right-hand side of the last step */
+    FLURSYS_FIELD_U_STAR = 5,
+    FLURSYS_FIELD_V_STAR = 6,
+    FLURSYS_FIELD_W_STAR = 7,
+    FLURSYS_FIELD_SPEED = 8,    /* 2D cell-centred speed (compute_cell_fields, :1381-1439) */
+    FLURSYS_FIELD_VORTICITY = 9,
+    FLURSYS_FIELD_U_CELL = 10,
+    FLURSYS_FIELD_V_CELL = 11
+} FlursysFieldId;
+
+typedef struct FlursysCudaHandle FlursysCudaHandle;
+
+/* Library ABI version (FLURSYS_CUDA_ABI_VERSION of the build). */
+uint32_t flursys_cuda_abi_version(void);
+
+/* Fills *cfg with the reference defaults: LidDrivenCavity3DConfig::default()
+ * (incompressible_3d.rs:27-47) when dimension == 3, otherwise the CLI cavity
+ * defaults of src/bin/flursys.rs:102-123,236-300. */
+int32_t flursys_cuda_default_config(int32_t dimension, FlursysCudaConfig *cfg);
+
+/* IncompressibleSolver::new (incompressible.rs:320-366) /
+ * LidDrivenCavity3DSolver::new (incompressible_3d.rs:118-134): validates the
+ * config, allocates device state, sets the initial field. */
+int32_t flursys_cuda_create(const FlursysCudaConfig *cfg, FlursysCudaHandle **out);
+
+/* Advances up to nsteps steps: advance_one_step (incompressible.rs:622-746,
+ * incompressible_3d.rs:164-172). Stops early (2D) when the steady test of
+ * run() (:478-485) passes or t_end is reached. `report` receives the last
+ * step's SolverStep fields. */
+int32_t flursys_cuda_step(FlursysCudaHandle *h, int64_t nsteps, FlursysStepReport *report);
+
+/* Copies a device field to host memory (`n` doubles; must equal the field size). */
+int32_t flursys_cuda_download(FlursysCudaHandle *h, int32_t field_id, double *host, size_t n);
+
+/* Copies a host field to the device (parity inputs, restarts). */
+int32_t flursys_cuda_upload(FlursysCudaHandle *h, int32_t field_id, const double *host, size_t n);
+
+/* Element count of a field for this handle, or 0 if the field does not exist. */
+size_t flursys_cuda_field_size(const FlursysCudaHandle *h, int32_t field_id);
+
+/* Current step count and physical time. */
+int32_t flursys_cuda_state(const FlursysCudaHandle *h, int64_t *step, double *time);
+
+/* Makes the handle enqueue its work on `stream` (a cudaStream_t of the same
+ * device; NULL restores the handle's own stream). Lets a caller time or
+ * order the solver's kernels on a stream it owns. No reference counterpart:
+ * the reference has no device streams. */
+int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream);
+
+/* Copies the last error message (NUL-terminated, truncated to `size`). */
+int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size);
+
+/* Releases device memory and the stream. */
+int32_t flursys_cuda_destroy(FlursysCudaHandle *h);
+
+/* Message for the last failed call on this thread that had no handle. */
+int32_t flursys_cuda_global_error(char *buf, size_t size);
+
+/* ------------------------------------------------------------------------
+ * Linear solvers with the src/linear signatures (src/linear/solver.rs:43-60,
+ * 155-160). CSR arrays are host memory with int64 offsets/columns; `x_inout`
+ * carries the initial guess in and the solution out. Status mirrors
+ * LinearAlgebraError. All arithmetic is FP64 on the device.
+ * ---------------------------------------------------------------------- */
+int32_t flursys_cuda_csr_cg(int64_t n, int64_t nnz, const int64_t *row_offsets,
+                            const int64_t *columns, const double *values, const double *rhs,
+                            double *x_inout, const FlursysLinearSolverOptions *options,
+                            FlursysLinearSolveReport *report);
+int32_t flursys_cuda_csr_pcg(int64_t n, int64_t nnz, const int64_t *row_offsets,
+                             const int64_t *columns, const double *values, const double *rhs,
+                             double *x_inout, const FlursysLinearSolverOptions *options,
+                             FlursysLinearSolveReport *report);
+int32_t flursys_cuda_csr_bicgstab(int64_t n, int64_t nnz, const int64_t *row_offsets,
+                                  const int64_t *columns, const double *values, const double *rhs,
+                                  double *x_inout, const FlursysLinearSolverOptions *options,
+                                  FlursysLinearSolveReport *report);
+
+/* CsrMatrix::spmv_into (src/linear/csr.rs:89-106) on the device. */
+int32_t flursys_cuda_csr_spmv(int64_t nrows, int64_t ncols, int64_t nnz,
+                              const int64_t *row_offsets, const int64_t *columns,
+                              const double *values, const double *input, double *output);
+
+/* Matrix-free pressure PCG on a structured grid: the operator of
+ * apply_pressure_operator (incompressible.rs:1216-1255) in 2D (nz == 1) or the
+ * pinned 7-point Neumann operator of incompressible_3d.rs:293-332 in 3D.
+ * `rhs` is the Poisson right-hand side (as built by build_pressure_rhs);
+ * the solved system is A x = -rhs with A the positive operator. */
+int32_t flursys_cuda_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
+                                 double dz, const double *rhs, double *x_inout,
+                                 int32_t precision, const FlursysLinearSolverOptions *options,
+                                 FlursysLinearSolveReport *report);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* FLURSYS_CUDA_H */

@@ -1,0 +1,210 @@
+"""ctypes binding of the CPU oracle (liboracle_flursys.so) — TEST INFRASTRUCTURE ONLY.
+
+Used by tests/ as the checker, by __graft_entry__.smoke() and by bench.py's
+CPU baseline. The configuration and report types are the C-ABI types of
+include/flursys_cuda.h (flursys_b200._abi).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from flursys_b200 import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_flursys.so")
+_lib = None
+
+_D = C.POINTER(C.c_double)
+_I64P = C.POINTER(C.c_int64)
+_P = C.c_void_p
+
+
+def build(force: bool = False) -> str:
+    """Compiles the oracle with the Makefile beside this file."""
+    src = os.path.join(HERE, "flursys_oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(
+            os.path.getmtime(src), os.path.getmtime(os.path.join(HERE, "flursys_oracle.h"))):
+        subprocess.run(["make", "-s", "-B" if force else "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    sig = {
+        "orc_set_threads": (None, [C.c_int32]),
+        "orc_get_threads": (C.c_int32, []),
+        "orc_csr_validate": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, _I64P, _I64P, _D, C.c_char_p, C.c_size_t]),
+        "orc_csr_build": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, _I64P, _I64P, _D, _I64P, _I64P, _D, _I64P]),
+        "orc_csr_spmv": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D]),
+        "orc_jacobi_inverse_diagonal": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _I64P]),
+        "orc_csr_solve": (C.c_int32, [C.c_int32, C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,
+                                      C.POINTER(_abi.LinearSolverOptions), C.POINTER(_abi.LinearSolveReport)]),
+        "orc_momentum_stability_numbers": (None, [C.c_double] * 6 + [_D, _D]),
+        "orc_adaptive_time_step": (C.c_int32, [C.c_double] * 12 + [_D, C.c_char_p, C.c_size_t]),
+        "orc_default_config": (C.c_int32, [C.c_int32, C.POINTER(_abi.CudaConfig)]),
+        "orc_create": (C.c_int32, [C.POINTER(_abi.CudaConfig), C.POINTER(_P), C.c_char_p, C.c_size_t]),
+        "orc_step": (C.c_int32, [_P, C.c_int64, C.POINTER(_abi.StepReport)]),
+        "orc_field_size": (C.c_size_t, [_P, C.c_int32]),
+        "orc_get_field": (C.c_int32, [_P, C.c_int32, _D, C.c_size_t]),
+        "orc_set_field": (C.c_int32, [_P, C.c_int32, _D, C.c_size_t]),
+        "orc_last_error": (C.c_int32, [_P, C.c_char_p, C.c_size_t]),
+        "orc_destroy": (None, [_P]),
+        "orc_phase_predict": (C.c_int32, [_P, C.c_double]),
+        "orc_phase_rhs": (C.c_int32, [_P, C.c_double]),
+        "orc_phase_pressure": (C.c_int32, [_P, _D, _I64P]),
+        "orc_phase_correct": (C.c_int32, [_P, C.c_double]),
+        "orc_max_divergence": (C.c_double, [_P]),
+        "orc_pressure_residual": (C.c_double, [_P]),
+        "orc_max_speed": (C.c_double, [_P]),
+        "orc_stencil_pcg": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, _D,
+                                        _D, C.POINTER(_abi.LinearSolverOptions),
+                                        C.POINTER(_abi.LinearSolveReport)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class OracleError(RuntimeError):
+    def __init__(self, message: str, status: int):
+        super().__init__(message)
+        self.status = status
+
+
+def set_threads(n: int) -> None:
+    load().orc_set_threads(int(n))
+
+
+class OracleSolver:
+    """One oracle solver (2D IncompressibleSolver or 3D LidDrivenCavity3DSolver)."""
+
+    def __init__(self, cfg: _abi.CudaConfig):
+        self.lib = load()
+        self.cfg = cfg
+        h = C.c_void_p()
+        msg = C.create_string_buffer(512)
+        st = self.lib.orc_create(C.byref(cfg), C.byref(h), msg, len(msg))
+        if st:
+            raise OracleError(msg.value.decode(), st)
+        self.h = h
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.orc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def _err(self, st: int) -> None:
+        if st:
+            msg = C.create_string_buffer(512)
+            self.lib.orc_last_error(self.h, msg, len(msg))
+            raise OracleError(msg.value.decode(), st)
+
+    def step(self, n: int = 1) -> _abi.StepReport:
+        rep = _abi.StepReport()
+        self._err(self.lib.orc_step(self.h, n, C.byref(rep)))
+        return rep
+
+    def get(self, fid: int) -> np.ndarray:
+        n = self.lib.orc_field_size(self.h, fid)
+        out = np.empty(n, dtype=np.float64)
+        self._err(self.lib.orc_get_field(self.h, fid, _abi.dptr(out), n))
+        return out
+
+    def set(self, fid: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        self._err(self.lib.orc_set_field(self.h, fid, _abi.dptr(a), a.size))
+
+    def predict(self, dt: float) -> None:
+        self._err(self.lib.orc_phase_predict(self.h, dt))
+
+    def rhs(self, dt: float) -> None:
+        self._err(self.lib.orc_phase_rhs(self.h, dt))
+
+    def pressure(self):
+        res = C.c_double()
+        its = C.c_int64()
+        self._err(self.lib.orc_phase_pressure(self.h, C.byref(res), C.byref(its)))
+        return res.value, its.value
+
+    def correct(self, dt: float) -> None:
+        self._err(self.lib.orc_phase_correct(self.h, dt))
+
+    def max_divergence(self) -> float:
+        return self.lib.orc_max_divergence(self.h)
+
+    def pressure_residual(self) -> float:
+        return self.lib.orc_pressure_residual(self.h)
+
+    def max_speed(self) -> float:
+        return self.lib.orc_max_speed(self.h)
+
+
+def default_config(dimension: int) -> _abi.CudaConfig:
+    cfg = _abi.CudaConfig()
+    load().orc_default_config(dimension, C.byref(cfg))
+    return cfg
+
+
+def csr_solve(method: str, row_offsets, columns, values, rhs, x0, options=None):
+    """method: "cg" | "pcg" | "bicgstab". Returns (status, x, report)."""
+    lib = load()
+    ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+    ci = np.ascontiguousarray(columns, dtype=np.int64)
+    va = np.ascontiguousarray(values, dtype=np.float64)
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64)
+    opt = options or _abi.LinearSolverOptions(1e-10, 1e-8, 1000)
+    rep = _abi.LinearSolveReport()
+    st = lib.orc_csr_solve({"cg": 0, "pcg": 1, "bicgstab": 2}[method], ro.size - 1, va.size, _abi.i64ptr(ro),
+                           _abi.i64ptr(ci), _abi.dptr(va), _abi.dptr(b), _abi.dptr(x), C.byref(opt), C.byref(rep))
+    return st, x, rep
+
+
+def csr_build(nrows: int, ncols: int, rows, cols, vals):
+    lib = load()
+    r = np.ascontiguousarray(rows, dtype=np.int64)
+    c = np.ascontiguousarray(cols, dtype=np.int64)
+    v = np.ascontiguousarray(vals, dtype=np.float64)
+    ro = np.zeros(nrows + 1, dtype=np.int64)
+    ci = np.zeros(max(1, r.size), dtype=np.int64)
+    va = np.zeros(max(1, r.size), dtype=np.float64)
+    nnz = C.c_int64()
+    st = lib.orc_csr_build(nrows, ncols, r.size, _abi.i64ptr(r), _abi.i64ptr(c), _abi.dptr(v), _abi.i64ptr(ro),
+                           _abi.i64ptr(ci), _abi.dptr(va), C.byref(nnz))
+    return st, ro, ci[:nnz.value], va[:nnz.value]
+
+
+def csr_spmv(row_offsets, columns, values, x, ncols=None):
+    lib = load()
+    ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+    ci = np.ascontiguousarray(columns, dtype=np.int64)
+    va = np.ascontiguousarray(values, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(ro.size - 1)
+    st = lib.orc_csr_spmv(ro.size - 1, xx.size if ncols is None else ncols, va.size, _abi.i64ptr(ro),
+                          _abi.i64ptr(ci), _abi.dptr(va), _abi.dptr(xx), _abi.dptr(y))
+    return st, y
+
+
+def stencil_pcg(nx, ny, nz, dx, dy, dz, rhs, x0, options):
+    lib = load()
+    b = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64)
+    rep = _abi.LinearSolveReport()
+    st = lib.orc_stencil_pcg(nx, ny, nz, dx, dy, dz, _abi.dptr(b), _abi.dptr(x), C.byref(options), C.byref(rep))
+    return st, x, rep

@@ -1,0 +1,1865 @@
+// flursys_oracle.cpp — TEST INFRASTRUCTURE ONLY: the CPU FP64 oracle.
+//
+// A restatement, in C++17, of the FLURSYS reference algorithms on the
+// structured MAC projection path and of src/linear. Each function cites the
+// reference file:line it follows (paths relative to the FLURSYS tree). It is
+// used only by tests/ (as the checker), by __graft_entry__.smoke() and by
+// bench.py's CPU baseline; the CUDA product library never links it.
+//
+// Reduction order: with orc_set_threads(1) every sum is serial left to right.
+// The reference reduces on a Rayon pool; its own test pins 1-vs-4-thread
+// results only to 1e-10 (tests/smoke.rs:132-155), so reduction order is a
+// rounding-level effect here too.
+#include "flursys_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+int g_threads = 1;
+
+void copy_msg(const std::string &s, char *buf, size_t size) {
+    if (!buf || size == 0) return;
+    size_t n = std::min(size - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+}
+
+// ---------------------------------------------------------------------------
+// Vector primitives (src/linear/vector.rs and the Rayon helpers of
+// incompressible.rs:1308-1320).
+// ---------------------------------------------------------------------------
+double dot(const std::vector<double> &a, const std::vector<double> &b) {
+    const int64_t n = (int64_t)a.size();
+    double s = 0.0;
+    if (g_threads <= 1) {
+        for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    } else {
+#pragma omp parallel for reduction(+ : s) num_threads(g_threads) schedule(static)
+        for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    }
+    return s;
+}
+
+double max_abs(const std::vector<double> &a) {
+    const int64_t n = (int64_t)a.size();
+    double m = 0.0;
+    if (g_threads <= 1) {
+        for (int64_t i = 0; i < n; ++i) m = std::max(m, std::fabs(a[i]));
+    } else {
+#pragma omp parallel for reduction(max : m) num_threads(g_threads) schedule(static)
+        for (int64_t i = 0; i < n; ++i) m = std::max(m, std::fabs(a[i]));
+    }
+    return m;
+}
+
+// Field2D::max_abs (field.rs:49-51): fold with f64::max, which ignores NaN
+// exactly as std::max(m, x) does with a NaN second argument.
+double field_max_abs(const std::vector<double> &a) {
+    double m = 0.0;
+    for (double x : a) m = std::max(m, std::fabs(x));
+    return m;
+}
+
+bool all_finite(const std::vector<double> &a, size_t *bad) {
+    for (size_t i = 0; i < a.size(); ++i)
+        if (!std::isfinite(a[i])) {
+            if (bad) *bad = i;
+            return false;
+        }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Shared matrix-free PCG core. It follows the iteration order of
+// solve_pressure_pcg (incompressible.rs:1048-1214): initial residual and test,
+// Jacobi z, d = z, loop { q = A d; dq; alpha; x += a d; r -= a q; residual;
+// test; z; rz_new; beta; d = z + beta d }. Zero-mean projections
+// (project_zero_mean, :2338-2377) run where the reference runs them when the
+// operator is pure Neumann.
+// ---------------------------------------------------------------------------
+struct StructuredOperator {
+    // Returns true when the row is an identity row (solid, outlet, pinned cell).
+    virtual bool identity_row(int64_t k) const = 0;
+    virtual void apply(const std::vector<double> &x, std::vector<double> &y) const = 0;
+    virtual double diagonal(int64_t k) const = 0;  // 0 for identity rows
+    virtual bool needs_projection() const = 0;
+    virtual void project(std::vector<double> &v) const = 0;
+    virtual ~StructuredOperator() = default;
+};
+
+struct PcgResult {
+    int32_t status = FLURSYS_OK;
+    int32_t linear_status = FLURSYS_LINEAR_CONVERGED;
+    int64_t iterations = 0;
+    double initial = 0.0;
+    double residual = 0.0;
+    std::string error;
+};
+
+struct StopRule {
+    int32_t rule = FLURSYS_STOP_ABS_INF;
+    double tol = 1e-5;   // ABS_INF / REFERENCE_RESIDUAL
+    double atol = 0.0;   // REL_L2
+    double rtol = 1e-8;  // REL_L2
+    double threshold = 0.0;
+    double norm(const std::vector<double> &r) const {
+        return rule == FLURSYS_STOP_REL_L2 ? std::sqrt(dot(r, r)) : max_abs(r);
+    }
+    void set_initial(double r0) {
+        threshold = rule == FLURSYS_STOP_REL_L2 ? atol + rtol * r0 : tol;
+    }
+    // ABS_INF keeps the strict `<` of incompressible.rs:1112,1162; REL_L2 the
+    // `<=` of src/linear/solver.rs:86,115.
+    bool done(double res) const {
+        return rule == FLURSYS_STOP_REL_L2 ? res <= threshold : res < threshold;
+    }
+};
+
+PcgResult pcg_core(const StructuredOperator &op, const std::vector<double> &b_in,
+                   std::vector<double> &x, StopRule stop, int64_t max_iters) {
+    const int64_t n = (int64_t)x.size();
+    std::vector<double> b(b_in), r(n), z(n), d(n), q(n);
+    PcgResult res;
+    const bool proj = op.needs_projection();
+    auto jacobi = [&](const std::vector<double> &rr, std::vector<double> &zz) {
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < n; ++k) {
+            double dg = op.diagonal(k);
+            zz[k] = (op.identity_row(k) || !(dg > 0.0)) ? rr[k] : rr[k] / dg;
+        }
+    };
+    if (proj) {
+        op.project(x);
+        op.project(b);
+    }
+    op.apply(x, q);
+    for (int64_t k = 0; k < n; ++k) r[k] = b[k] - q[k];
+    if (proj) op.project(r);
+    double residual = stop.norm(r);
+    res.initial = residual;
+    stop.set_initial(residual);
+    if (stop.done(residual)) {
+        res.residual = residual;
+        return res;
+    }
+    jacobi(r, z);
+    if (proj) op.project(z);
+    d = z;
+    double rz_old = dot(r, z);
+    int64_t iterations = 0;
+    bool converged = false;
+    for (int64_t it = 0; it < max_iters; ++it) {
+        iterations = it + 1;
+        op.apply(d, q);
+        double den = dot(d, q);
+        if (std::fabs(den) < 1.0e-30 || !std::isfinite(den)) {
+            res.status = FLURSYS_ERR_BREAKDOWN;
+            res.error = "PCG pressure solver encountered a singular search direction";
+            return res;
+        }
+        double alpha = rz_old / den;
+        if (!std::isfinite(alpha)) {
+            res.status = FLURSYS_ERR_BREAKDOWN;
+            res.error = "PCG pressure solver produced a non-finite step length";
+            return res;
+        }
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < n; ++k) {
+            x[k] += alpha * d[k];
+            r[k] -= alpha * q[k];
+        }
+        if (proj) {
+            op.project(x);
+            op.project(r);
+        }
+        residual = stop.norm(r);
+        if (!std::isfinite(residual)) {
+            res.status = FLURSYS_ERR_NON_FINITE;
+            res.error = "PCG pressure solver produced a non-finite residual";
+            return res;
+        }
+        if (stop.done(residual)) {
+            converged = true;
+            break;
+        }
+        jacobi(r, z);
+        if (proj) op.project(z);
+        double rz_new = dot(r, z);
+        if (std::fabs(rz_old) < 1.0e-30) break;
+        double beta = rz_new / rz_old;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < n; ++k) d[k] = z[k] + beta * d[k];
+        if (proj) op.project(d);
+        rz_old = rz_new;
+    }
+    res.iterations = iterations;
+    res.residual = residual;
+    res.linear_status = converged ? FLURSYS_LINEAR_CONVERGED : FLURSYS_LINEAR_MAX_ITERATIONS;
+    return res;
+}
+
+// ---------------------------------------------------------------------------
+// 3D pinned Neumann operator: the system that the 3D SOR converges to
+// (incompressible_3d.rs:293-332, pressure_neighbor :450-474). For cells other
+// than (0,0,0): (A x)_c = sum_{in-range nb} w (x_c - x_nb) with x_(0,0,0) = 0;
+// cell (0,0,0) is an identity row. A x = -rhs is Lap(p) = rhs with p pinned.
+// ---------------------------------------------------------------------------
+struct Pinned3DOperator final : StructuredOperator {
+    int64_t nx, ny, nz;
+    double ix2, iy2, iz2;
+    Pinned3DOperator(int64_t nx_, int64_t ny_, int64_t nz_, double dx, double dy, double dz)
+        : nx(nx_), ny(ny_), nz(nz_), ix2(1.0 / (dx * dx)), iy2(1.0 / (dy * dy)),
+          iz2(1.0 / (dz * dz)) {}
+    bool identity_row(int64_t k) const override { return k == 0; }
+    double diagonal(int64_t k) const override {
+        if (k == 0) return 0.0;
+        int64_t i = k % nx, j = (k / nx) % ny, kk = k / (nx * ny);
+        double dg = 0.0;
+        if (i + 1 < nx) dg += ix2;
+        if (i > 0) dg += ix2;
+        if (j + 1 < ny) dg += iy2;
+        if (j > 0) dg += iy2;
+        if (kk + 1 < nz) dg += iz2;
+        if (kk > 0) dg += iz2;
+        return dg;
+    }
+    void apply(const std::vector<double> &x, std::vector<double> &y) const override {
+        const int64_t sxy = nx * ny;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t kk = 0; kk < nz; ++kk)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    int64_t c = i + nx * (j + ny * kk);
+                    if (c == 0) {
+                        y[c] = x[c];
+                        continue;
+                    }
+                    double dg = 0.0, s = 0.0;
+                    if (i + 1 < nx) { dg += ix2; s += ix2 * (c + 1 == 0 ? 0.0 : x[c + 1]); }
+                    if (i > 0) { dg += ix2; s += ix2 * (c - 1 == 0 ? 0.0 : x[c - 1]); }
+                    if (j + 1 < ny) { dg += iy2; s += iy2 * x[c + nx]; }
+                    if (j > 0) { dg += iy2; s += iy2 * (c - nx == 0 ? 0.0 : x[c - nx]); }
+                    if (kk + 1 < nz) { dg += iz2; s += iz2 * x[c + sxy]; }
+                    if (kk > 0) { dg += iz2; s += iz2 * (c - sxy == 0 ? 0.0 : x[c - sxy]); }
+                    y[c] = dg * x[c] - s;
+                }
+    }
+    bool needs_projection() const override { return false; }
+    void project(std::vector<double> &) const override {}
+};
+
+// ---------------------------------------------------------------------------
+// Case data (src/cases/mod.rs:120-227, cavity.rs, channel.rs, cylinder.rs,
+// backward_step.rs) and boundary overrides (src/preprocess.rs:1362-1406).
+// ---------------------------------------------------------------------------
+enum BKind { BK_VELOCITY = 0, BK_SYMMETRY = 1, BK_OUTLET = 2 };
+
+struct CaseModel {
+    FlursysCaseParams c;
+    FlursysBoundaryOverride ov[4];
+
+    // Case::boundary_kind (mod.rs:120-139)
+    BKind case_kind(int side, double *outlet_p) const {
+        *outlet_p = 0.0;
+        switch (c.kind) {
+            case FLURSYS_CASE_CAVITY: return BK_VELOCITY;
+            case FLURSYS_CASE_CYLINDER:
+                if (side == FLURSYS_SIDE_LEFT) return BK_VELOCITY;
+                if (side == FLURSYS_SIDE_RIGHT) return BK_OUTLET;
+                return BK_SYMMETRY;
+            default:  // backward step, channel
+                if (side == FLURSYS_SIDE_RIGHT) return BK_OUTLET;
+                return BK_VELOCITY;
+        }
+    }
+    // SolverBoundaryOverrides::kind (preprocess.rs:1370-1379)
+    BKind kind(int side, double *outlet_p = nullptr) const {
+        double dummy;
+        double *op = outlet_p ? outlet_p : &dummy;
+        switch (ov[side].kind) {
+            case FLURSYS_BOUNDARY_VELOCITY: *op = 0.0; return BK_VELOCITY;
+            case FLURSYS_BOUNDARY_PRESSURE_OUTLET: *op = ov[side].pressure; return BK_OUTLET;
+            case FLURSYS_BOUNDARY_SYMMETRY: *op = 0.0; return BK_SYMMETRY;
+            default: return case_kind(side, op);
+        }
+    }
+    // Case::boundary_velocity (mod.rs:142-175)
+    void case_velocity(int side, double /*x*/, double y, double *u, double *v) const {
+        *u = 0.0;
+        *v = 0.0;
+        switch (c.kind) {
+            case FLURSYS_CASE_CAVITY:
+                if (side == FLURSYS_SIDE_TOP) *u = c.reference_velocity;
+                return;
+            case FLURSYS_CASE_CYLINDER: *u = c.reference_velocity; return;
+            case FLURSYS_CASE_BACKWARD_STEP:
+                if (side == FLURSYS_SIDE_LEFT) {
+                    if (y <= c.step_height) return;
+                    double inlet = c.height - c.step_height;
+                    double eta = std::clamp((y - c.step_height) / inlet, 0.0, 1.0);
+                    *u = 6.0 * c.reference_velocity * eta * (1.0 - eta);
+                } else if (side == FLURSYS_SIDE_RIGHT) {
+                    *u = c.reference_velocity;
+                }
+                return;
+            default:  // channel
+                if (side == FLURSYS_SIDE_LEFT) {
+                    double eta = std::clamp(y / c.height, 0.0, 1.0);
+                    *u = 6.0 * c.reference_velocity * eta * (1.0 - eta);
+                } else if (side == FLURSYS_SIDE_RIGHT) {
+                    *u = c.reference_velocity;
+                }
+                return;
+        }
+    }
+    // SolverBoundaryOverrides::velocity (preprocess.rs:1381-1388)
+    void velocity(int side, double x, double y, double *u, double *v) const {
+        switch (ov[side].kind) {
+            case FLURSYS_BOUNDARY_VELOCITY: *u = ov[side].u; *v = ov[side].v; return;
+            case FLURSYS_BOUNDARY_PRESSURE_OUTLET:
+            case FLURSYS_BOUNDARY_SYMMETRY: *u = 0.0; *v = 0.0; return;
+            default: case_velocity(side, x, y, u, v);
+        }
+    }
+    // Case::initial_velocity (mod.rs:177-216)
+    void initial_velocity(double x, double y, double *u, double *v) const {
+        *u = 0.0;
+        *v = 0.0;
+        switch (c.kind) {
+            case FLURSYS_CASE_CAVITY: return;
+            case FLURSYS_CASE_CYLINDER: {
+                double r2 = (x - c.cylinder_xc) * (x - c.cylinder_xc) +
+                            (y - c.cylinder_yc) * (y - c.cylinder_yc);
+                double rad = 0.5 * c.cylinder_diameter;
+                if (r2 <= rad * rad) return;
+                double xp = c.cylinder_xc + 1.5 * c.cylinder_diameter;
+                double yp = c.cylinder_yc + 0.25 * c.cylinder_diameter;
+                double sigma2 = c.cylinder_diameter * c.cylinder_diameter;
+                double ddx = x - xp, ddy = y - yp;
+                double psi = c.cylinder_perturbation * std::exp(-(ddx * ddx + ddy * ddy) / sigma2);
+                *u = c.reference_velocity + (-2.0 * ddy / sigma2 * psi);
+                *v = 2.0 * ddx / sigma2 * psi;
+                return;
+            }
+            case FLURSYS_CASE_BACKWARD_STEP:
+                if (x < c.step_x && y < c.step_height) return;
+                if (y > c.step_height) {
+                    double inlet = c.height - c.step_height;
+                    double eta = std::clamp((y - c.step_height) / inlet, 0.0, 1.0);
+                    *u = 6.0 * c.reference_velocity * eta * (1.0 - eta);
+                } else {
+                    *u = c.reference_velocity;
+                }
+                return;
+            default: {
+                double eta = std::clamp(y / c.height, 0.0, 1.0);
+                *u = 6.0 * c.reference_velocity * eta * (1.0 - eta);
+                return;
+            }
+        }
+    }
+    // Case::is_solid (mod.rs:218-227)
+    bool is_solid(double x, double y) const {
+        switch (c.kind) {
+            case FLURSYS_CASE_CYLINDER: {
+                double rad = 0.5 * c.cylinder_diameter;
+                return (x - c.cylinder_xc) * (x - c.cylinder_xc) +
+                           (y - c.cylinder_yc) * (y - c.cylinder_yc) <=
+                       rad * rad;
+            }
+            case FLURSYS_CASE_BACKWARD_STEP: return x < c.step_x && y < c.step_height;
+            default: return false;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// adaptive_time_step (incompressible.rs:2308-2336) and
+// momentum_stability_numbers (:2294-2306).
+// ---------------------------------------------------------------------------
+int32_t adaptive_dt(double current_dt, double mu, double mv, double dx, double dy, double nu,
+                    double alpha_thermal, double min_dt, double max_dt, double target_cfl,
+                    double target_diff, double growth, double *out, std::string *err) {
+    double advective_rate = mu / dx + mv / dy;
+    double cfl_dt = advective_rate > 2.220446049250313e-16 ? target_cfl / advective_rate : max_dt;
+    double inv = 1.0 / (dx * dx) + 1.0 / (dy * dy);
+    double eff = alpha_thermal >= 0.0 ? std::max(alpha_thermal, nu) : nu;
+    double diffusion_dt = target_diff / (eff * inv);
+    double stable = std::min(std::min(max_dt, cfl_dt), diffusion_dt);
+    if (stable < min_dt) {
+        char buf[512];
+        std::snprintf(buf, sizeof buf,
+                      "required stable time step %.3e is below configured min_dt %.3e; CFL "
+                      "constraint=%.3e, diffusion constraint=%.3e",
+                      stable, min_dt, cfl_dt, diffusion_dt);
+        if (err) *err = buf;
+        return FLURSYS_ERR_INVALID_CONFIG;
+    }
+    double limited = std::min(stable, current_dt * growth);
+    *out = std::clamp(limited, min_dt, max_dt);
+    return FLURSYS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solver base.
+// ---------------------------------------------------------------------------
+}  // namespace
+
+struct OracleSolver {
+    FlursysCudaConfig cfg{};
+    std::string err;
+    int64_t step = 0;
+    double time = 0.0;
+    virtual ~OracleSolver() = default;
+    virtual int32_t advance(FlursysStepReport *rep) = 0;
+    virtual std::vector<double> *field(int32_t id) = 0;
+    virtual int32_t predict(double dt) = 0;
+    virtual int32_t rhs_phase(double dt) = 0;
+    virtual int32_t pressure(double *res, int64_t *its) = 0;
+    virtual int32_t correct(double dt) = 0;
+    virtual double max_divergence() const = 0;
+    virtual double pressure_residual() const = 0;
+    virtual double max_speed() const = 0;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// 3D: LidDrivenCavity3DSolver (incompressible_3d.rs).
+// ---------------------------------------------------------------------------
+struct Solver3D final : OracleSolver {
+    int64_t nx, ny, nz;
+    double dx, dy, dz, nu, lid, rho, dt;
+    std::vector<double> p, rhs, u, v, w, us, vs, ws;
+
+    size_t iu(int64_t i, int64_t j, int64_t k) const { return i + (nx + 1) * (j + ny * k); }
+    size_t iv(int64_t i, int64_t j, int64_t k) const { return i + nx * (j + (ny + 1) * k); }
+    size_t iw(int64_t i, int64_t j, int64_t k) const { return i + nx * (j + ny * k); }
+    size_t ic(int64_t i, int64_t j, int64_t k) const { return i + nx * (j + ny * k); }
+
+    explicit Solver3D(const FlursysCudaConfig &c) {
+        cfg = c;
+        nx = c.nx; ny = c.ny; nz = c.nz;
+        dx = c.case_params.length / nx;
+        dy = c.case_params.height / ny;
+        dz = c.case_params.depth / nz;
+        lid = c.case_params.reference_velocity;
+        rho = c.case_params.density;
+        nu = lid * c.case_params.length / c.case_params.reynolds;  // viscosity() :86-88
+        dt = c.dt;
+        size_t nc = nx * ny * nz;
+        p.assign(nc, 0.0);
+        rhs.assign(nc, 0.0);
+        u.assign((nx + 1) * ny * nz, 0.0);
+        v.assign(nx * (ny + 1) * nz, 0.0);
+        w.assign(nx * ny * (nz + 1), 0.0);
+        us = u; vs = v; ws = w;
+    }
+
+    // u_neighbor / v_neighbor / w_neighbor (:365-447)
+    double u_nb(int64_t i, int64_t j, int64_t k, int di, int dj, int dk, double c) const {
+        int64_t ni = i + di, nj = j + dj, nk = k + dk;
+        if (ni >= 0 && ni <= nx && nj >= 0 && nj < ny && nk >= 0 && nk < nz) return u[iu(ni, nj, nk)];
+        return nj >= ny ? 2.0 * lid - c : -c;
+    }
+    double v_nb(int64_t i, int64_t j, int64_t k, int di, int dj, int dk, double c) const {
+        int64_t ni = i + di, nj = j + dj, nk = k + dk;
+        if (ni >= 0 && ni < nx && nj >= 0 && nj <= ny && nk >= 0 && nk < nz) return v[iv(ni, nj, nk)];
+        return -c;
+    }
+    double w_nb(int64_t i, int64_t j, int64_t k, int di, int dj, int dk, double c) const {
+        int64_t ni = i + di, nj = j + dj, nk = k + dk;
+        if (ni >= 0 && ni < nx && nj >= 0 && nj < ny && nk >= 0 && nk <= nz) return w[iw(ni, nj, nk)];
+        return -c;
+    }
+    double p_nb(int64_t i, int64_t j, int64_t k, int di, int dj, int dk, double c) const {
+        int64_t ni = i + di, nj = j + dj, nk = k + dk;
+        if (ni >= 0 && ni < nx && nj >= 0 && nj < ny && nk >= 0 && nk < nz) return p[ic(ni, nj, nk)];
+        return c;
+    }
+
+    // predict_momentum (:174-273)
+    int32_t predict(double step_dt) override {
+        std::fill(us.begin(), us.end(), 0.0);
+        std::fill(vs.begin(), vs.end(), 0.0);
+        std::fill(ws.begin(), ws.end(), 0.0);
+        const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 1; i < nx; ++i) {
+                    double c = u[iu(i, j, k)];
+                    double e = u_nb(i, j, k, 1, 0, 0, c), wst = u_nb(i, j, k, -1, 0, 0, c);
+                    double n = u_nb(i, j, k, 0, 1, 0, c), s = u_nb(i, j, k, 0, -1, 0, c);
+                    double f = u_nb(i, j, k, 0, 0, 1, c), b = u_nb(i, j, k, 0, 0, -1, c);
+                    double vb = 0.25 * (v[iv(i - 1, j, k)] + v[iv(i, j, k)] + v[iv(i - 1, j + 1, k)] +
+                                        v[iv(i, j + 1, k)]);
+                    double wb = 0.25 * (w[iw(i - 1, j, k)] + w[iw(i, j, k)] + w[iw(i - 1, j, k + 1)] +
+                                        w[iw(i, j, k + 1)]);
+                    us[iu(i, j, k)] =
+                        c + step_dt * (-c * (e - wst) / (2.0 * dx) - vb * (n - s) / (2.0 * dy) -
+                                       wb * (f - b) / (2.0 * dz) +
+                                       nu * ((e - 2.0 * c + wst) / dx2 + (n - 2.0 * c + s) / dy2 +
+                                             (f - 2.0 * c + b) / dz2));
+                }
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 1; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double c = v[iv(i, j, k)];
+                    double e = v_nb(i, j, k, 1, 0, 0, c), wst = v_nb(i, j, k, -1, 0, 0, c);
+                    double n = v_nb(i, j, k, 0, 1, 0, c), s = v_nb(i, j, k, 0, -1, 0, c);
+                    double f = v_nb(i, j, k, 0, 0, 1, c), b = v_nb(i, j, k, 0, 0, -1, c);
+                    double ub = 0.25 * (u[iu(i, j - 1, k)] + u[iu(i + 1, j - 1, k)] + u[iu(i, j, k)] +
+                                        u[iu(i + 1, j, k)]);
+                    double wb = 0.25 * (w[iw(i, j - 1, k)] + w[iw(i, j, k)] + w[iw(i, j - 1, k + 1)] +
+                                        w[iw(i, j, k + 1)]);
+                    vs[iv(i, j, k)] =
+                        c + step_dt * (-ub * (e - wst) / (2.0 * dx) - c * (n - s) / (2.0 * dy) -
+                                       wb * (f - b) / (2.0 * dz) +
+                                       nu * ((e - 2.0 * c + wst) / dx2 + (n - 2.0 * c + s) / dy2 +
+                                             (f - 2.0 * c + b) / dz2));
+                }
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 1; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double c = w[iw(i, j, k)];
+                    double e = w_nb(i, j, k, 1, 0, 0, c), wst = w_nb(i, j, k, -1, 0, 0, c);
+                    double n = w_nb(i, j, k, 0, 1, 0, c), s = w_nb(i, j, k, 0, -1, 0, c);
+                    double f = w_nb(i, j, k, 0, 0, 1, c), b = w_nb(i, j, k, 0, 0, -1, c);
+                    double ub = 0.25 * (u[iu(i, j, k - 1)] + u[iu(i + 1, j, k - 1)] + u[iu(i, j, k)] +
+                                        u[iu(i + 1, j, k)]);
+                    double vb = 0.25 * (v[iv(i, j, k - 1)] + v[iv(i, j + 1, k - 1)] + v[iv(i, j, k)] +
+                                        v[iv(i, j + 1, k)]);
+                    ws[iw(i, j, k)] =
+                        c + step_dt * (-ub * (e - wst) / (2.0 * dx) - vb * (n - s) / (2.0 * dy) -
+                                       c * (f - b) / (2.0 * dz) +
+                                       nu * ((e - 2.0 * c + wst) / dx2 + (n - 2.0 * c + s) / dy2 +
+                                             (f - 2.0 * c + b) / dz2));
+                }
+        return FLURSYS_OK;
+    }
+
+    // build_pressure_rhs (:275-291)
+    int32_t rhs_phase(double step_dt) override {
+        const double scale = rho / step_dt;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i)
+                    rhs[ic(i, j, k)] = scale * (us[iu(i + 1, j, k)] - us[iu(i, j, k)]) / dx +
+                                       scale * (vs[iv(i, j + 1, k)] - vs[iv(i, j, k)]) / dy +
+                                       scale * (ws[iw(i, j, k + 1)] - ws[iw(i, j, k)]) / dz;
+        rhs[0] = 0.0;
+        return FLURSYS_OK;
+    }
+
+    // pressure_residual (:476-502)
+    double pressure_residual() const override {
+        const double ix2 = 1.0 / (dx * dx), iy2 = 1.0 / (dy * dy), iz2 = 1.0 / (dz * dz);
+        double m = 0.0;
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    if (i == 0 && j == 0 && k == 0) continue;
+                    double c = p[ic(i, j, k)];
+                    double lap = ix2 * (p_nb(i, j, k, 1, 0, 0, c) - 2.0 * c + p_nb(i, j, k, -1, 0, 0, c)) +
+                                 iy2 * (p_nb(i, j, k, 0, 1, 0, c) - 2.0 * c + p_nb(i, j, k, 0, -1, 0, c)) +
+                                 iz2 * (p_nb(i, j, k, 0, 0, 1, c) - 2.0 * c + p_nb(i, j, k, 0, 0, -1, c));
+                    // f64::max ignores NaN, as std::max(m, a) does here.
+                    m = std::max(m, std::fabs(lap - rhs[ic(i, j, k)]));
+                }
+        return m;
+    }
+
+    // solve_pressure_poisson (:293-332): lexicographic SOR, p(0,0,0) = 0.
+    int32_t pressure_sor(double *res_out, int64_t *its_out) {
+        const double ix2 = 1.0 / (dx * dx), iy2 = 1.0 / (dy * dy), iz2 = 1.0 / (dz * dz);
+        const double diag = 2.0 * (ix2 + iy2 + iz2);
+        const double omega = cfg.pressure_omega;
+        double residual = INFINITY;
+        int64_t its = 0;
+        for (int64_t it = 0; it < cfg.pressure_max_iters; ++it) {
+            its = it + 1;
+            for (int64_t k = 0; k < nz; ++k)
+                for (int64_t j = 0; j < ny; ++j)
+                    for (int64_t i = 0; i < nx; ++i) {
+                        if (i == 0 && j == 0 && k == 0) {
+                            p[0] = 0.0;
+                            continue;
+                        }
+                        double c = p[ic(i, j, k)];
+                        double s = ix2 * (p_nb(i, j, k, 1, 0, 0, c) + p_nb(i, j, k, -1, 0, 0, c)) +
+                                   iy2 * (p_nb(i, j, k, 0, 1, 0, c) + p_nb(i, j, k, 0, -1, 0, c)) +
+                                   iz2 * (p_nb(i, j, k, 0, 0, 1, c) + p_nb(i, j, k, 0, 0, -1, c));
+                        double cand = (s - rhs[ic(i, j, k)]) / diag;
+                        p[ic(i, j, k)] += omega * (cand - p[ic(i, j, k)]);
+                    }
+            residual = pressure_residual();
+            if (!std::isfinite(residual)) {
+                err = "3D pressure solver produced a non-finite residual";
+                return FLURSYS_ERR_NON_FINITE;
+            }
+            if (residual < cfg.pressure_tolerance) break;
+        }
+        *res_out = residual;
+        *its_out = its;
+        return FLURSYS_OK;
+    }
+
+    int32_t pressure(double *res_out, int64_t *its_out) override {
+        if (cfg.pressure_solver == FLURSYS_PRESSURE_SOR) return pressure_sor(res_out, its_out);
+        // Jacobi-PCG on the same pinned system (the 3D configs name PCG).
+        Pinned3DOperator op(nx, ny, nz, dx, dy, dz);
+        std::vector<double> b(rhs.size());
+        for (size_t k = 0; k < b.size(); ++k) b[k] = -rhs[k];
+        b[0] = 0.0;
+        std::vector<double> x(p);
+        x[0] = 0.0;
+        StopRule stop;
+        stop.rule = cfg.stop_rule == FLURSYS_STOP_REL_L2 ? FLURSYS_STOP_REL_L2 : FLURSYS_STOP_ABS_INF;
+        stop.tol = cfg.pressure_tolerance;
+        stop.atol = cfg.pressure_atol;
+        stop.rtol = cfg.pressure_rtol;
+        PcgResult r = pcg_core(op, b, x, stop, cfg.pressure_max_iters);
+        if (r.status != FLURSYS_OK) {
+            err = r.error;
+            return r.status;
+        }
+        p = x;
+        last_initial = r.initial;
+        last_linear_status = r.linear_status;
+        *res_out = r.residual;
+        *its_out = r.iterations;
+        return FLURSYS_OK;
+    }
+    double last_initial = 0.0;
+    int32_t last_linear_status = FLURSYS_LINEAR_CONVERGED;
+
+    // correct_velocity (:334-363)
+    int32_t correct(double step_dt) override {
+        const double scale = step_dt / rho;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t k = 0; k < nz; ++k) {
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 1; i < nx; ++i)
+                    u[iu(i, j, k)] = us[iu(i, j, k)] - scale * (p[ic(i, j, k)] - p[ic(i - 1, j, k)]) / dx;
+            for (int64_t j = 1; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i)
+                    v[iv(i, j, k)] = vs[iv(i, j, k)] - scale * (p[ic(i, j, k)] - p[ic(i, j - 1, k)]) / dy;
+            if (k >= 1)
+                for (int64_t j = 0; j < ny; ++j)
+                    for (int64_t i = 0; i < nx; ++i)
+                        w[iw(i, j, k)] = ws[iw(i, j, k)] - scale * (p[ic(i, j, k)] - p[ic(i, j, k - 1)]) / dz;
+        }
+        return FLURSYS_OK;
+    }
+
+    // max_divergence (:504-517)
+    double max_divergence() const override {
+        double m = 0.0;
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double d = (u[iu(i + 1, j, k)] - u[iu(i, j, k)]) / dx +
+                               (v[iv(i, j + 1, k)] - v[iv(i, j, k)]) / dy +
+                               (w[iw(i, j, k + 1)] - w[iw(i, j, k)]) / dz;
+                    m = std::max(m, std::fabs(d));
+                }
+        return m;
+    }
+    // max_speed (:519-532)
+    double max_speed() const override {
+        double m = 0.0;
+        for (int64_t k = 0; k < nz; ++k)
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double a = 0.5 * (u[iu(i, j, k)] + u[iu(i + 1, j, k)]);
+                    double b = 0.5 * (v[iv(i, j, k)] + v[iv(i, j + 1, k)]);
+                    double c = 0.5 * (w[iw(i, j, k)] + w[iw(i, j, k + 1)]);
+                    m = std::max(m, std::sqrt(a * a + b * b + c * c));
+                }
+        return m;
+    }
+
+    // advance_one_step (:164-172)
+    int32_t advance(FlursysStepReport *rep) override {
+        int32_t st = predict(dt);
+        if (st) return st;
+        rhs_phase(dt);
+        double res = 0.0;
+        int64_t its = 0;
+        st = pressure(&res, &its);
+        if (st) return st;
+        correct(dt);
+        step += 1;
+        time = step * dt;
+        // ensure_finite (:534-554)
+        const char *names[4] = {"pressure", "u", "v", "w"};
+        std::vector<double> *fs[4] = {&p, &u, &v, &w};
+        for (int f = 0; f < 4; ++f) {
+            size_t bad = 0;
+            if (!all_finite(*fs[f], &bad)) {
+                char buf[256];
+                std::snprintf(buf, sizeof buf, "Non-finite 3D %s value at flat index %zu: %g",
+                              names[f], bad, (*fs[f])[bad]);
+                err = buf;
+                return FLURSYS_ERR_NON_FINITE;
+            }
+        }
+        if (rep) {
+            std::memset(rep, 0, sizeof *rep);
+            rep->iteration = step;
+            rep->time = time;
+            rep->time_step = dt;
+            rep->continuity_residual = max_divergence();
+            rep->pressure_residual = res;
+            rep->pressure_iterations = its;
+            rep->max_speed = max_speed();
+            rep->pressure_initial_residual = last_initial;
+            rep->pressure_status = last_linear_status;
+        }
+        return FLURSYS_OK;
+    }
+
+    std::vector<double> *field(int32_t id) override {
+        switch (id) {
+            case FLURSYS_FIELD_U: return &u;
+            case FLURSYS_FIELD_V: return &v;
+            case FLURSYS_FIELD_W: return &w;
+            case FLURSYS_FIELD_PRESSURE: return &p;
+            case FLURSYS_FIELD_RHS: return &rhs;
+            case FLURSYS_FIELD_U_STAR: return &us;
+            case FLURSYS_FIELD_V_STAR: return &vs;
+            case FLURSYS_FIELD_W_STAR: return &ws;
+            default: return nullptr;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// 2D: IncompressibleSolver (incompressible.rs), without thermal physics.
+// ---------------------------------------------------------------------------
+struct Solver2D;
+
+struct Operator2D final : StructuredOperator {
+    const Solver2D *s;
+    explicit Operator2D(const Solver2D *s_) : s(s_) {}
+    bool identity_row(int64_t k) const override;
+    double diagonal(int64_t k) const override;
+    void apply(const std::vector<double> &x, std::vector<double> &y) const override;
+    bool needs_projection() const override;
+    void project(std::vector<double> &v) const override;
+};
+
+struct Solver2D final : OracleSolver {
+    int64_t nx, ny;
+    double dx, dy, length, height, rho, nu;
+    CaseModel cm;
+    std::vector<uint8_t> solid;
+    std::vector<double> p, rhs, u, v, us, vs, uc, vc, speed, vort;
+    double current_dt;
+
+    size_t iu(int64_t i, int64_t j) const { return i + (nx + 1) * j; }
+    size_t iv(int64_t i, int64_t j) const { return i + nx * j; }
+    size_t ic(int64_t i, int64_t j) const { return i + nx * j; }
+    bool sol(int64_t i, int64_t j) const { return solid[ic(i, j)] != 0; }
+
+    explicit Solver2D(const FlursysCudaConfig &c) {
+        cfg = c;
+        nx = c.nx; ny = c.ny;
+        length = c.case_params.length;
+        height = c.case_params.height;
+        dx = length / nx;
+        dy = height / ny;
+        rho = c.case_params.density;
+        nu = c.case_params.kinematic_viscosity;
+        cm.c = c.case_params;
+        std::memcpy(cm.ov, c.overrides, sizeof cm.ov);
+        solid.assign(nx * ny, 0);
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i)
+                solid[ic(i, j)] = cm.is_solid((i + 0.5) * dx, (j + 0.5) * dy) ? 1 : 0;
+        current_dt = c.dt;
+        p.assign(nx * ny, 0.0);
+        rhs = p; uc = p; vc = p; speed = p; vort = p;
+        u.assign((nx + 1) * ny, 0.0);
+        v.assign(nx * (ny + 1), 0.0);
+        us = u; vs = v;
+        initialize_velocity();
+        compute_cell_fields();
+    }
+
+    // u_face_open / v_face_open (:2046-2064)
+    bool u_open(int64_t i, int64_t j) const {
+        if (i == 0) return !sol(0, j);
+        if (i == nx) return !sol(nx - 1, j);
+        return !sol(i - 1, j) && !sol(i, j);
+    }
+    bool v_open(int64_t i, int64_t j) const {
+        if (j == 0) return !sol(i, 0);
+        if (j == ny) return !sol(i, ny - 1);
+        return !sol(i, j - 1) && !sol(i, j);
+    }
+    // pressure_outlet_cell (:2066-2080)
+    bool outlet_cell(int64_t i, int64_t j) const {
+        return i + 1 == nx && !sol(i, j) && cm.kind(FLURSYS_SIDE_RIGHT) == BK_OUTLET;
+    }
+    double outlet_pressure() const {
+        double pr = 0.0;
+        return cm.kind(FLURSYS_SIDE_RIGHT, &pr) == BK_OUTLET ? pr : 0.0;
+    }
+    bool reference_required() const { return cm.kind(FLURSYS_SIDE_RIGHT) != BK_OUTLET; }
+
+    // tangential_ghost_u / tangential_ghost_v (:2159-2199)
+    double ghost_u(int side, double center, double x) const {
+        if (cm.kind(side) == BK_VELOCITY) {
+            double y = side == FLURSYS_SIDE_BOTTOM ? 0.0 : height;
+            double wu, wv;
+            cm.velocity(side, x, y, &wu, &wv);
+            return 2.0 * wu - center;
+        }
+        return center;
+    }
+    double ghost_v(int side, double center, double y) const {
+        if (cm.kind(side) == BK_VELOCITY) {
+            double x = side == FLURSYS_SIDE_LEFT ? 0.0 : length;
+            double wu, wv;
+            cm.velocity(side, x, y, &wu, &wv);
+            return 2.0 * wv - center;
+        }
+        return center;
+    }
+    // MomentumStencil::u_neighbor / v_neighbor (:2089-2157)
+    double u_nb(const std::vector<double> &uu, int64_t i, int64_t j, int di, int dj, double c) const {
+        int64_t ii = i + di, jj = j + dj;
+        if (ii >= 0 && ii <= nx && jj >= 0 && jj < ny) return u_open(ii, jj) ? uu[iu(ii, jj)] : -c;
+        if (jj < 0) return ghost_u(FLURSYS_SIDE_BOTTOM, c, i * dx);
+        if (jj >= ny) return ghost_u(FLURSYS_SIDE_TOP, c, i * dx);
+        return c;
+    }
+    double v_nb(const std::vector<double> &vv, int64_t i, int64_t j, int di, int dj, double c) const {
+        int64_t ii = i + di, jj = j + dj;
+        if (ii >= 0 && ii < nx && jj >= 0 && jj <= ny) return v_open(ii, jj) ? vv[iv(ii, jj)] : -c;
+        if (ii < 0) return ghost_v(FLURSYS_SIDE_LEFT, c, j * dy);
+        if (ii >= nx) return ghost_v(FLURSYS_SIDE_RIGHT, c, j * dy);
+        return c;
+    }
+    // transported (:2201-2212)
+    double transported(double fv, double left, double right) const {
+        if (cfg.convection == FLURSYS_CONVECTION_UPWIND) return fv >= 0.0 ? left : right;
+        return 0.5 * (left + right);
+    }
+
+    // apply_velocity_boundaries (:1981-2044)
+    void apply_boundaries(std::vector<double> &uu, std::vector<double> &vv) const {
+        double bu, bv;
+        for (int64_t j = 0; j < ny; ++j) {
+            double y = (j + 0.5) * dy;
+            switch (cm.kind(FLURSYS_SIDE_LEFT)) {
+                case BK_VELOCITY: cm.velocity(FLURSYS_SIDE_LEFT, 0.0, y, &bu, &bv); uu[iu(0, j)] = bu; break;
+                case BK_SYMMETRY: uu[iu(0, j)] = 0.0; break;
+                case BK_OUTLET: uu[iu(0, j)] = uu[iu(1, j)]; break;
+            }
+            switch (cm.kind(FLURSYS_SIDE_RIGHT)) {
+                case BK_VELOCITY: cm.velocity(FLURSYS_SIDE_RIGHT, length, y, &bu, &bv); uu[iu(nx, j)] = bu; break;
+                case BK_SYMMETRY: uu[iu(nx, j)] = 0.0; break;
+                case BK_OUTLET: uu[iu(nx, j)] = uu[iu(nx - 1, j)]; break;
+            }
+        }
+        for (int64_t i = 0; i < nx; ++i) {
+            double x = (i + 0.5) * dx;
+            switch (cm.kind(FLURSYS_SIDE_BOTTOM)) {
+                case BK_VELOCITY: cm.velocity(FLURSYS_SIDE_BOTTOM, x, 0.0, &bu, &bv); vv[iv(i, 0)] = bv; break;
+                case BK_SYMMETRY: vv[iv(i, 0)] = 0.0; break;
+                case BK_OUTLET: vv[iv(i, 0)] = vv[iv(i, 1)]; break;
+            }
+            switch (cm.kind(FLURSYS_SIDE_TOP)) {
+                case BK_VELOCITY: cm.velocity(FLURSYS_SIDE_TOP, x, height, &bu, &bv); vv[iv(i, ny)] = bv; break;
+                case BK_SYMMETRY: vv[iv(i, ny)] = 0.0; break;
+                case BK_OUTLET: vv[iv(i, ny)] = vv[iv(i, ny - 1)]; break;
+            }
+        }
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 1; i < nx; ++i)
+                if (!u_open(i, j)) uu[iu(i, j)] = 0.0;
+        for (int64_t j = 1; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i)
+                if (!v_open(i, j)) vv[iv(i, j)] = 0.0;
+    }
+
+    // initialize_velocity (:588-620)
+    void initialize_velocity() {
+        double a, b;
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i <= nx; ++i) {
+                cm.initial_velocity(i * dx, (j + 0.5) * dy, &a, &b);
+                u[iu(i, j)] = u_open(i, j) ? a : 0.0;
+            }
+        for (int64_t j = 0; j <= ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                cm.initial_velocity((i + 0.5) * dx, j * dy, &a, &b);
+                v[iv(i, j)] = v_open(i, j) ? b : 0.0;
+            }
+        apply_boundaries(u, v);
+    }
+
+    bool simple() const { return cfg.coupling == FLURSYS_COUPLING_SIMPLE; }
+
+    // predict_momentum (:748-922), without buoyancy.
+    int32_t predict(double step_dt) override {
+        std::fill(us.begin(), us.end(), 0.0);
+        std::fill(vs.begin(), vs.end(), 0.0);
+        const bool with_p = simple();
+        const double relax = with_p ? cfg.velocity_relaxation : 1.0;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 1; i < nx; ++i) {
+                if (!u_open(i, j)) continue;
+                double up = u[iu(i, j)];
+                double ue_nb = u_nb(u, i, j, 1, 0, up), uw_nb = u_nb(u, i, j, -1, 0, up);
+                double un_nb = u_nb(u, i, j, 0, 1, up), us_nb = u_nb(u, i, j, 0, -1, up);
+                double ue = 0.5 * (up + ue_nb), uw = 0.5 * (uw_nb + up);
+                double vn = 0.5 * (v[iv(i - 1, j + 1)] + v[iv(i, j + 1)]);
+                double vsf = 0.5 * (v[iv(i - 1, j)] + v[iv(i, j)]);
+                double pe = transported(ue, up, ue_nb), pw = transported(uw, uw_nb, up);
+                double pn = transported(vn, up, un_nb), ps = transported(vsf, us_nb, up);
+                double conv = (ue * pe - uw * pw) / dx + (vn * pn - vsf * ps) / dy;
+                double diff = (ue_nb - 2.0 * up + uw_nb) / (dx * dx) + (un_nb - 2.0 * up + us_nb) / (dy * dy);
+                double pg = with_p ? (p[ic(i, j)] - p[ic(i - 1, j)]) / dx : 0.0;
+                us[iu(i, j)] = up + relax * step_dt * (-conv + nu * diff - pg / rho);
+            }
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+        for (int64_t j = 1; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                if (!v_open(i, j)) continue;
+                double vp = v[iv(i, j)];
+                double ve_nb = v_nb(v, i, j, 1, 0, vp), vw_nb = v_nb(v, i, j, -1, 0, vp);
+                double vn_nb = v_nb(v, i, j, 0, 1, vp), vs_nb = v_nb(v, i, j, 0, -1, vp);
+                double ue = 0.5 * (u[iu(i + 1, j - 1)] + u[iu(i + 1, j)]);
+                double uw = 0.5 * (u[iu(i, j - 1)] + u[iu(i, j)]);
+                double vn = 0.5 * (vp + vn_nb), vsf = 0.5 * (vs_nb + vp);
+                double pe = transported(ue, vp, ve_nb), pw = transported(uw, vw_nb, vp);
+                double pn = transported(vn, vp, vn_nb), ps = transported(vsf, vs_nb, vp);
+                double conv = (ue * pe - uw * pw) / dx + (vn * pn - vsf * ps) / dy;
+                double diff = (ve_nb - 2.0 * vp + vw_nb) / (dx * dx) + (vn_nb - 2.0 * vp + vs_nb) / (dy * dy);
+                double pg = with_p ? (p[ic(i, j)] - p[ic(i, j - 1)]) / dy : 0.0;
+                vs[iv(i, j)] = vp + relax * step_dt * (-conv + nu * diff - pg / rho);
+            }
+        return FLURSYS_OK;
+    }
+
+    // build_pressure_rhs (:924-970)
+    int32_t rhs_phase(double step_dt) override {
+        const double scale = simple() ? cfg.velocity_relaxation : 1.0;
+        const double rho_over_dt = rho / (scale * step_dt);
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                if (sol(i, j) || outlet_cell(i, j)) {
+                    rhs[ic(i, j)] = 0.0;
+                    continue;
+                }
+                double div = (us[iu(i + 1, j)] - us[iu(i, j)]) / dx + (vs[iv(i, j + 1)] - vs[iv(i, j)]) / dy;
+                rhs[ic(i, j)] = rho_over_dt * div;
+            }
+        return FLURSYS_OK;
+    }
+
+    // pressure_residual (:1532-1567)
+    double pressure_residual() const override {
+        const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy);
+        double m = 0.0;
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                if (sol(i, j) || outlet_cell(i, j)) continue;
+                double p0 = p[ic(i, j)];
+                double pe = (i + 1 < nx && !sol(i + 1, j)) ? p[ic(i + 1, j)] : p0;
+                double pw = (i > 0 && !sol(i - 1, j)) ? p[ic(i - 1, j)] : p0;
+                double pn = (j + 1 < ny && !sol(i, j + 1)) ? p[ic(i, j + 1)] : p0;
+                double ps = (j > 0 && !sol(i, j - 1)) ? p[ic(i, j - 1)] : p0;
+                double lap = (pe - 2.0 * p0 + pw) * idx2 + (pn - 2.0 * p0 + ps) * idy2;
+                m = std::max(m, std::fabs(lap - rhs[ic(i, j)]));
+            }
+        return m;
+    }
+
+    // solve_pressure_sor (:979-1046)
+    int32_t pressure_sor(double *res_out, int64_t *its_out) {
+        const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy);
+        const double omega = cfg.pressure_omega;
+        double residual = INFINITY;
+        int64_t its = 0;
+        for (int64_t it = 0; it < cfg.pressure_max_iters; ++it) {
+            its = it + 1;
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    if (sol(i, j)) { p[ic(i, j)] = 0.0; continue; }
+                    if (outlet_cell(i, j)) { p[ic(i, j)] = outlet_pressure(); continue; }
+                    double ap = 0.0, s = 0.0;
+                    if (i + 1 < nx && !sol(i + 1, j)) { ap += idx2; s += idx2 * p[ic(i + 1, j)]; }
+                    if (i > 0 && !sol(i - 1, j)) { ap += idx2; s += idx2 * p[ic(i - 1, j)]; }
+                    if (j + 1 < ny && !sol(i, j + 1)) { ap += idy2; s += idy2 * p[ic(i, j + 1)]; }
+                    if (j > 0 && !sol(i, j - 1)) { ap += idy2; s += idy2 * p[ic(i, j - 1)]; }
+                    if (ap > 0.0) {
+                        double cand = (s - rhs[ic(i, j)]) / ap;
+                        double old = p[ic(i, j)];
+                        p[ic(i, j)] = old + omega * (cand - old);
+                    }
+                }
+            if (reference_required()) {
+                int64_t ref = -1;  // find_reference_cell (:1614-1623)
+                for (int64_t k = 0; k < nx * ny && ref < 0; ++k)
+                    if (!solid[k]) ref = k;
+                if (ref >= 0) {
+                    double pr = p[ref];
+                    for (int64_t k = 0; k < nx * ny; ++k)
+                        if (!solid[k]) p[k] -= pr;
+                }
+            }
+            residual = pressure_residual();
+            if (!std::isfinite(residual)) {
+                err = "Pressure solver produced a non-finite residual";
+                return FLURSYS_ERR_NON_FINITE;
+            }
+            if (residual < cfg.pressure_tolerance) break;
+        }
+        *res_out = residual;
+        *its_out = its;
+        return FLURSYS_OK;
+    }
+
+    double last_initial = 0.0;
+    int32_t last_linear_status = FLURSYS_LINEAR_CONVERGED;
+
+    // solve_pressure_pcg (:1048-1214)
+    int32_t pressure(double *res_out, int64_t *its_out) override {
+        if (cfg.pressure_solver == FLURSYS_PRESSURE_SOR) return pressure_sor(res_out, its_out);
+        const int64_t n = nx * ny;
+        std::vector<double> x(p), b(n);
+        const double op_ = outlet_pressure();
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t k = ic(i, j);
+                if (sol(i, j) || outlet_cell(i, j)) {
+                    double val = outlet_cell(i, j) ? op_ : 0.0;
+                    x[k] = val;
+                    b[k] = val;
+                } else {
+                    b[k] = -rhs[k];
+                }
+            }
+        Operator2D op(this);
+        StopRule stop;
+        stop.rule = cfg.stop_rule == FLURSYS_STOP_REL_L2 ? FLURSYS_STOP_REL_L2 : FLURSYS_STOP_ABS_INF;
+        stop.tol = cfg.pressure_tolerance;
+        stop.atol = cfg.pressure_atol;
+        stop.rtol = cfg.pressure_rtol;
+        PcgResult r = pcg_core(op, b, x, stop, cfg.pressure_max_iters);
+        if (r.status != FLURSYS_OK) {
+            err = r.error;
+            return r.status;
+        }
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t k = ic(i, j);
+                p[k] = sol(i, j) ? 0.0 : (outlet_cell(i, j) ? op_ : x[k]);
+            }
+        last_initial = r.initial;
+        last_linear_status = r.linear_status;
+        *res_out = r.residual;
+        *its_out = r.iterations;
+        return FLURSYS_OK;
+    }
+
+    // correct_velocity (:1322-1379)
+    int32_t correct(double step_dt) override {
+        const double scale = simple() ? cfg.velocity_relaxation : 1.0;
+        const double dt_over_rho = scale * step_dt / rho;
+        u = us;
+        v = vs;
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 1; i < nx; ++i)
+                u[iu(i, j)] = u_open(i, j) ? us[iu(i, j)] - dt_over_rho * ((p[ic(i, j)] - p[ic(i - 1, j)]) / dx) : 0.0;
+        for (int64_t j = 1; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i)
+                v[iv(i, j)] = v_open(i, j) ? vs[iv(i, j)] - dt_over_rho * ((p[ic(i, j)] - p[ic(i, j - 1)]) / dy) : 0.0;
+        return FLURSYS_OK;
+    }
+
+    // derivative_x_slice / derivative_y_slice (:2227-2285)
+    double ddx_cell(const std::vector<double> &f, int64_t i, int64_t j) const {
+        double c = f[ic(i, j)];
+        bool e_ok = i + 1 < nx && !sol(i + 1, j), w_ok = i > 0 && !sol(i - 1, j);
+        double e = e_ok ? f[ic(i + 1, j)] : c, w = w_ok ? f[ic(i - 1, j)] : c;
+        if (e_ok && w_ok) return (e - w) / (2.0 * dx);
+        if (e_ok) return (e - c) / dx;
+        if (w_ok) return (c - w) / dx;
+        return 0.0;
+    }
+    double ddy_cell(const std::vector<double> &f, int64_t i, int64_t j) const {
+        double c = f[ic(i, j)];
+        bool n_ok = j + 1 < ny && !sol(i, j + 1), s_ok = j > 0 && !sol(i, j - 1);
+        double n = n_ok ? f[ic(i, j + 1)] : c, s = s_ok ? f[ic(i, j - 1)] : c;
+        if (n_ok && s_ok) return (n - s) / (2.0 * dy);
+        if (n_ok) return (n - c) / dy;
+        if (s_ok) return (c - s) / dy;
+        return 0.0;
+    }
+    // compute_cell_fields (:1381-1439)
+    void compute_cell_fields() {
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t k = ic(i, j);
+                if (sol(i, j)) { uc[k] = vc[k] = speed[k] = 0.0; continue; }
+                double a = 0.5 * (u[iu(i, j)] + u[iu(i + 1, j)]);
+                double b = 0.5 * (v[iv(i, j)] + v[iv(i, j + 1)]);
+                uc[k] = a;
+                vc[k] = b;
+                speed[k] = std::sqrt(a * a + b * b);
+            }
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i)
+                vort[ic(i, j)] = sol(i, j) ? 0.0 : ddx_cell(vc, i, j) - ddy_cell(uc, i, j);
+    }
+    // max_divergence (:1569-1582)
+    double max_divergence() const override {
+        double m = 0.0;
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                if (sol(i, j)) continue;
+                double d = (u[iu(i + 1, j)] - u[iu(i, j)]) / dx + (v[iv(i, j + 1)] - v[iv(i, j)]) / dy;
+                m = std::max(m, std::fabs(d));
+            }
+        return m;
+    }
+    double max_speed() const override { return field_max_abs(speed); }
+
+    // cylinder_force_coefficients (:1634-1676)
+    void forces(double *cd, double *cl) const {
+        *cd = *cl = 0.0;
+        if (cm.c.kind != FLURSYS_CASE_CYLINDER) return;
+        double mu = cm.c.cylinder_mu, fx = 0.0, fy = 0.0;
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                if (sol(i, j)) continue;
+                double pp = p[ic(i, j)], a = uc[ic(i, j)], b = vc[ic(i, j)];
+                if (i + 1 < nx && sol(i + 1, j)) { fx += pp * dy; fy += mu * b / (0.5 * dx) * dy; }
+                if (i > 0 && sol(i - 1, j)) { fx -= pp * dy; fy += mu * b / (0.5 * dx) * dy; }
+                if (j + 1 < ny && sol(i, j + 1)) { fy += pp * dx; fx += mu * a / (0.5 * dy) * dx; }
+                if (j > 0 && sol(i, j - 1)) { fy -= pp * dx; fx += mu * a / (0.5 * dy) * dx; }
+            }
+        double q = 0.5 * rho * cm.c.reference_velocity * cm.c.reference_velocity * cm.c.cylinder_diameter;
+        if (q > 0.0) { *cd = fx / q; *cl = fy / q; }
+    }
+
+    // reached_end_time (:557-561)
+    bool reached_end_time() const {
+        double tol = 2.220446049250313e-16 * std::max(std::fabs(cfg.t_end), 1.0) * 16.0;
+        return cfg.coupling == FLURSYS_COUPLING_PROJECTION && time >= cfg.t_end - tol;
+    }
+
+    // advance_one_step (:622-746) + advance() (:523-555)
+    int32_t advance(FlursysStepReport *rep) override {
+        if (reached_end_time()) {
+            err = "projection simulation has already reached t_end";
+            return FLURSYS_ERR_REACHED_END_TIME;
+        }
+        double step_dt = cfg.dt;
+        if (cfg.adaptive) {
+            int32_t st = adaptive_dt(current_dt, field_max_abs(u), field_max_abs(v), dx, dy, nu, -1.0,
+                                     cfg.min_dt, cfg.max_dt, cfg.target_cfl, cfg.target_diffusion_number,
+                                     cfg.max_growth_factor, &step_dt, &err);
+            if (st) return st;
+        }
+        if (cfg.coupling == FLURSYS_COUPLING_PROJECTION) {
+            double remaining = cfg.t_end - time;
+            step_dt = std::min(step_dt, remaining);
+            if (step_dt <= 0.0) {
+                err = "projection simulation has already reached t_end";
+                return FLURSYS_ERR_REACHED_END_TIME;
+            }
+        }
+        if (cfg.adaptive) current_dt = step_dt;
+        std::vector<double> old_u(u), old_v(v);
+        const bool smp = simple();
+        predict(step_dt);
+        apply_boundaries(us, vs);
+        std::vector<double> old_p;
+        if (smp) {
+            old_p = p;
+            std::fill(p.begin(), p.end(), 0.0);
+        }
+        rhs_phase(step_dt);
+        double res = 0.0;
+        int64_t its = 0;
+        int32_t st = pressure(&res, &its);
+        if (st) return st;
+        correct(step_dt);
+        if (smp)
+            for (size_t k = 0; k < p.size(); ++k) p[k] = old_p[k] + cfg.pressure_relaxation * p[k];
+        apply_boundaries(u, v);
+        step += 1;
+        if (cfg.coupling == FLURSYS_COUPLING_PROJECTION) time += step_dt;
+        else time = step * cfg.dt;
+        compute_cell_fields();
+        // ensure_finite (:1707-1742)
+        const char *names[4] = {"pressure", "u", "v", "speed"};
+        std::vector<double> *fs[4] = {&p, &u, &v, &speed};
+        for (int f = 0; f < 4; ++f) {
+            size_t bad = 0;
+            if (!all_finite(*fs[f], &bad)) {
+                char buf[256];
+                std::snprintf(buf, sizeof buf, "Non-finite %s value at flat index %zu: %g (step %lld)",
+                              names[f], bad, (*fs[f])[bad], (long long)step);
+                err = buf;
+                return FLURSYS_ERR_NON_FINITE;
+            }
+        }
+        double mu_ = field_max_abs(u), mv_ = field_max_abs(v);
+        double vel_change = 0.0;
+        for (size_t k = 0; k < u.size(); ++k) vel_change = std::max(vel_change, std::fabs(u[k] - old_u[k]));
+        double vch = 0.0;
+        for (size_t k = 0; k < v.size(); ++k) vch = std::max(vch, std::fabs(v[k] - old_v[k]));
+        vel_change = std::max(vel_change, vch);
+        if (rep) {
+            std::memset(rep, 0, sizeof *rep);
+            rep->iteration = step;
+            rep->time = time;
+            rep->time_step = step_dt;
+            rep->continuity_residual = max_divergence();
+            rep->pressure_residual = res;
+            rep->pressure_iterations = its;
+            rep->momentum_residual = vel_change;
+            rep->max_speed = max_speed();
+            rep->momentum_cfl = step_dt * (mu_ / dx + mv_ / dy);
+            rep->viscous_diffusion_number = nu * step_dt * (1.0 / (dx * dx) + 1.0 / (dy * dy));
+            forces(&rep->drag_coefficient, &rep->lift_coefficient);
+            rep->converged = cm.c.kind != FLURSYS_CASE_CYLINDER && step >= cfg.minimum_steps &&
+                             vel_change < cfg.steady_tolerance &&
+                             rep->continuity_residual < 10.0 * cfg.pressure_tolerance;
+            rep->reached_end_time = reached_end_time();
+            rep->pressure_initial_residual = last_initial;
+            rep->pressure_status = last_linear_status;
+        }
+        return FLURSYS_OK;
+    }
+
+    std::vector<double> *field(int32_t id) override {
+        switch (id) {
+            case FLURSYS_FIELD_U: return &u;
+            case FLURSYS_FIELD_V: return &v;
+            case FLURSYS_FIELD_PRESSURE: return &p;
+            case FLURSYS_FIELD_RHS: return &rhs;
+            case FLURSYS_FIELD_U_STAR: return &us;
+            case FLURSYS_FIELD_V_STAR: return &vs;
+            case FLURSYS_FIELD_SPEED: return &speed;
+            case FLURSYS_FIELD_VORTICITY: return &vort;
+            case FLURSYS_FIELD_U_CELL: return &uc;
+            case FLURSYS_FIELD_V_CELL: return &vc;
+            default: return nullptr;
+        }
+    }
+};
+
+bool Operator2D::identity_row(int64_t k) const {
+    int64_t i = k % s->nx, j = k / s->nx;
+    return s->sol(i, j) || s->outlet_cell(i, j);
+}
+double Operator2D::diagonal(int64_t k) const {
+    int64_t i = k % s->nx, j = k / s->nx;
+    const double idx2 = 1.0 / (s->dx * s->dx), idy2 = 1.0 / (s->dy * s->dy);
+    if (identity_row(k)) return 0.0;
+    double dg = 0.0;
+    if (i + 1 < s->nx && !s->sol(i + 1, j)) dg += idx2;
+    if (i > 0 && !s->sol(i - 1, j)) dg += idx2;
+    if (j + 1 < s->ny && !s->sol(i, j + 1)) dg += idy2;
+    if (j > 0 && !s->sol(i, j - 1)) dg += idy2;
+    return dg;
+}
+// apply_pressure_operator (:1216-1255)
+void Operator2D::apply(const std::vector<double> &x, std::vector<double> &y) const {
+    const int64_t nx = s->nx, ny = s->ny;
+    const double idx2 = 1.0 / (s->dx * s->dx), idy2 = 1.0 / (s->dy * s->dy);
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+    for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i) {
+            int64_t k = i + nx * j;
+            if (s->sol(i, j) || s->outlet_cell(i, j)) { y[k] = x[k]; continue; }
+            double dg = 0.0, nb = 0.0;
+            if (i + 1 < nx && !s->sol(i + 1, j)) { dg += idx2; nb += idx2 * x[k + 1]; }
+            if (i > 0 && !s->sol(i - 1, j)) { dg += idx2; nb += idx2 * x[k - 1]; }
+            if (j + 1 < ny && !s->sol(i, j + 1)) { dg += idy2; nb += idy2 * x[k + nx]; }
+            if (j > 0 && !s->sol(i, j - 1)) { dg += idy2; nb += idy2 * x[k - nx]; }
+            y[k] = dg * x[k] - nb;
+        }
+}
+bool Operator2D::needs_projection() const { return s->reference_required(); }
+// project_zero_mean (:2338-2377) over fluid, non-Dirichlet cells.
+void Operator2D::project(std::vector<double> &vals) const {
+    const int64_t nx = s->nx, ny = s->ny;
+    double sum = 0.0;
+    int64_t count = 0;
+    for (int64_t j = 0; j < ny; ++j) {
+        double row = 0.0;
+        int64_t rc = 0;
+        for (int64_t i = 0; i < nx; ++i)
+            if (!s->sol(i, j) && !s->outlet_cell(i, j)) { row += vals[i + nx * j]; rc += 1; }
+        sum += row;
+        count += rc;
+    }
+    if (count == 0) return;
+    double mean = sum / (double)count;
+    for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i)
+            if (!s->sol(i, j) && !s->outlet_cell(i, j)) vals[i + nx * j] -= mean;
+}
+
+// Pure-Neumann 2D operator without solids for orc_stencil_pcg (the cavity
+// operator of apply_pressure_operator with zero-mean projections).
+struct Neumann2DOperator final : StructuredOperator {
+    int64_t nx, ny;
+    double idx2, idy2;
+    Neumann2DOperator(int64_t nx_, int64_t ny_, double dx, double dy)
+        : nx(nx_), ny(ny_), idx2(1.0 / (dx * dx)), idy2(1.0 / (dy * dy)) {}
+    bool identity_row(int64_t) const override { return false; }
+    double diagonal(int64_t k) const override {
+        int64_t i = k % nx, j = k / nx;
+        double dg = 0.0;
+        if (i + 1 < nx) dg += idx2;
+        if (i > 0) dg += idx2;
+        if (j + 1 < ny) dg += idy2;
+        if (j > 0) dg += idy2;
+        return dg;
+    }
+    void apply(const std::vector<double> &x, std::vector<double> &y) const override {
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                int64_t k = i + nx * j;
+                double dg = 0.0, nb = 0.0;
+                if (i + 1 < nx) { dg += idx2; nb += idx2 * x[k + 1]; }
+                if (i > 0) { dg += idx2; nb += idx2 * x[k - 1]; }
+                if (j + 1 < ny) { dg += idy2; nb += idy2 * x[k + nx]; }
+                if (j > 0) { dg += idy2; nb += idy2 * x[k - nx]; }
+                y[k] = dg * x[k] - nb;
+            }
+    }
+    bool needs_projection() const override { return true; }
+    void project(std::vector<double> &vals) const override {
+        double sum = 0.0;
+        for (int64_t j = 0; j < ny; ++j) {
+            double row = 0.0;
+            for (int64_t i = 0; i < nx; ++i) row += vals[i + nx * j];
+            sum += row;
+        }
+        double mean = sum / (double)(nx * ny);
+        for (auto &x : vals) x -= mean;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// src/linear: CSR (csr.rs), Jacobi (preconditioner.rs), solvers (solver.rs).
+// ---------------------------------------------------------------------------
+struct Csr {
+    int64_t nrows, ncols;
+    const int64_t *ro;
+    const int64_t *ci;
+    const double *v;
+};
+
+// validate_csr (csr.rs:194-247)
+int32_t validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t *ro, const int64_t *ci,
+                     const double *v, std::string *msg) {
+    if (!ro) { *msg = "row_offsets length must equal nrows + 1"; return FLURSYS_ERR_INVALID_CSR; }
+    if (ro[0] != 0) { *msg = "first row offset must be zero"; return FLURSYS_ERR_INVALID_CSR; }
+    if (ro[nrows] != nnz) { *msg = "last row offset must equal value count"; return FLURSYS_ERR_INVALID_CSR; }
+    for (int64_t r = 0; r < nrows; ++r) {
+        if (ro[r] > ro[r + 1]) { *msg = "row offsets must be monotonic"; return FLURSYS_ERR_INVALID_CSR; }
+        for (int64_t e = ro[r] + 1; e < ro[r + 1]; ++e)
+            if (ci[e - 1] >= ci[e]) { *msg = "row columns must be strictly ascending"; return FLURSYS_ERR_INVALID_CSR; }
+    }
+    for (int64_t e = 0; e < nnz; ++e)
+        if (ci[e] < 0 || ci[e] >= ncols) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "column %lld at entry %lld exceeds ncols", (long long)ci[e], (long long)e);
+            *msg = buf;
+            return FLURSYS_ERR_INVALID_CSR;
+        }
+    for (int64_t e = 0; e < nnz; ++e)
+        if (!std::isfinite(v[e])) { *msg = "non-finite matrix value"; return FLURSYS_ERR_NON_FINITE; }
+    return FLURSYS_OK;
+}
+
+// spmv_into (csr.rs:89-106)
+int32_t spmv(const Csr &a, const double *x, double *y) {
+    for (int64_t r = 0; r < a.nrows; ++r) {
+        double s = 0.0;
+        for (int64_t e = a.ro[r]; e < a.ro[r + 1]; ++e) s += a.v[e] * x[a.ci[e]];
+        if (!std::isfinite(s)) return FLURSYS_ERR_NON_FINITE;
+        y[r] = s;
+    }
+    return FLURSYS_OK;
+}
+
+// diagonal_entry (csr.rs:67-82) + JacobiPreconditioner::new (preconditioner.rs:10-30)
+int32_t jacobi(const Csr &a, std::vector<double> &inv, int64_t *bad) {
+    inv.assign(a.nrows, 0.0);
+    for (int64_t r = 0; r < a.nrows; ++r) {
+        const int64_t *b = a.ci + a.ro[r], *e = a.ci + a.ro[r + 1];
+        const int64_t *f = std::lower_bound(b, e, r);
+        if (f == e || *f != r) { *bad = r; return FLURSYS_ERR_MISSING_DIAGONAL; }
+        double d = a.v[a.ro[r] + (f - b)];
+        if (!std::isfinite(d)) { *bad = r; return FLURSYS_ERR_NON_FINITE; }
+        if (d == 0.0) { *bad = r; return FLURSYS_ERR_ZERO_DIAGONAL; }
+        double iv = 1.0 / d;
+        if (!std::isfinite(iv)) { *bad = r; return FLURSYS_ERR_NON_FINITE; }
+        inv[r] = iv;
+    }
+    return FLURSYS_OK;
+}
+
+double sdot(const double *a, const double *b, int64_t n) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+void fill_report(FlursysLinearSolveReport *rep, int32_t status, int64_t its, double initial, double fin) {
+    if (!rep) return;
+    rep->status = status;
+    rep->reserved = 0;
+    rep->iterations = its;
+    rep->initial_residual = initial;
+    rep->final_residual = fin;
+    rep->relative_residual = initial == 0.0 ? 0.0 : fin / initial;
+}
+
+// validate_solve_inputs (solver.rs:258-300); dimensions are implied by n here.
+int32_t validate_inputs(int64_t n, const double *rhs, const double *x, const FlursysLinearSolverOptions &o) {
+    if (!std::isfinite(o.absolute_tolerance) || o.absolute_tolerance < 0.0 ||
+        !std::isfinite(o.relative_tolerance) || o.relative_tolerance < 0.0)
+        return FLURSYS_ERR_BREAKDOWN;
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(rhs[i])) return FLURSYS_ERR_NON_FINITE;
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(x[i])) return FLURSYS_ERR_NON_FINITE;
+    return FLURSYS_OK;
+}
+
+// solve_cg (solver.rs:62-153)
+int32_t solve_cg(const Csr &a, const double *rhs, double *x, const FlursysLinearSolverOptions &o,
+                 const std::vector<double> *inv, FlursysLinearSolveReport *rep) {
+    const int64_t n = a.nrows;
+    int32_t st = validate_inputs(n, rhs, x, o);
+    if (st) return st;
+    std::vector<double> r(n), d(n), q(n), z(n);
+    if ((st = spmv(a, x, r.data()))) return st;
+    for (int64_t i = 0; i < n; ++i) {
+        r[i] = rhs[i] - r[i];
+        if (!std::isfinite(r[i])) return FLURSYS_ERR_NON_FINITE;
+    }
+    double initial = std::sqrt(sdot(r.data(), r.data(), n));
+    if (!std::isfinite(initial)) return FLURSYS_ERR_NON_FINITE;
+    double threshold = o.absolute_tolerance + o.relative_tolerance * initial;
+    if (initial <= threshold) { fill_report(rep, FLURSYS_LINEAR_CONVERGED, 0, initial, initial); return FLURSYS_OK; }
+    auto precond = [&]() -> int32_t {
+        if (inv) {
+            for (int64_t i = 0; i < n; ++i) {
+                z[i] = r[i] * (*inv)[i];
+                if (!std::isfinite(z[i])) return FLURSYS_ERR_NON_FINITE;
+            }
+        } else {
+            z = r;
+        }
+        return FLURSYS_OK;
+    };
+    if ((st = precond())) return st;
+    d = z;
+    double rho = sdot(r.data(), z.data(), n);
+    if (!std::isfinite(rho)) return FLURSYS_ERR_NON_FINITE;
+    for (int64_t it = 1; it <= o.max_iterations; ++it) {
+        if ((st = spmv(a, d.data(), q.data()))) return st;
+        double den = sdot(d.data(), q.data(), n);
+        if (!std::isfinite(den) || std::fabs(den) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        double alpha = rho / den;
+        if (!std::isfinite(alpha)) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * d[i];
+            r[i] -= alpha * q[i];
+        }
+        double rn2 = sdot(r.data(), r.data(), n);
+        if (!std::isfinite(rn2)) return FLURSYS_ERR_NON_FINITE;
+        double rn = std::sqrt(rn2);
+        if (rn <= threshold) { fill_report(rep, FLURSYS_LINEAR_CONVERGED, it, initial, rn); return FLURSYS_OK; }
+        if ((st = precond())) return st;
+        double rho_new = sdot(r.data(), z.data(), n);
+        if (!std::isfinite(rho_new) || std::fabs(rho) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        double beta = rho_new / rho;
+        if (!std::isfinite(beta)) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t i = 0; i < n; ++i) d[i] = z[i] + beta * d[i];
+        rho = rho_new;
+    }
+    double fin = std::sqrt(sdot(r.data(), r.data(), n));
+    fill_report(rep, FLURSYS_LINEAR_MAX_ITERATIONS, o.max_iterations, initial, fin);
+    return FLURSYS_OK;
+}
+
+// bicgstab (solver.rs:155-256)
+int32_t solve_bicgstab(const Csr &a, const double *rhs, double *x, const FlursysLinearSolverOptions &o,
+                       FlursysLinearSolveReport *rep) {
+    const int64_t n = a.nrows;
+    int32_t st = validate_inputs(n, rhs, x, o);
+    if (st) return st;
+    std::vector<double> r(n), rh, p(n, 0.0), v(n, 0.0), s(n), t(n);
+    if ((st = spmv(a, x, r.data()))) return st;
+    for (int64_t i = 0; i < n; ++i) {
+        r[i] = rhs[i] - r[i];
+        if (!std::isfinite(r[i])) return FLURSYS_ERR_NON_FINITE;
+    }
+    rh = r;
+    double initial = std::sqrt(sdot(r.data(), r.data(), n));
+    if (!std::isfinite(initial)) return FLURSYS_ERR_NON_FINITE;
+    double threshold = o.absolute_tolerance + o.relative_tolerance * initial;
+    if (initial <= threshold) { fill_report(rep, FLURSYS_LINEAR_CONVERGED, 0, initial, initial); return FLURSYS_OK; }
+    double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+    for (int64_t it = 1; it <= o.max_iterations; ++it) {
+        double rho = sdot(rh.data(), r.data(), n);
+        if (!std::isfinite(rho) || std::fabs(rho) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        double beta = (rho / rho_prev) * (alpha / omega);
+        if (!std::isfinite(beta)) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        if ((st = spmv(a, p.data(), v.data()))) return st;
+        double den = sdot(rh.data(), v.data(), n);
+        if (!std::isfinite(den) || std::fabs(den) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        alpha = rho / den;
+        if (!std::isfinite(alpha)) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+        double sn2 = sdot(s.data(), s.data(), n);
+        if (!std::isfinite(sn2)) return FLURSYS_ERR_NON_FINITE;
+        double sn = std::sqrt(sn2);
+        if (sn <= threshold) {
+            for (int64_t i = 0; i < n; ++i) x[i] += alpha * p[i];
+            fill_report(rep, FLURSYS_LINEAR_CONVERGED, it, initial, sn);
+            return FLURSYS_OK;
+        }
+        if ((st = spmv(a, s.data(), t.data()))) return st;
+        double tt = sdot(t.data(), t.data(), n);
+        if (!std::isfinite(tt) || std::fabs(tt) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        omega = sdot(t.data(), s.data(), n) / tt;
+        if (!std::isfinite(omega) || std::fabs(omega) <= 1.0e-30) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p[i] + omega * s[i];
+            r[i] = s[i] - omega * t[i];
+        }
+        double rn2 = sdot(r.data(), r.data(), n);
+        if (!std::isfinite(rn2)) return FLURSYS_ERR_NON_FINITE;
+        double rn = std::sqrt(rn2);
+        if (rn <= threshold) { fill_report(rep, FLURSYS_LINEAR_CONVERGED, it, initial, rn); return FLURSYS_OK; }
+        rho_prev = rho;
+    }
+    double fin = std::sqrt(sdot(r.data(), r.data(), n));
+    fill_report(rep, FLURSYS_LINEAR_MAX_ITERATIONS, o.max_iterations, initial, fin);
+    return FLURSYS_OK;
+}
+
+// SimulationConfig::validate (incompressible.rs:93-191) without thermal
+// checks, and LidDrivenCavity3DConfig::validate (incompressible_3d.rs:50-84).
+int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
+    auto fin_pos = [](double x) { return std::isfinite(x) && x > 0.0; };
+    if (c.dimension == 3) {
+        if (c.nx < 4 || c.ny < 4 || c.nz < 4) { *msg = "nx, ny, and nz must all be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0 && c.case_params.depth > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.density)) { *msg = "density must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.reference_velocity)) { *msg = "lid_velocity must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.case_params.reynolds)) { *msg = "reynolds must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.dt)) { *msg = "dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.max_steps <= 0 || c.pressure_max_iters <= 0) { *msg = "iteration limits must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.pressure_tolerance)) { *msg = "pressure_tolerance must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!(std::isfinite(c.pressure_omega) && c.pressure_omega > 0.0 && c.pressure_omega < 2.0)) { *msg = "pressure_omega must lie between 0 and 2"; return FLURSYS_ERR_INVALID_CONFIG; }
+        return FLURSYS_OK;
+    }
+    if (c.dimension != 2) { *msg = "dimension must be 2 or 3"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.nx < 4 || c.ny < 4) { *msg = "nx and ny must be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.dt)) { *msg = "dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.t_end) || c.t_end < 0.0) { *msg = "t_end must be finite and non-negative"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.coupling == FLURSYS_COUPLING_PROJECTION && c.t_end == 0.0) { *msg = "t_end must be positive for projection coupling"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.max_steps <= 0) { *msg = "max_steps must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.pressure_max_iters <= 0) { *msg = "pressure_max_iters must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.pressure_omega) || c.pressure_omega <= 0.0 || c.pressure_omega >= 2.0) { *msg = "pressure_omega must lie between 0 and 2"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.velocity_relaxation) || c.velocity_relaxation <= 0.0 || c.velocity_relaxation > 1.0) { *msg = "velocity_relaxation must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!std::isfinite(c.pressure_relaxation) || c.pressure_relaxation <= 0.0 || c.pressure_relaxation > 1.0) { *msg = "pressure_relaxation must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.steady_tolerance)) { *msg = "steady_tolerance must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (!fin_pos(c.case_params.density) || !fin_pos(c.case_params.kinematic_viscosity)) { *msg = "fluid density and kinematic viscosity must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.adaptive) {
+        if (c.coupling != FLURSYS_COUPLING_PROJECTION) { *msg = "adaptive time stepping requires transient projection coupling"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.min_dt)) { *msg = "adaptive min_dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!fin_pos(c.max_dt)) { *msg = "adaptive max_dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.min_dt > c.max_dt) { *msg = "adaptive min_dt must not exceed max_dt"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (c.dt < c.min_dt || c.dt > c.max_dt) { *msg = "adaptive initial dt must lie between min_dt and max_dt"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.target_cfl) || c.target_cfl <= 0.0 || c.target_cfl > 1.0) { *msg = "adaptive target_cfl must lie between 0 (exclusive) and 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.target_diffusion_number) || c.target_diffusion_number <= 0.0 || c.target_diffusion_number > 0.5) { *msg = "adaptive target_diffusion_number must lie between 0 (exclusive) and 0.5"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(c.max_growth_factor) || c.max_growth_factor < 1.0) { *msg = "adaptive max_growth_factor must be finite and at least 1"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
+    if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    return FLURSYS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C API
+// ===========================================================================
+extern "C" {
+
+void orc_set_threads(int32_t threads) { g_threads = threads < 1 ? 1 : threads; }
+int32_t orc_get_threads(void) { return g_threads; }
+
+int32_t orc_csr_validate(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t *ro, const int64_t *ci,
+                         const double *v, char *msg, size_t msg_size) {
+    std::string m;
+    int32_t st = validate_csr(nrows, ncols, nnz, ro, ci, v, &m);
+    copy_msg(m, msg, msg_size);
+    return st;
+}
+
+// CsrBuilder::add + finalize (csr.rs:131-192)
+int32_t orc_csr_build(int64_t nrows, int64_t ncols, int64_t nentries, const int64_t *rows,
+                      const int64_t *cols, const double *vals, int64_t *ro_out, int64_t *ci_out,
+                      double *v_out, int64_t *nnz_out) {
+    std::vector<std::tuple<int64_t, int64_t, double>> e;
+    e.reserve(nentries);
+    for (int64_t k = 0; k < nentries; ++k) {
+        if (rows[k] < 0 || rows[k] >= nrows || cols[k] < 0 || cols[k] >= ncols) return FLURSYS_ERR_INDEX_OUT_OF_BOUNDS;
+        if (!std::isfinite(vals[k])) return FLURSYS_ERR_NON_FINITE;
+        e.emplace_back(rows[k], cols[k], vals[k]);
+    }
+    // The reference sorts by (row, column) with an unstable sort and then sums
+    // duplicates in sorted order; duplicates of one (row, column) are summed
+    // in insertion order here (stable sort), which equals the reference's sum
+    // up to rounding when there are three or more duplicates.
+    std::stable_sort(e.begin(), e.end(), [](const auto &a, const auto &b) {
+        return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b) : std::get<1>(a) < std::get<1>(b);
+    });
+    int64_t nnz = 0;
+    size_t k = 0;
+    ro_out[0] = 0;
+    for (int64_t r = 0; r < nrows; ++r) {
+        while (k < e.size() && std::get<0>(e[k]) == r) {
+            int64_t col = std::get<1>(e[k]);
+            double s = 0.0;
+            while (k < e.size() && std::get<0>(e[k]) == r && std::get<1>(e[k]) == col) s += std::get<2>(e[k++]);
+            if (!std::isfinite(s)) return FLURSYS_ERR_NON_FINITE;
+            if (s != 0.0) { ci_out[nnz] = col; v_out[nnz] = s; ++nnz; }
+        }
+        ro_out[r + 1] = nnz;
+    }
+    *nnz_out = nnz;
+    return FLURSYS_OK;
+}
+
+int32_t orc_csr_spmv(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t *ro, const int64_t *ci,
+                     const double *v, const double *input, double *output) {
+    std::string m;
+    int32_t st = validate_csr(nrows, ncols, nnz, ro, ci, v, &m);
+    if (st) return st;
+    Csr a{nrows, ncols, ro, ci, v};
+    return spmv(a, input, output);
+}
+
+int32_t orc_jacobi_inverse_diagonal(int64_t n, int64_t nnz, const int64_t *ro, const int64_t *ci,
+                                    const double *v, double *inv_out, int64_t *bad_row) {
+    (void)nnz;
+    Csr a{n, n, ro, ci, v};
+    std::vector<double> inv;
+    int64_t bad = -1;
+    int32_t st = jacobi(a, inv, &bad);
+    if (bad_row) *bad_row = bad;
+    if (st) return st;
+    std::memcpy(inv_out, inv.data(), n * sizeof(double));
+    return FLURSYS_OK;
+}
+
+int32_t orc_csr_solve(int32_t method, int64_t n, int64_t nnz, const int64_t *ro, const int64_t *ci,
+                      const double *v, const double *rhs, double *x, const FlursysLinearSolverOptions *o,
+                      FlursysLinearSolveReport *rep) {
+    std::string m;
+    int32_t st = validate_csr(n, n, nnz, ro, ci, v, &m);
+    if (st) return st;
+    Csr a{n, n, ro, ci, v};
+    FlursysLinearSolverOptions opt = o ? *o : FlursysLinearSolverOptions{1e-10, 1e-8, 1000};
+    if (method == 2) return solve_bicgstab(a, rhs, x, opt, rep);
+    if (method == 1) {
+        std::vector<double> inv;
+        int64_t bad = -1;
+        if ((st = jacobi(a, inv, &bad))) return st;
+        return solve_cg(a, rhs, x, opt, &inv, rep);
+    }
+    return solve_cg(a, rhs, x, opt, nullptr, rep);
+}
+
+void orc_momentum_stability_numbers(double dt, double nu, double dx, double dy, double mu, double mv,
+                                    double *cfl, double *dnu) {
+    *cfl = dt * (mu / dx + mv / dy);
+    *dnu = nu * dt * (1.0 / (dx * dx) + 1.0 / (dy * dy));
+}
+
+int32_t orc_adaptive_time_step(double current_dt, double mu, double mv, double dx, double dy, double nu,
+                               double thermal, double min_dt, double max_dt, double target_cfl,
+                               double target_diff, double growth, double *dt_out, char *msg, size_t msg_size) {
+    std::string e;
+    int32_t st = adaptive_dt(current_dt, mu, mv, dx, dy, nu, thermal, min_dt, max_dt, target_cfl, target_diff,
+                             growth, dt_out, &e);
+    copy_msg(e, msg, msg_size);
+    return st;
+}
+
+// Defaults: LidDrivenCavity3DConfig::default() (incompressible_3d.rs:27-47)
+// and the CLI cavity defaults (src/bin/flursys.rs:102-123,236-300).
+int32_t orc_default_config(int32_t dimension, FlursysCudaConfig *c) {
+    if (!c) return FLURSYS_ERR_INVALID_ARGUMENT;
+    std::memset(c, 0, sizeof *c);
+    c->abi_version = FLURSYS_CUDA_ABI_VERSION;
+    c->dimension = dimension == 3 ? 3 : 2;
+    c->case_params.kind = FLURSYS_CASE_CAVITY;
+    c->case_params.length = 1.0;
+    c->case_params.height = 1.0;
+    c->case_params.depth = 1.0;
+    c->case_params.density = 1.0;
+    c->case_params.reference_velocity = 1.0;
+    c->case_params.reynolds = 100.0;
+    c->case_params.kinematic_viscosity = 0.01;
+    c->min_dt = 1.0e-6;
+    c->max_dt = 1.0e-2;
+    c->target_cfl = 0.5;
+    c->target_diffusion_number = 0.25;
+    c->max_growth_factor = 1.1;
+    c->pressure_solver = FLURSYS_PRESSURE_PCG;
+    c->pressure_atol = 0.0;
+    c->pressure_rtol = 1.0e-8;
+    c->precision = FLURSYS_PRECISION_F64;
+    c->residual_replacement_every = 50;
+    if (c->dimension == 3) {
+        c->nx = c->ny = c->nz = 32;
+        c->dt = 5.0e-4;
+        c->max_steps = 10000;
+        c->pressure_max_iters = 2000;
+        c->pressure_tolerance = 1.0e-6;
+        c->pressure_omega = 1.7;
+        c->pressure_solver = FLURSYS_PRESSURE_SOR;
+        c->stop_rule = FLURSYS_STOP_REFERENCE_RESIDUAL;
+        c->convection = FLURSYS_CONVECTION_CENTRAL;
+        c->t_end = 1e300;
+    } else {
+        c->nx = c->ny = 64;
+        c->nz = 1;
+        c->dt = 0.001;
+        c->t_end = 100.0;
+        c->max_steps = 100000;
+        c->convection = FLURSYS_CONVECTION_UPWIND;
+        c->coupling = FLURSYS_COUPLING_PROJECTION;
+        c->stop_rule = FLURSYS_STOP_ABS_INF;
+        c->pressure_max_iters = 1200;
+        c->pressure_tolerance = 1.0e-5;
+        c->pressure_omega = 1.7;
+        c->velocity_relaxation = 0.7;
+        c->pressure_relaxation = 0.3;
+        c->steady_tolerance = 1.0e-7;
+        c->minimum_steps = 2000;
+    }
+    return FLURSYS_OK;
+}
+
+int32_t orc_create(const FlursysCudaConfig *cfg, OracleSolver **out, char *msg, size_t msg_size) {
+    if (!cfg || !out) return FLURSYS_ERR_INVALID_ARGUMENT;
+    std::string m;
+    int32_t st = validate_config(*cfg, &m);
+    if (st) {
+        copy_msg(m, msg, msg_size);
+        return st;
+    }
+    if (cfg->dimension == 3) *out = new Solver3D(*cfg);
+    else *out = new Solver2D(*cfg);
+    return FLURSYS_OK;
+}
+
+int32_t orc_step(OracleSolver *s, int64_t nsteps, FlursysStepReport *rep) {
+    if (!s) return FLURSYS_ERR_INVALID_ARGUMENT;
+    for (int64_t n = 0; n < nsteps; ++n) {
+        int32_t st = s->advance(rep);
+        if (st) return st;
+        if (rep && s->cfg.dimension == 2 && (rep->converged || rep->reached_end_time)) break;
+    }
+    return FLURSYS_OK;
+}
+
+size_t orc_field_size(const OracleSolver *s, int32_t id) {
+    auto *f = const_cast<OracleSolver *>(s)->field(id);
+    return f ? f->size() : 0;
+}
+int32_t orc_get_field(const OracleSolver *s, int32_t id, double *out, size_t n) {
+    auto *f = const_cast<OracleSolver *>(s)->field(id);
+    if (!f) return FLURSYS_ERR_INVALID_ARGUMENT;
+    if (f->size() != n) return FLURSYS_ERR_DIMENSION_MISMATCH;
+    std::memcpy(out, f->data(), n * sizeof(double));
+    return FLURSYS_OK;
+}
+int32_t orc_set_field(OracleSolver *s, int32_t id, const double *in, size_t n) {
+    auto *f = s->field(id);
+    if (!f) return FLURSYS_ERR_INVALID_ARGUMENT;
+    if (f->size() != n) return FLURSYS_ERR_DIMENSION_MISMATCH;
+    std::memcpy(f->data(), in, n * sizeof(double));
+    return FLURSYS_OK;
+}
+int32_t orc_last_error(const OracleSolver *s, char *buf, size_t size) {
+    copy_msg(s ? s->err : std::string(), buf, size);
+    return FLURSYS_OK;
+}
+void orc_destroy(OracleSolver *s) { delete s; }
+
+int32_t orc_phase_predict(OracleSolver *s, double dt) { return s->predict(dt); }
+int32_t orc_phase_rhs(OracleSolver *s, double dt) { return s->rhs_phase(dt); }
+int32_t orc_phase_pressure(OracleSolver *s, double *res, int64_t *its) { return s->pressure(res, its); }
+int32_t orc_phase_correct(OracleSolver *s, double dt) { return s->correct(dt); }
+double orc_max_divergence(const OracleSolver *s) { return s->max_divergence(); }
+double orc_pressure_residual(const OracleSolver *s) { return s->pressure_residual(); }
+double orc_max_speed(const OracleSolver *s) { return s->max_speed(); }
+
+int32_t orc_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz,
+                        const double *rhs, double *x_inout, const FlursysLinearSolverOptions *o,
+                        FlursysLinearSolveReport *rep) {
+    if (nx < 1 || ny < 1 || nz < 1 || !rhs || !x_inout || !o) return FLURSYS_ERR_INVALID_ARGUMENT;
+    const int64_t n = nx * ny * nz;
+    std::vector<double> b(n), x(x_inout, x_inout + n);
+    for (int64_t k = 0; k < n; ++k) b[k] = -rhs[k];
+    StopRule stop;
+    stop.rule = FLURSYS_STOP_REL_L2;
+    stop.atol = o->absolute_tolerance;
+    stop.rtol = o->relative_tolerance;
+    PcgResult r;
+    if (nz == 1) {
+        Neumann2DOperator op(nx, ny, dx, dy);
+        r = pcg_core(op, b, x, stop, o->max_iterations);
+    } else {
+        Pinned3DOperator op(nx, ny, nz, dx, dy, dz);
+        b[0] = 0.0;
+        x[0] = 0.0;
+        r = pcg_core(op, b, x, stop, o->max_iterations);
+    }
+    if (r.status) return r.status;
+    std::memcpy(x_inout, x.data(), n * sizeof(double));
+    fill_report(rep, r.linear_status, r.iterations, r.initial, r.residual);
+    return FLURSYS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+"""3D lid-driven cavity: CUDA backend (through the C ABI) against the FP64
+oracle of src/solver/incompressible_3d.rs."""
+import numpy as np
+import pytest
+
+from flursys_b200 import _abi
+from flursys_b200.solver import _Handle
+
+from .paritylib import assert_close, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PARITY_TOL = 1e-10  # f64 mode: velocity and pressure rel L2 / rel max
+MIXED_TOL = 1e-6    # mixed mode: velocity rel L2 against the FP64 oracle
+
+
+def cfg3d(oracle, nx, ny, nz, solver=_abi.PRESSURE_PCG, rule=_abi.STOP_REL_L2, rtol=1e-13, precision=_abi.PRECISION_F64,
+          re=400.0, dt=None):
+    cfg = oracle.default_config(3)
+    cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+    cfg.case_params.reynolds = re
+    h = 1.0 / max(nx, ny, nz)
+    nu = 1.0 / re
+    cfg.dt = dt if dt is not None else min(0.5 * h, 0.25 * h * h / (3 * nu))
+    cfg.pressure_solver = solver
+    cfg.stop_rule = rule
+    cfg.pressure_rtol = rtol
+    cfg.pressure_atol = 0.0
+    cfg.pressure_max_iters = 20000
+    cfg.precision = precision
+    return cfg
+
+
+FIELDS = [(_abi.FIELD_U, "u"), (_abi.FIELD_V, "v"), (_abi.FIELD_W, "w"), (_abi.FIELD_PRESSURE, "p")]
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 20, 12)])
+def test_f64_steps_match_oracle(oracle, shape):
+    cfg = cfg3d(oracle, *shape)
+    ref = oracle.OracleSolver(cfg)
+    gpu = _Handle(cfg)
+    for _ in range(4):
+        r_ref = ref.step(1)
+        r_gpu = gpu.step(1)
+        assert abs(r_gpu.pressure_iterations - r_ref.pressure_iterations) <= 1
+    for fid, name in FIELDS:
+        assert_close(gpu.download(fid), ref.get(fid), PARITY_TOL, name)
+    assert abs(r_gpu.continuity_residual - ref.max_divergence()) <= 1e-9 * max(1.0, ref.max_divergence())
+    assert abs(r_gpu.max_speed - ref.max_speed()) <= 1e-12
+
+
+def test_phases_match_oracle_from_a_random_state(oracle):
+    nx, ny, nz = 12, 10, 14
+    cfg = cfg3d(oracle, nx, ny, nz)
+    rng = np.random.default_rng(7)
+    ref = oracle.OracleSolver(cfg)
+    gpu = _Handle(cfg)
+    for fid in (_abi.FIELD_U, _abi.FIELD_V, _abi.FIELD_W, _abi.FIELD_PRESSURE):
+        x = rng.standard_normal(gpu.field_size(fid))
+        if fid == _abi.FIELD_PRESSURE:
+            x[0] = 0.0
+        ref.set(fid, x)
+        gpu.upload(fid, x)
+    ref.step(1)
+    gpu.step(1)
+    for fid, name in [(_abi.FIELD_U_STAR, "u*"), (_abi.FIELD_V_STAR, "v*"), (_abi.FIELD_W_STAR, "w*"),
+                      (_abi.FIELD_RHS, "rhs")]:
+        assert_close(gpu.download(fid), ref.get(fid), 1e-14, name)
+    for fid, name in FIELDS:
+        assert_close(gpu.download(fid), ref.get(fid), PARITY_TOL, name)
+
+
+def test_iteration_counts_match_at_config_tolerance(oracle):
+    cfg = cfg3d(oracle, 20, 20, 20, rtol=1e-8)
+    ref = oracle.OracleSolver(cfg)
+    gpu = _Handle(cfg)
+    for _ in range(3):
+        a, b = ref.step(1), gpu.step(1)
+        assert abs(a.pressure_iterations - b.pressure_iterations) <= 1
+        assert b.pressure_true_relative_residual <= 1.01e-8
+
+
+def test_abs_inf_rule_matches_oracle(oracle):
+    cfg = cfg3d(oracle, 16, 16, 16, rule=_abi.STOP_REFERENCE_RESIDUAL)
+    cfg.pressure_tolerance = 1e-9
+    ref = oracle.OracleSolver(cfg)
+    gpu = _Handle(cfg)
+    a, b = ref.step(2), gpu.step(2)
+    assert abs(a.pressure_iterations - b.pressure_iterations) <= 1
+    assert b.pressure_residual < 1e-9
+    assert_close(gpu.download(_abi.FIELD_U), ref.get(_abi.FIELD_U), 1e-8, "u")
+
+
+def test_mixed_precision_against_fp64_oracle(oracle):
+    cfg64 = cfg3d(oracle, 32, 32, 32, rtol=1e-8)
+    cfgm = cfg3d(oracle, 32, 32, 32, rtol=1e-8, precision=_abi.PRECISION_MIXED)
+    ref = oracle.OracleSolver(cfg64)
+    gpu = _Handle(cfgm)
+    for _ in range(6):
+        ref.step(1)
+        rep = gpu.step(1)
+        assert rep.pressure_status == _abi.LINEAR_CONVERGED
+        assert rep.pressure_true_relative_residual <= 1.0e-8 * 1.0001
+    for fid, name in FIELDS[:3]:
+        assert rel_l2(gpu.download(fid), ref.get(fid)) <= MIXED_TOL, name
+
+
+def test_red_black_sor_meets_the_reference_smoke_gates(oracle):
+    # tests/smoke.rs:113-130 with the reference defaults (SOR, tol 1e-6)
+    cfg = oracle.default_config(3)
+    cfg.nx = cfg.ny = cfg.nz = 8
+    gpu = _Handle(cfg)
+    rep = gpu.step(2)
+    assert rep.iteration == 2
+    assert np.isfinite(rep.continuity_residual) and rep.continuity_residual < 1e-5
+    assert rep.max_speed > 0.0
+    assert rep.pressure_residual < 1e-6
+    ref = oracle.OracleSolver(cfg)
+    ref.step(2)
+    # Both solve the same system to 1e-6 in the reference residual.
+    assert rel_l2(gpu.download(_abi.FIELD_U), ref.get(_abi.FIELD_U)) < 1e-3
+
+
+def test_run_writes_field_vtk(tmp_path):
+    from flursys_b200 import LidDrivenCavity3DConfig, LidDrivenCavity3DSolver
+    cfg = LidDrivenCavity3DConfig(nx=8, ny=8, nz=8, max_steps=2, output_dir=str(tmp_path / "cavity-3d"))
+    summary = LidDrivenCavity3DSolver.new(cfg).run()
+    assert summary.steps == 2 and summary.max_divergence < 1e-5 and summary.max_speed > 0
+    assert (tmp_path / "cavity-3d" / "field.vtk").is_file()
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_F64, _abi.PRECISION_MIXED])
+def test_stencil_pcg_entry_matches_oracle(oracle, cudalib, precision):
+    import ctypes as C
+    nx, ny, nz = 20, 16, 12
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal(nx * ny * nz)
+    rhs[0] = 0.0
+    opts = _abi.LinearSolverOptions(0.0, 1e-10, 5000)
+    st, xref, rref = oracle.stencil_pcg(nx, ny, nz, 1 / nx, 1 / ny, 1 / nz, rhs, np.zeros_like(rhs), opts)
+    assert st == 0
+    x = np.zeros_like(rhs)
+    rep = _abi.LinearSolveReport()
+    st = cudalib.flursys_cuda_stencil_pcg(nx, ny, nz, 1 / nx, 1 / ny, 1 / nz, _abi.dptr(rhs), _abi.dptr(x), precision,
+                                          C.byref(opts), C.byref(rep))
+    assert st == 0 and rep.status == _abi.LINEAR_CONVERGED
+    tol = 1e-9 if precision == _abi.PRECISION_F64 else 1e-7
+    assert rel_l2(x, xref) < tol
+    if precision == _abi.PRECISION_F64:
+        assert abs(rep.iterations - rref.iterations) <= 1
