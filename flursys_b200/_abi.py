@@ -185,6 +185,7 @@ SIGNATURES = {
     "flursys_cuda_state": (C.c_int32, [_P, _I64P, _D]),
     "flursys_cuda_set_stream": (C.c_int32, [_P, _P]),
     "flursys_cuda_last_error": (C.c_int32, [_P, C.c_char_p, C.c_size_t]),
+    "flursys_cuda_solver_profile": (C.c_int32, [_P, _D, C.c_size_t]),
     "flursys_cuda_destroy": (C.c_int32, [_P]),
     "flursys_cuda_global_error": (C.c_int32, [C.c_char_p, C.c_size_t]),
     "flursys_cuda_csr_cg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,

@@ -62,8 +62,9 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
         if (c.max_steps <= 0 || c.pressure_max_iters <= 0) { *msg = "iteration limits must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!fin_pos(c.pressure_tolerance)) { *msg = "pressure_tolerance must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!(std::isfinite(c.pressure_omega) && c.pressure_omega > 0.0 && c.pressure_omega < 2.0)) { *msg = "pressure_omega must lie between 0 and 2"; return FLURSYS_ERR_INVALID_CONFIG; }
-        // Indices are 32-bit per dimension and 64-bit overall on the device.
-        if (c.nx > (1 << 20) || c.ny > (1 << 20) || c.nz > (1 << 20)) { *msg = "grid dimension too large"; return FLURSYS_ERR_INVALID_CONFIG; }
+        // Device indices are 32-bit: the face arrays must stay below 2^31 entries.
+        if (c.nx > (1 << 20) || c.ny > (1 << 20) || c.nz > (1 << 20) ||
+            (c.nx + 1) * (c.ny + 1) * (c.nz + 1) >= (1LL << 31)) { *msg = "grid too large for this backend"; return FLURSYS_ERR_INVALID_CONFIG; }
         return FLURSYS_OK;
     }
     if (c.dimension != 2) { *msg = "dimension must be 2 or 3"; return FLURSYS_ERR_INVALID_ARGUMENT; }
@@ -121,6 +122,8 @@ int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy
     a.partials = ws.partials; a.barrier = ws.barrier; a.result = ws.result;
     a.stop_rule = stop_rule; a.tol = tol; a.atol = atol; a.rtol = rtol;
     a.max_iters = max_iters; a.replace_every = replace_every > 0 ? replace_every : 50;
+    a.precision_vec_width = precision == FLURSYS_PRECISION_MIXED ? 4 : 2;
+    a.row_class = ws.row_class;
     cudaError_t e = cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream);
     if (e == cudaSuccess) e = pcg3d_launch(a, ws.grid, precision, stream);
     if (e != cudaSuccess) return set_cuda_error(err, e, "pcg3d launch");
@@ -129,6 +132,7 @@ int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy
 
 cudaError_t PcgWorkspace::allocate(long long n, int precision, int device, int dim) {
     free_all();
+    this->precision = precision;
     int maxgrid = 0;
     cudaError_t e = dim == 3 ? pcg3d_max_grid(precision, device, &maxgrid) : pcg2d_max_grid(precision, device, &maxgrid);
     if (e != cudaSuccess) return e;
@@ -149,7 +153,17 @@ cudaError_t PcgWorkspace::allocate(long long n, int precision, int device, int d
     return cudaSuccess;
 }
 
+cudaError_t PcgWorkspace::allocate3d(int nx, int ny, int nz, int prec, int device, cudaStream_t stream) {
+    cudaError_t e = allocate((long long)nx * ny * nz, prec, device, 3);
+    if (e == cudaSuccess) e = pcg3d_make_row_class(ny, nz, &row_class, stream);
+    return e;
+}
+
 void PcgWorkspace::free_all() {
+    cudaFree(row_class);
+    row_class = nullptr;
+    cudaFree(r_z);
+    r_z = nullptr;
     cudaFree(r); cudaFree(d0); cudaFree(d1); cudaFree(q); cudaFree(dx);
     cudaFree(partials); cudaFree(barrier); cudaFree(result);
     if (h_result) cudaFreeHost(h_result);
@@ -307,6 +321,13 @@ int32_t flursys_cuda_state(const FlursysCudaHandle *h, int64_t *step, double *ti
 int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream) {
     if (!h) { g_error = "null handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
     h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms, size_t n) {
+    if (!h || !phase_ms) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    const PcgResultDev *r = h->pcg.h_result;
+    for (size_t i = 0; i < n && i < 4; ++i) phase_ms[i] = r ? 1e-6 * (double)r->phase_ns[i] : 0.0;
     return FLURSYS_OK;
 }
 

@@ -17,12 +17,17 @@ namespace flursys {
 struct PcgWorkspace {
     int grid = 0;
     void *r = nullptr, *d0 = nullptr, *d1 = nullptr, *q = nullptr;
+    void *r_z = nullptr;  // 2D: stored preconditioned residual
     float *dx = nullptr;
     double *partials = nullptr;
     GridBarrier *barrier = nullptr;
     PcgResultDev *result = nullptr;
     PcgResultDev *h_result = nullptr;  // pinned host copy
+    unsigned char *row_class = nullptr;  // 3D: per-row boundary class
+    int precision = 0;
     cudaError_t allocate(long long n, int precision, int device, int dim);
+    // 3D pressure solves also need the per-row boundary class table.
+    cudaError_t allocate3d(int nx, int ny, int nz, int precision, int device, cudaStream_t stream);
     void free_all();
 };
 

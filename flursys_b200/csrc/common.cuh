@@ -31,7 +31,7 @@ struct GridBarrier {
 // Sense-free generation barrier for a cooperative (co-resident) launch.
 // Every wait is bounded: on timeout the error word is set and the caller is
 // told to leave its loop. Returns false when the barrier failed.
-__device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
+__device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -41,7 +41,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
         int ok = 1;
         const unsigned my_gen = gen.load(cuda::memory_order_acquire);
         const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-        if (arrived == gridDim.x - 1u) {
+        if (arrived == nblocks - 1u) {
             cnt.store(0u, cuda::memory_order_relaxed);
             gen.fetch_add(1u, cuda::memory_order_release);
         } else {
@@ -55,11 +55,15 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
                 __nanosleep(100);
             }
         }
+        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
     return s_ok != 0;
 }
+
+// Barrier over the whole (cooperative) grid.
+__device__ __forceinline__ bool grid_sync(GridBarrier *bar) { return grid_sync(bar, gridDim.x); }
 
 // Deterministic block sum of one double per thread (fixed shuffle tree).
 template <int BLOCK>

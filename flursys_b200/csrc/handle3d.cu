@@ -51,7 +51,7 @@ static int32_t init3d(FlursysCudaHandle *h) {
     }
     cudaError_t e = cudaMalloc(&h->diag3, sizeof(Diag3Dev));
     if (e == cudaSuccess) e = cudaMallocHost(&h->h_diag3, sizeof(Diag3Dev));
-    if (e == cudaSuccess) e = h->pcg.allocate(nc, c.precision, h->device, 3);
+    if (e == cudaSuccess) e = h->pcg.allocate3d((int)c.nx, (int)c.ny, (int)c.nz, c.precision, h->device, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "allocating 3D solver workspace");
     return FLURSYS_OK;
@@ -194,7 +194,8 @@ extern "C" int32_t flursys_cuda_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, 
     double *dxp = nullptr, *drhs = nullptr;
     std::string err;
     int32_t status = FLURSYS_OK;
-    cudaError_t e = ws.allocate(n, precision, device, 3);
+    if (n >= (1LL << 31)) return FLURSYS_ERR_INVALID_ARGUMENT;
+    cudaError_t e = ws.allocate3d((int)nx, (int)ny, (int)nz, precision, device, st);
     if (e == cudaSuccess) e = cudaMalloc(&dxp, sizeof(double) * n);
     if (e == cudaSuccess) e = cudaMalloc(&drhs, sizeof(double) * n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dxp, x_inout, sizeof(double) * n, cudaMemcpyHostToDevice, st);

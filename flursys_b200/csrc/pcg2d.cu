@@ -1,0 +1,458 @@
+// pcg2d.cu — persistent pressure solvers of the 2D structured solver
+// (src/solver/incompressible.rs), batched over independent instances.
+//
+// PCG follows solve_pressure_pcg (:1048-1214) with the operator of
+// apply_pressure_operator (:1216-1255): fluid rows sum over in-range,
+// non-solid neighbours; solid and pressure-outlet cells are identity rows
+// holding 0 or the outlet pressure. Without a pressure outlet the system is
+// pure Neumann and x, b, r, z and d are projected to zero mean over the fluid
+// cells as in project_zero_mean (:2338-2377). The projections are folded into
+// the passes that produce each vector:
+//   pass 1  d = (z - mean z) + beta (d_old - mean d_old) on the fly, q = A d,
+//           sums d.q, sum q, sum d      -> barrier -> mean d, d.q, alpha
+//   pass 2  x += alpha d, r -= alpha q, sums x, r       -> barrier -> means
+//   pass 3  x, r projected and stored, stop residual, z = r/diag stored,
+//           sums z, r.z, r              -> barrier -> residual, mean z, rz
+// Since A annihilates the fluid indicator, A(d - m) = A d and
+// d'.q = d.q - m sum q, so each projected quantity equals the reference's up
+// to rounding. With an outlet, passes 2 and 3 merge (two barriers).
+//
+// SOR follows solve_pressure_sor (:979-1046) with red-black ordering (not
+// iterate-identical to the reference's lexicographic sweep), the reference
+// cell shift of :1024-1035 and the stop test of pressure_residual
+// (:1532-1567).
+//
+// Every barrier wait is bounded (common.cuh); all blocks of an instance
+// reduce the same partials in the same order and leave their loops together.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "pcg2d.cuh"
+
+namespace flursys {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kParts = 8;
+
+__device__ __forceinline__ bool solid(const uint8_t *f, long long c) { return (f[c] & kCellSolid) != 0; }
+__device__ __forceinline__ bool ident(const uint8_t *f, long long c) { return (f[c] & 3) != 0; }
+
+struct Ctx {
+    Pcg2dInstance in;
+    int lb;  // block index within the instance
+    long long n, c_begin, c_end;
+};
+
+// Diagonal of a fluid row.
+__device__ __forceinline__ double diag2(const Ctx &k, long long c, int i, int j) {
+    const uint8_t *f = k.in.flags;
+    double d = 0.0;
+    if (i + 1 < k.in.nx && !solid(f, c + 1)) d += k.in.idx2;
+    if (i > 0 && !solid(f, c - 1)) d += k.in.idx2;
+    if (j + 1 < k.in.ny && !solid(f, c + k.in.nx)) d += k.in.idy2;
+    if (j > 0 && !solid(f, c - k.in.nx)) d += k.in.idy2;
+    return d;
+}
+
+// (A v)_c for a fluid row with `val(nb)` giving the operand.
+template <typename T, typename F>
+__device__ __forceinline__ T apply_row(const Ctx &k, long long c, int i, int j, T vc, F val) {
+    const uint8_t *f = k.in.flags;
+    const T wx = T(k.in.idx2), wy = T(k.in.idy2);
+    T dg = T(0), s = T(0);
+    if (i + 1 < k.in.nx && !solid(f, c + 1)) { dg += wx; s += wx * val(c + 1); }
+    if (i > 0 && !solid(f, c - 1)) { dg += wx; s += wx * val(c - 1); }
+    if (j + 1 < k.in.ny && !solid(f, c + k.in.nx)) { dg += wy; s += wy * val(c + k.in.nx); }
+    if (j > 0 && !solid(f, c - k.in.nx)) { dg += wy; s += wy * val(c - k.in.nx); }
+    return dg * vc - s;
+}
+
+__device__ __forceinline__ void write_parts(const Ctx &k, const double *v, int nv, double *red) {
+    for (int p = 0; p < nv; ++p) {
+        const double t = block_sum<kBlock>(v[p], red);
+        if (threadIdx.x == 0) k.in.partials[k.lb * kParts + p] = t;
+    }
+}
+__device__ __forceinline__ double read_sum(const Ctx &k, int p, double *red) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s += k.in.partials[b * kParts + p];
+    return block_sum<kBlock>(s, red);
+}
+__device__ __forceinline__ double read_max(const Ctx &k, int p, double *red) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s = fmax(s, k.in.partials[b * kParts + p]);
+    return block_max<kBlock>(s, red);
+}
+__device__ __forceinline__ void write_max(const Ctx &k, int p, double v, double *red) {
+    const double t = block_max<kBlock>(v, red);
+    if (threadIdx.x == 0) k.in.partials[k.lb * kParts + p] = t;
+}
+
+template <typename V, bool MIXED>
+__device__ void pcg_instance(Ctx &k, double *red) {
+    const Pcg2dInstance &in = k.in;
+    const uint8_t *f = in.flags;
+    double *x = in.x;
+    V *r = static_cast<V *>(in.r);
+    V *z = static_cast<V *>(in.z);
+    V *dbuf[2] = {static_cast<V *>(in.d0), static_cast<V *>(in.d1)};
+    V *q = static_cast<V *>(in.q);
+    const bool proj = in.project != 0;
+    const bool l2 = in.stop_rule == FLURSYS_STOP_REL_L2;
+    const double cnt = in.count_fluid > 0 ? double(in.count_fluid) : 1.0;
+    const unsigned nb = in.nblocks;
+    const int nx = in.nx;
+    auto bval = [&](long long c) -> double {  // b of the system (before projection)
+        const uint8_t fc = f[c];
+        if (fc & kCellOutlet) return in.outlet_pressure;
+        if (fc & kCellSolid) return 0.0;
+        return -__ldg(in.rhs + c);
+    };
+
+    int status = FLURSYS_LINEAR_MAX_ITERATIONS, error = 0;
+    long long iterations = 0;
+    double residual = 0.0, initial = 0.0, initial_l2 = 0.0, threshold = 0.0;
+    double mb = 0.0;  // mean of b over fluid cells (pure Neumann)
+    double rz_old = 0.0, mz = 0.0;
+
+    // ---- I1: identity rows take their fixed values; sums of x and b ----
+    {
+        double sx = 0.0, sb = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            const uint8_t fc = f[c];
+            if (fc & 3) {
+                x[c] = (fc & kCellOutlet) ? in.outlet_pressure : 0.0;
+            } else {
+                sx += x[c];
+                sb += bval(c);
+            }
+        }
+        double v[2] = {sx, sb};
+        write_parts(k, v, 2, red);
+    }
+    if (!grid_sync(in.barrier, nb)) return;
+    double mx = proj ? read_sum(k, 0, red) / cnt : 0.0;
+    mb = proj ? read_sum(k, 1, red) / cnt : 0.0;
+    if (proj) {
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
+            if (!ident(f, c)) x[c] -= mx;
+        if (!grid_sync(in.barrier, nb)) return;
+    }
+
+    // ---- r = b' - A x (FP64), projected; residual; z; r.z ----
+    auto residual_pass = [&]() -> bool {
+        double sr = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            const int j = int(c / nx), i = int(c - (long long)j * nx);
+            double rv = 0.0;
+            if (!ident(f, c)) {
+                rv = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](long long m) { return x[m]; });
+                sr += rv;
+            }
+            r[c] = V(rv);
+        }
+        double v[1] = {sr};
+        write_parts(k, v, 1, red);
+        if (!grid_sync(in.barrier, nb)) return false;
+        const double mr = proj ? read_sum(k, 0, red) / cnt : 0.0;
+        double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            const int j = int(c / nx), i = int(c - (long long)j * nx);
+            double rv = double(r[c]);
+            double zv = rv;
+            if (!ident(f, c)) {
+                if (proj) {
+                    rv = double(V(rv - mr));
+                    r[c] = V(rv);
+                }
+                const double dg = diag2(k, c, i, j);
+                zv = dg > 0.0 ? rv / dg : rv;
+                s_z += zv;
+                s_r += rv;
+            }
+            z[c] = V(zv);
+            s_rr += rv * rv;
+            s_max = fmax(s_max, fabs(rv));
+            s_rz += rv * double(V(zv));
+        }
+        double v2[4] = {s_rr, s_z, s_rz, s_r};
+        write_parts(k, v2, 4, red);
+        write_max(k, 4, s_max, red);
+        return grid_sync(in.barrier, nb);
+    };
+    auto read_residual_sums = [&](double &rr, double &rmax, double &rz) {
+        rr = read_sum(k, 0, red);
+        const double sz = read_sum(k, 1, red);
+        const double srz = read_sum(k, 2, red);
+        const double sr = read_sum(k, 3, red);
+        rmax = read_max(k, 4, red);
+        mz = proj ? sz / cnt : 0.0;
+        rz = srz - mz * sr;  // r'.(z - mean z)
+    };
+    if (!residual_pass()) return;
+    double rr, rmax;
+    read_residual_sums(rr, rmax, rz_old);
+    initial_l2 = sqrt(rr);
+    initial = l2 ? initial_l2 : rmax;
+    threshold = l2 ? in.atol + in.rtol * initial : in.tol;
+    residual = initial;
+    bool done = l2 ? (residual <= threshold) : (residual < threshold);
+    if (done) status = FLURSYS_LINEAR_CONVERGED;
+    double beta = 0.0, md_old = 0.0;
+    bool first = true;
+
+    for (long long it = 0; !done && it < in.max_iters; ++it) {
+        iterations = it + 1;
+        V *dcur = dbuf[it & 1];
+        const V *dold = dbuf[(it + 1) & 1];
+        // ---- pass 1: direction + stencil ----
+        auto dn = [&](long long m) -> V {
+            if (ident(f, m)) return V(0);
+            const double zm = double(z[m]) - mz;
+            return first ? V(zm) : V(zm + beta * (double(dold[m]) - md_old));
+        };
+        double s_dq = 0.0, s_q = 0.0, s_d = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            const int j = int(c / nx), i = int(c - (long long)j * nx);
+            const V dc = dn(c);
+            V qc = dc;
+            if (!ident(f, c)) {
+                qc = apply_row<V>(k, c, i, j, dc, dn);
+                s_q += double(qc);
+                s_d += double(dc);
+            }
+            dcur[c] = dc;
+            q[c] = qc;
+            s_dq += double(dc) * double(qc);
+        }
+        {
+            double v[3] = {s_dq, s_q, s_d};
+            write_parts(k, v, 3, red);
+        }
+        if (!grid_sync(in.barrier, nb)) return;
+        const double sdq = read_sum(k, 0, red);
+        const double md = proj ? read_sum(k, 2, red) / cnt : 0.0;
+        const double dq = proj ? sdq - md * read_sum(k, 1, red) : sdq;
+        if (fabs(dq) < 1.0e-30 || !isfinite(dq)) { error = FLURSYS_ERR_BREAKDOWN; break; }
+        const double alpha = rz_old / dq;
+        if (!isfinite(alpha)) { error = FLURSYS_ERR_BREAKDOWN; break; }
+        // ---- pass 2: updates (and their sums when projecting) ----
+        double mr = 0.0;
+        if (proj) {
+            double s_x = 0.0, s_r = 0.0;
+            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+                if (ident(f, c)) continue;
+                const double dc = double(dcur[c]) - md;
+                const double xv = x[c] + alpha * dc;
+                const V rv = V(double(r[c]) - alpha * double(q[c]));
+                x[c] = xv;
+                r[c] = rv;
+                s_x += xv;
+                s_r += double(rv);
+            }
+            double v[2] = {s_x, s_r};
+            write_parts(k, v, 2, red);
+            if (!grid_sync(in.barrier, nb)) return;
+            mx = read_sum(k, 0, red) / cnt;
+            mr = read_sum(k, 1, red) / cnt;
+        }
+        // ---- pass 3: projection, residual, z, r.z ----
+        double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            const int j = int(c / nx), i = int(c - (long long)j * nx);
+            double rv;
+            double zv;
+            if (ident(f, c)) {
+                rv = double(r[c]);
+                zv = rv;
+            } else {
+                if (proj) {
+                    x[c] -= mx;
+                    rv = double(V(double(r[c]) - mr));
+                } else {
+                    x[c] += alpha * double(dcur[c]);
+                    rv = double(V(double(r[c]) - alpha * double(q[c])));
+                }
+                r[c] = V(rv);
+                const double dg = diag2(k, c, i, j);
+                zv = dg > 0.0 ? rv / dg : rv;
+                s_z += zv;
+                s_r += rv;
+            }
+            z[c] = V(zv);
+            s_rr += rv * rv;
+            s_max = fmax(s_max, fabs(rv));
+            s_rz += rv * double(V(zv));
+        }
+        {
+            double v[4] = {s_rr, s_z, s_rz, s_r};
+            write_parts(k, v, 4, red);
+            write_max(k, 4, s_max, red);
+        }
+        if (!grid_sync(in.barrier, nb)) return;
+        double rz_new;
+        read_residual_sums(rr, rmax, rz_new);
+        residual = l2 ? sqrt(rr) : rmax;
+        if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
+        bool conv = l2 ? (residual <= threshold) : (residual < threshold);
+        if (MIXED && (conv || ((it + 1) % in.replace_every) == 0)) {
+            if (!residual_pass()) return;  // FP64 true residual replaces r
+            read_residual_sums(rr, rmax, rz_new);
+            residual = l2 ? sqrt(rr) : rmax;
+            if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
+            conv = l2 ? (residual <= threshold) : (residual < threshold);
+        }
+        if (conv) { status = FLURSYS_LINEAR_CONVERGED; break; }
+        if (fabs(rz_old) < 1.0e-30) break;
+        beta = rz_new / rz_old;
+        rz_old = rz_new;
+        md_old = md;
+        first = false;
+    }
+    // ---- final FP64 check ||b' - A x||_2 over fluid rows ----
+    if (!grid_sync(in.barrier, nb)) return;
+    double s_true = 0.0;
+    for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+        if (ident(f, c)) continue;
+        const int j = int(c / nx), i = int(c - (long long)j * nx);
+        const double t = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](long long m) { return x[m]; });
+        s_true += t * t;
+    }
+    {
+        double v[1] = {s_true};
+        write_parts(k, v, 1, red);
+    }
+    if (!grid_sync(in.barrier, nb)) return;
+    const double true_rr = read_sum(k, 0, red);
+    if (k.lb == 0 && threadIdx.x == 0) {
+        PcgResultDev *res = in.result;
+        res->error = error;
+        res->status = status;
+        res->iterations = iterations;
+        res->initial = initial;
+        res->residual = residual;
+        res->true_l2 = sqrt(true_rr);
+        res->initial_l2 = initial_l2;
+        res->device_error = in.barrier->error;
+    }
+}
+
+__device__ void sor_instance(Ctx &k, double *red) {
+    const Pcg2dInstance &in = k.in;
+    const uint8_t *f = in.flags;
+    double *p = in.x;
+    const unsigned nb = in.nblocks;
+    const int nx = in.nx;
+    double residual = INFINITY;
+    long long its = 0;
+    int error = 0;
+    for (long long it = 0; it < in.max_iters; ++it) {
+        its = it + 1;
+        for (int color = 0; color < 2; ++color) {
+            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+                const int j = int(c / nx), i = int(c - (long long)j * nx);
+                if (((i + j) & 1) != color) continue;
+                const uint8_t fc = f[c];
+                if (fc & kCellSolid) { p[c] = 0.0; continue; }
+                if (fc & kCellOutlet) { p[c] = in.outlet_pressure; continue; }
+                double ap = 0.0, s = 0.0;
+                if (i + 1 < nx && !solid(f, c + 1)) { ap += in.idx2; s += in.idx2 * p[c + 1]; }
+                if (i > 0 && !solid(f, c - 1)) { ap += in.idx2; s += in.idx2 * p[c - 1]; }
+                if (j + 1 < in.ny && !solid(f, c + nx)) { ap += in.idy2; s += in.idy2 * p[c + nx]; }
+                if (j > 0 && !solid(f, c - nx)) { ap += in.idy2; s += in.idy2 * p[c - nx]; }
+                if (ap > 0.0) {
+                    const double old = p[c];
+                    p[c] = old + in.omega * ((s - __ldg(in.rhs + c)) / ap - old);
+                }
+            }
+            if (!grid_sync(in.barrier, nb)) return;
+        }
+        if (in.project && in.ref_cell >= 0) {
+            const double pr = p[in.ref_cell];
+            if (!grid_sync(in.barrier, nb)) return;
+            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
+                if (!solid(f, c)) p[c] -= pr;
+            if (!grid_sync(in.barrier, nb)) return;
+        }
+        double m = 0.0;
+        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            if (ident(f, c)) continue;
+            const int j = int(c / nx), i = int(c - (long long)j * nx);
+            const double p0 = p[c];
+            const double pe = (i + 1 < nx && !solid(f, c + 1)) ? p[c + 1] : p0;
+            const double pw = (i > 0 && !solid(f, c - 1)) ? p[c - 1] : p0;
+            const double pn = (j + 1 < in.ny && !solid(f, c + nx)) ? p[c + nx] : p0;
+            const double ps = (j > 0 && !solid(f, c - nx)) ? p[c - nx] : p0;
+            const double lap = (pe - 2.0 * p0 + pw) * in.idx2 + (pn - 2.0 * p0 + ps) * in.idy2;
+            m = fmax(m, fabs(lap - __ldg(in.rhs + c)));
+        }
+        write_max(k, (int)(it & 1), m, red);
+        if (!grid_sync(in.barrier, nb)) return;
+        residual = read_max(k, (int)(it & 1), red);
+        if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
+        if (residual < in.tol) break;
+    }
+    if (k.lb == 0 && threadIdx.x == 0) {
+        PcgResultDev *res = in.result;
+        res->error = error;
+        res->status = residual < in.tol ? FLURSYS_LINEAR_CONVERGED : FLURSYS_LINEAR_MAX_ITERATIONS;
+        res->iterations = its;
+        res->initial = 0.0;
+        res->residual = residual;
+        res->true_l2 = 0.0;
+        res->initial_l2 = 0.0;
+        res->device_error = in.barrier->error;
+    }
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
+    __shared__ double red[kBlock / 32];
+    int id = 0;
+    for (int t = 0; t < ninst; ++t)
+        if ((int)blockIdx.x >= insts[t].block0) id = t;
+    Ctx k;
+    k.in = insts[id];
+    k.lb = (int)blockIdx.x - k.in.block0;
+    if (k.lb >= k.in.nblocks) return;  // spare block of the launch
+    k.n = (long long)k.in.nx * k.in.ny;
+    const long long chunk = (k.n + k.in.nblocks - 1) / k.in.nblocks;
+    k.c_begin = (long long)k.lb * chunk;
+    k.c_end = k.c_begin + chunk < k.n ? k.c_begin + chunk : k.n;
+    if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red);
+    else pcg_instance<V, MIXED>(k, red);
+}
+
+}  // namespace
+
+cudaError_t pcg2d_max_grid(int precision, int device, int *grid) {
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    if (precision == FLURSYS_PRECISION_MIXED)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg2d_kernel<float, true>, kBlock, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg2d_kernel<double, false>, kBlock, 0);
+    if (e != cudaSuccess) return e;
+    *grid = sms * per_sm;
+    return cudaSuccess;
+}
+
+int pcg2d_block_size() { return kBlock; }
+int pcg2d_num_partials() { return kParts; }
+
+cudaError_t pcg2d_launch(const Pcg2dInstance *inst_dev, int ninst, int total_blocks, int precision,
+                         cudaStream_t stream) {
+    void *params[] = {(void *)&inst_dev, &ninst};
+    if (precision == FLURSYS_PRECISION_MIXED)
+        return cudaLaunchCooperativeKernel((const void *)pcg2d_kernel<float, true>, dim3(total_blocks),
+                                           dim3(kBlock), params, 0, stream);
+    return cudaLaunchCooperativeKernel((const void *)pcg2d_kernel<double, false>, dim3(total_blocks), dim3(kBlock),
+                                       params, 0, stream);
+}
+
+}  // namespace flursys

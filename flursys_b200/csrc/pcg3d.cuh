@@ -19,6 +19,9 @@ struct PcgResultDev {
     double initial_l2;
     unsigned device_error;  // DeviceError bits
     unsigned pad;
+    // Nanoseconds block 0 spent in: [0] stencil passes, [1] pointwise passes,
+    // [2] grid barriers + partial reductions, [3] residual replacements.
+    unsigned long long phase_ns[4];
 };
 
 struct Pcg3dArgs {
@@ -35,9 +38,14 @@ struct Pcg3dArgs {
     double tol, atol, rtol;
     long long max_iters;
     int replace_every;
+    int precision_vec_width;  // cells per vector in the pointwise pass (4 FP32, 2 FP64)
+    const unsigned char *row_class;  // ny*nz bytes: 3*missing(j) + missing(k)
 };
 
 size_t pcg3d_vector_bytes(int precision);
+// Device table of 3*missing(j) + missing(k) for every row (j, k) of an
+// nx x ny x nz grid (missing = number of absent neighbours on that axis).
+cudaError_t pcg3d_make_row_class(int ny, int nz, unsigned char **out, cudaStream_t stream);
 cudaError_t pcg3d_max_grid(int precision, int device, int *grid);
 int pcg3d_block_size();
 int pcg3d_num_partials();

@@ -256,6 +256,12 @@ int32_t flursys_cuda_state(const FlursysCudaHandle *h, int64_t *step, double *ti
  * the reference has no device streams. */
 int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream);
 
+/* Device-time split of the last pressure solve of this handle, in ms:
+ * [0] stencil passes, [1] pointwise passes, [2] grid barriers and partial
+ * reductions, [3] FP64 residual replacements (as seen by block 0). `n` is
+ * the capacity of `phase_ms` (4 used). No reference counterpart. */
+int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms, size_t n);
+
 /* Copies the last error message (NUL-terminated, truncated to `size`). */
 int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size);
 
