@@ -110,10 +110,9 @@ int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? FLURSYS_ERR_OUT_OF_MEMORY : FLURSYS_ERR_CUDA;
 }
 
-// Enqueues one persistent 3D PCG solve of A x = -rhs on `stream`.
-int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
-                  const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
-                  long long max_iters, int replace_every, cudaStream_t stream, std::string *err) {
+Pcg3dArgs make_pcg3d_args(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                          const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
+                          long long max_iters, int replace_every) {
     Pcg3dArgs a{};
     a.nx = nx; a.ny = ny; a.nz = nz;
     a.ix2 = 1.0 / (dx * dx); a.iy2 = 1.0 / (dy * dy); a.iz2 = 1.0 / (dz * dz);
@@ -124,6 +123,15 @@ int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy
     a.max_iters = max_iters; a.replace_every = replace_every > 0 ? replace_every : 50;
     a.precision_vec_width = precision == FLURSYS_PRECISION_MIXED ? 4 : 2;
     a.row_class = ws.row_class;
+    return a;
+}
+
+// Enqueues one persistent 3D PCG solve of A x = -rhs on `stream`.
+int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                  const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
+                  long long max_iters, int replace_every, cudaStream_t stream, std::string *err) {
+    Pcg3dArgs a = make_pcg3d_args(ws, nx, ny, nz, dx, dy, dz, x, rhs, precision, stop_rule, tol, atol, rtol, max_iters,
+                                  replace_every);
     cudaError_t e = cudaMemsetAsync(ws.barrier, 0, sizeof(GridBarrier), stream);
     if (e == cudaSuccess) e = pcg3d_launch(a, ws.grid, precision, stream);
     if (e != cudaSuccess) return set_cuda_error(err, e, "pcg3d launch");

@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "flursys_cuda.h"
 #include "pcg3d.cuh"
+#include "pcg3d_seq.cuh"
 
 namespace flursys {
 
@@ -49,6 +50,9 @@ struct FlursysCudaHandle {
     flursys::Diag3Dev *diag3 = nullptr;
     flursys::Diag3Dev *h_diag3 = nullptr;
     flursys::PcgWorkspace pcg;
+    flursys::Pcg3dSeqPlan seq;   // graph-driven PCG (default 3D PCG path)
+    bool use_seq = false;
+    flursys::CgSeqState *h_seq = nullptr;  // pinned host copy of the solve state
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // 2D state
     flursys::Handle2D *h2 = nullptr;
@@ -77,5 +81,9 @@ int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy
                   long long max_iters, int replace_every, cudaStream_t stream, std::string *err);
 // Maps a finished PcgResultDev to a status and message.
 int32_t pcg_result_status(const PcgResultDev &r, std::string *err);
+// Fills the argument block of a 3D pressure solve on the workspace buffers.
+Pcg3dArgs make_pcg3d_args(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                          const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
+                          long long max_iters, int replace_every);
 
 }  // namespace flursys

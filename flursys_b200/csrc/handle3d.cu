@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "capi_internal.cuh"
@@ -54,6 +55,19 @@ static int32_t init3d(FlursysCudaHandle *h) {
     if (e == cudaSuccess) e = h->pcg.allocate3d((int)c.nx, (int)c.ny, (int)c.nz, c.precision, h->device, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "allocating 3D solver workspace");
+    // The graph-driven PCG is the default; FLURSYS_PCG_VARIANT=persistent
+    // selects the single cooperative kernel instead.
+    const char *variant = std::getenv("FLURSYS_PCG_VARIANT");
+    h->use_seq = c.pressure_solver != FLURSYS_PRESSURE_SOR && !(variant && std::strcmp(variant, "persistent") == 0);
+    if (h->use_seq) {
+        const int rule = c.stop_rule == FLURSYS_STOP_REFERENCE_RESIDUAL ? FLURSYS_STOP_ABS_INF : c.stop_rule;
+        Pcg3dArgs a = make_pcg3d_args(h->pcg, s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.p, s.rhs, c.precision, rule,
+                                      c.pressure_tolerance, c.pressure_atol, c.pressure_rtol, c.pressure_max_iters,
+                                      c.residual_replacement_every);
+        e = pcg3d_seq_plan(h->seq, a, c.precision, h->device);
+        if (e == cudaSuccess) e = cudaMallocHost(&h->h_seq, sizeof(CgSeqState));
+        if (e != cudaSuccess) return set_cuda_error(&h->err, e, "building the pressure-solve graph");
+    }
     return FLURSYS_OK;
 }
 
@@ -83,6 +97,8 @@ void handle_free(FlursysCudaHandle *h) {
     cudaFree(h->diag3);
     if (h->h_diag3) cudaFreeHost(h->h_diag3);
     h->pcg.free_all();
+    pcg3d_seq_destroy(h->seq);
+    if (h->h_seq) cudaFreeHost(h->h_seq);
     for (auto &ev : h->ev)
         if (ev) cudaEventDestroy(ev);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -103,6 +119,9 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (sor) {
         status = run_sor3d(h->pcg, s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.p, s.rhs, c.pressure_omega,
                            c.pressure_tolerance, c.pressure_max_iters, st, &h->err);
+    } else if (h->use_seq) {
+        const cudaError_t le = pcg3d_seq_launch(h->seq, st);
+        status = le == cudaSuccess ? FLURSYS_OK : set_cuda_error(&h->err, le, "pressure-solve graph");
     } else {
         const int rule = c.stop_rule == FLURSYS_STOP_REFERENCE_RESIDUAL ? FLURSYS_STOP_ABS_INF : c.stop_rule;
         status = run_pcg3d(h->pcg, s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.p, s.rhs, c.precision, rule,
@@ -114,10 +133,27 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (e == cudaSuccess) e = cavity3d_correct(s, dt, st);
     if (e == cudaSuccess) e = cavity3d_diagnostics(s, h->diag3, st);
     if (e == cudaSuccess) e = cudaEventRecord(h->ev[3], st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h->pcg.h_result, h->pcg.result, sizeof(PcgResultDev), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) {
+        if (h->use_seq && !sor)
+            e = cudaMemcpyAsync(h->h_seq, h->seq.state, sizeof(CgSeqState), cudaMemcpyDeviceToHost, st);
+        else
+            e = cudaMemcpyAsync(h->pcg.h_result, h->pcg.result, sizeof(PcgResultDev), cudaMemcpyDeviceToHost, st);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h->h_diag3, h->diag3, sizeof(Diag3Dev), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "3D step");
+    if (h->use_seq && !sor) {
+        const CgSeqState &q = *h->h_seq;
+        PcgResultDev &m = *h->pcg.h_result;  // the shared result record
+        m.error = q.error;
+        m.status = q.status;
+        m.iterations = q.iterations;
+        m.initial = q.initial;
+        m.residual = q.residual;
+        m.true_l2 = q.true_l2;
+        m.initial_l2 = q.initial_l2;
+        m.device_error = 0;
+    }
     const PcgResultDev &r = *h->pcg.h_result;
     status = pcg_result_status(r, &h->err);
     if (status) return status;

@@ -108,7 +108,7 @@ __device__ __forceinline__ unsigned fast_div(const FastDiv &f, unsigned n) {
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     __shared__ SmemBase sb;
-    __shared__ double tile[(TY + 2) * (TX + 2)];  // one plane with halo (FP64 or FP32 view)
+    __shared__ double tile[(4 * TY + 2) * (TX + 2)];  // one plane with halo (FP64 or FP32 view)
     const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
     double *x = a.x;
     const double *__restrict__ rhs = a.rhs;
@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
                                                        : reinterpret_cast<const V *>(sb.inv_diag);
 
     // ------------------------------------------------------------------
-    // 2.5D stencil sweep over the block's tiles. For a cell index c:
+    // 2.5D stencil sweep over the block's tiles. A tile is TX columns by
+    // TY*RY rows (each thread owns RY rows) by a chunk of planes. For a cell c:
     //   load(c)              issues the loads of the operand's raw inputs,
     //   make(raw, cls, pin)  forms the operand value (0 at the pinned cell),
     //   emit(c, cls, pin, v, Av) consumes (A v)_c (Av = v at the pinned cell).
@@ -143,47 +144,63 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     // ahead for the column and for the x/y halo, so the loads of a plane are
     // in flight while the two planes before it are computed.
     // ------------------------------------------------------------------
-    auto stencil_pass = [&](auto load, auto make, auto emit) {
+    auto stencil_pass = [&](auto ry_tag, auto load, auto make, auto emit) {
+        constexpr int RY = decltype(ry_tag)::value;
+        constexpr int TYR = TY * RY;
+        constexpr int SW = TX + 2;
         using Raw = decltype(load(0));
         using T = decltype(make(load(0), 0, false));
         const T wx = T(g.ix2), wy = T(g.iy2), wz = T(g.iz2);
         const int nxy = g.nx * g.ny;
-        const int ntiles = g.tiles_x * g.tiles_y * g.chunks;
+        const int tiles_y = (g.ny + TYR - 1) / TYR;
+        const int ntiles = g.tiles_x * tiles_y * g.chunks;
         T *ts = reinterpret_cast<T *>(tile);
-        const int sp = (ty + 1) * (TX + 2) + tx + 1;
         const int h = threadIdx.x;
-        const bool halo_thread = h < 2 * TX + 2 * TY;
+        const bool halo_thread = h < 2 * TX + 2 * TYR;
         for (int t = blockIdx.x; t < ntiles; t += nblk) {
             const int ch = t % g.chunks, col = t / g.chunks;
-            const int i0 = (col % g.tiles_x) * TX, j0 = (col / g.tiles_x) * TY;
+            const int i0 = (col % g.tiles_x) * TX, j0 = (col / g.tiles_x) * TYR;
             const int k0 = ch * g.kc, k1 = min(g.nz, k0 + g.kc);
-            const int kmax = min(k1, g.nz - 1);  // last plane the column reads
-            const int i = i0 + tx, j = j0 + ty;
-            const bool in = i < g.nx && j < g.ny;
-            const int base = in ? j * g.nx + i : 0;
-            const int cxy = 9 * miss(i, g.nx) + 3 * miss(j, g.ny);
-            const T wxm = (in && i > 0) ? wx : T(0), wxp = (in && i + 1 < g.nx) ? wx : T(0);
-            const T wym = (in && j > 0) ? wy : T(0), wyp = (in && j + 1 < g.ny) ? wy : T(0);
-            const T dgxy = wxm + wxp + wym + wyp;
-            const bool pcol = in && i == 0 && j == 0;
+            const int kmax = min(k1, g.nz - 1);  // last plane the columns read
+            const int i = i0 + tx;
+            const bool inx = i < g.nx;
+            const T wxm = (inx && i > 0) ? wx : T(0), wxp = (inx && i + 1 < g.nx) ? wx : T(0);
+            const int cx = 9 * miss(i, g.nx);
+            int base[RY];
+            bool in[RY];
+#pragma unroll
+            for (int m = 0; m < RY; ++m) {
+                const int j = j0 + ty + m * TY;
+                in[m] = inx && j < g.ny;
+                base[m] = in[m] ? j * g.nx + i : 0;
+            }
             int hi = 0, hj = 0;
             if (h < TX) { hi = i0 + h; hj = j0 - 1; }
-            else if (h < 2 * TX) { hi = i0 + h - TX; hj = j0 + TY; }
-            else if (h < 2 * TX + TY) { hi = i0 - 1; hj = j0 + h - 2 * TX; }
-            else { hi = i0 + TX; hj = j0 + h - 2 * TX - TY; }
+            else if (h < 2 * TX) { hi = i0 + h - TX; hj = j0 + TYR; }
+            else if (h < 2 * TX + TYR) { hi = i0 - 1; hj = j0 + h - 2 * TX; }
+            else { hi = i0 + TX; hj = j0 + h - 2 * TX - TYR; }
             const bool hv = halo_thread && hi >= 0 && hi < g.nx && hj >= 0 && hj < g.ny;
             const int hbase = hv ? hj * g.nx + hi : 0;
             const int hcls = hv ? 9 * miss(hi, g.nx) + 3 * miss(hj, g.ny) : 0;
-            const int hslot = halo_thread ? (hj - j0 + 1) * (TX + 2) + (hi - i0 + 1) : 0;
+            const int hslot = halo_thread ? (hj - j0 + 1) * SW + (hi - i0 + 1) : 0;
             const bool hpcol = hv && hi == 0 && hj == 0;
             // prologue: below, cur, and two planes of lookahead
-            T below = T(0), cur = T(0);
-            Raw a1{}, a2{}, h1{}, h2{};
-            if (in) {
-                if (k0 > 0) below = make(load(base + (k0 - 1) * nxy), cxy + miss(k0 - 1, g.nz), false);
-                cur = make(load(base + k0 * nxy), cxy + miss(k0, g.nz), pcol && k0 == 0);
-                if (k0 + 1 <= kmax) a1 = load(base + (k0 + 1) * nxy);
-                if (k0 + 2 <= kmax) a2 = load(base + (k0 + 2) * nxy);
+            T below[RY], cur[RY];
+            Raw a1[RY], a2[RY], h1{}, h2{};
+#pragma unroll
+            for (int m = 0; m < RY; ++m) {
+                below[m] = T(0);
+                cur[m] = T(0);
+                a1[m] = Raw{};
+                a2[m] = Raw{};
+                if (in[m]) {
+                    const int cxy = cx + 3 * miss(j0 + ty + m * TY, g.ny);
+                    const bool pc = base[m] == 0;
+                    if (k0 > 0) below[m] = make(load(base[m] + (k0 - 1) * nxy), cxy + miss(k0 - 1, g.nz), false);
+                    cur[m] = make(load(base[m] + k0 * nxy), cxy + miss(k0, g.nz), pc && k0 == 0);
+                    if (k0 + 1 <= kmax) a1[m] = load(base[m] + (k0 + 1) * nxy);
+                    if (k0 + 2 <= kmax) a2[m] = load(base[m] + (k0 + 2) * nxy);
+                }
             }
             if (hv) {
                 h1 = load(hbase + k0 * nxy);
@@ -191,11 +208,16 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
             }
             for (int k = k0; k < k1; ++k) {
                 const int mk = miss(k, g.nz);
-                T above = T(0);
-                if (in) {
-                    if (k + 1 < g.nz) above = make(a1, cxy + miss(k + 1, g.nz), false);
-                    a1 = a2;
-                    if (k + 3 <= kmax) a2 = load(base + (k + 3) * nxy);
+                T above[RY];
+#pragma unroll
+                for (int m = 0; m < RY; ++m) {
+                    above[m] = T(0);
+                    if (in[m]) {
+                        if (k + 1 < g.nz)
+                            above[m] = make(a1[m], cx + 3 * miss(j0 + ty + m * TY, g.ny) + miss(k + 1, g.nz), false);
+                        a1[m] = a2[m];
+                        if (k + 3 <= kmax) a2[m] = load(base[m] + (k + 3) * nxy);
+                    }
                 }
                 T hval = T(0);
                 if (hv) {
@@ -203,23 +225,36 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
                     h1 = h2;
                     if (k + 2 < k1) h2 = load(hbase + (k + 2) * nxy);
                 }
-                ts[sp] = cur;
+#pragma unroll
+                for (int m = 0; m < RY; ++m) ts[(ty + m * TY + 1) * SW + tx + 1] = cur[m];
                 if (halo_thread) ts[hslot] = hval;
                 __syncthreads();
-                if (in) {
-                    const T wzm = k > 0 ? wz : T(0), wzp = k + 1 < g.nz ? wz : T(0);
-                    const T ax = (dgxy + wzm + wzp) * cur -
-                                 (wxm * ts[sp - 1] + wxp * ts[sp + 1] + wym * ts[sp - (TX + 2)] +
-                                  wyp * ts[sp + (TX + 2)] + wzm * below + wzp * above);
-                    const bool pin = pcol && k == 0;
-                    emit(base + k * nxy, cxy + mk, pin, cur, pin ? cur : ax);
+                const T wzm = k > 0 ? wz : T(0), wzp = k + 1 < g.nz ? wz : T(0);
+#pragma unroll
+                for (int m = 0; m < RY; ++m) {
+                    if (in[m]) {
+                        const int j = j0 + ty + m * TY;
+                        const T wym = j > 0 ? wy : T(0), wyp = j + 1 < g.ny ? wy : T(0);
+                        const int sp = (ty + m * TY + 1) * SW + tx + 1;
+                        const T ax = (wxm + wxp + wym + wyp + wzm + wzp) * cur[m] -
+                                     (wxm * ts[sp - 1] + wxp * ts[sp + 1] + wym * ts[sp - SW] + wyp * ts[sp + SW] +
+                                      wzm * below[m] + wzp * above[m]);
+                        const bool pin = base[m] == 0 && k == 0;
+                        emit(base[m] + k * nxy, cx + 3 * miss(j, g.ny) + mk, pin, cur[m], pin ? cur[m] : ax);
+                    }
                 }
                 __syncthreads();
-                below = cur;
-                cur = above;
+#pragma unroll
+                for (int m = 0; m < RY; ++m) {
+                    below[m] = cur[m];
+                    cur[m] = above[m];
+                }
             }
         }
     };
+    constexpr int kRyA = 1;  // rows per thread, operand passes
+    using RyA = std::integral_constant<int, kRyA>;
+    using RyX = std::integral_constant<int, 1>;  // FP64 residual passes
 
     const long long tid0 = (long long)blockIdx.x * kBlock + threadIdx.x;
     const long long stride = (long long)nblk * kBlock;
@@ -256,7 +291,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     auto make_x = [&](double v, int, bool pin) -> double { return pin ? 0.0 : v; };
     auto residual_pass = [&](bool zero_dx) {
         double srr = 0.0, srz = 0.0, smax = 0.0;
-        stencil_pass(load_x, make_x, [&](int c, int cls, bool pin, double, double ax) {
+        stencil_pass(RyX{}, load_x, make_x, [&](int c, int cls, bool pin, double, double ax) {
             const double rr = pin ? 0.0 : -__ldg(rhs + c) - ax;
             const V rv = V(rr);
             r[c] = rv;
@@ -317,7 +352,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
             const V z = v.r * inv_diag_v[cls];
             return first ? z : V(z + vbeta * v.d);
         };
-        stencil_pass(load_a, make_a, [&](int c, int, bool, V dc, V qc) {
+        stencil_pass(RyA{}, load_a, make_a, [&](int c, int, bool, V dc, V qc) {
             dcur[c] = dc;
             q[c] = qc;
             sdq += double(dc) * double(qc);
@@ -424,7 +459,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     if (!grid_sync(bar)) return;
     // ---- final FP64 check: ||b - A x||_2 of the solution in HBM ----
     double s_true = 0.0;
-    stencil_pass(load_x, make_x, [&](int c, int, bool pin, double, double ax) {
+    stencil_pass(RyX{}, load_x, make_x, [&](int c, int, bool pin, double, double ax) {
         const double t = pin ? 0.0 : -__ldg(rhs + c) - ax;
         s_true += t * t;
     });
@@ -454,8 +489,9 @@ Geo make_geo(const Pcg3dArgs &a, int grid) {
     g.nxy = (long long)a.nx * a.ny;
     g.n = g.nxy * a.nz;
     g.ix2 = a.ix2; g.iy2 = a.iy2; g.iz2 = a.iz2;
+    const int ry = 1;  // rows per thread of the operand pass
     g.tiles_x = (a.nx + TX - 1) / TX;
-    g.tiles_y = (a.ny + TY - 1) / TY;
+    g.tiles_y = (a.ny + TY * ry - 1) / (TY * ry);
     const long long cols = (long long)g.tiles_x * g.tiles_y;
     // About eight tiles per block, at least four planes per tile.
     long long want = std::max(1LL, (long long)grid * 8 / std::max(1LL, cols));

@@ -1,0 +1,622 @@
+// pcg3d_seq.cu — the 3D pressure PCG as a kernel sequence in one CUDA graph.
+//
+// Same system, iteration order, precision modes and stop semantics as the
+// persistent kernel of pcg3d.cu (see there), but each phase is its own
+// high-occupancy launch and the loop runs on the device:
+//
+//   graph:  init -> WHILE(continue) { dir_spmv -> update -> IF(replace) { fold -> replace } } -> final
+//
+//   init      r = b - A x (FP64), sums r.r, r.z, max|r|; sets `continue`
+//   dir_spmv  d = z + beta d_old formed on the fly (cells and halo), q = A d,
+//             sum d.q -> alpha
+//   update    x (or the FP32 increment) += alpha d, r -= alpha q, sums ->
+//             stop test, beta; in MIXED mode every `replace_every`
+//             iterations and before accepting convergence it raises `replace`
+//   fold      x += increment (MIXED)
+//   replace   r = b - A x in FP64 (residual replacement), sums -> stop test, beta
+//   final     FP64 ||b - A x||_2 of the returned pressure
+//
+// Reductions use the last-block pattern: every block writes one partial,
+// fences, and bumps a counter; the block that arrives last sums the partials
+// in block order (deterministic) and updates the scalar state, which later
+// launches read. Nothing spins. The stencil launches walk one tile each
+// (32 x 8 columns, a chunk of planes) with the 2.5D scheme of pcg3d.cu; the
+// hardware schedules tiles dynamically across the SMs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "common.cuh"
+#include "pcg3d.cuh"
+#include "pcg3d_seq.cuh"
+
+namespace flursys {
+
+namespace {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int kBlock = TX * TY;
+
+struct SeqGeo {
+    int nx, ny, nz, nxy, n;
+    int tiles_x, tiles_y, kc, chunks;
+    double ix2, iy2, iz2;
+    double inv_diag[27];  // 1/diag by missing-neighbour class 9*mx + 3*my + mz
+};
+
+struct SeqArgs {
+    SeqGeo g;
+    double *x;
+    const double *rhs;
+    void *r, *d0, *d1, *q;
+    float *dx;
+    double *partials;  // nblocks * 4
+    CgSeqState *st;
+    const unsigned char *row_class;
+    cudaGraphConditionalHandle h_loop, h_replace;
+    int stop_rule;
+    double tol, atol, rtol;
+    long long max_iters;
+    int replace_every;
+    int nblocks_stencil, nblocks_point;
+};
+
+__device__ __forceinline__ int miss(int i, int n) { return (i == 0) + (i == n - 1); }
+
+// Writes this block's partials; returns true in the block that arrives last.
+template <int NV>
+__device__ __forceinline__ bool reduce_arrive(const double (&v)[NV], double *partials, unsigned *counter,
+                                              double *red) {
+    __shared__ bool s_last;
+    const int nb = gridDim.x;
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) t[k] = k == 2 ? block_max<kBlock>(v[k], red) : block_sum<kBlock>(v[k], red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) partials[blockIdx.x * 4 + k] = t[k];
+        __threadfence();
+        const unsigned prev = atomicAdd(counter, 1u);
+        s_last = prev == (unsigned)nb - 1u;
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+// Fixed-order sums over all blocks' partials (slot 2 is a max).
+template <int NV>
+__device__ __forceinline__ void reduce_finish(double (&out)[NV], const double *partials, double *red) {
+    const int nb = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nb; b += kBlock) {
+            const double p = __ldcg(partials + b * 4 + k);
+            s = k == 2 ? fmax(s, p) : s + p;
+        }
+        out[k] = k == 2 ? block_max<kBlock>(s, red) : block_sum<kBlock>(s, red);
+    }
+}
+
+// One tile of the 2.5D sweep (see pcg3d.cu). Raw inputs are prefetched two
+// planes ahead for the column and the x/y halo.
+template <typename Load, typename Make, typename Emit>
+__device__ __forceinline__ void tile_sweep(const SeqGeo &g, int t, void *tile_mem, Load load, Make make, Emit emit) {
+    using Raw = decltype(load(0));
+    using T = decltype(make(load(0), 0, false));
+    constexpr int SW = TX + 2;
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const T wx = T(g.ix2), wy = T(g.iy2), wz = T(g.iz2);
+    T *ts = reinterpret_cast<T *>(tile_mem);
+    const int h = threadIdx.x;
+    const bool halo_thread = h < 2 * TX + 2 * TY;
+    const int ch = t % g.chunks, col = t / g.chunks;
+    const int i0 = (col % g.tiles_x) * TX, j0 = (col / g.tiles_x) * TY;
+    const int k0 = ch * g.kc, k1 = min(g.nz, k0 + g.kc);
+    const int kmax = min(k1, g.nz - 1);
+    const int i = i0 + tx, j = j0 + ty;
+    const bool in = i < g.nx && j < g.ny;
+    const int base = in ? j * g.nx + i : 0;
+    const int cxy = 9 * miss(i, g.nx) + 3 * miss(j, g.ny);
+    const T wxm = (in && i > 0) ? wx : T(0), wxp = (in && i + 1 < g.nx) ? wx : T(0);
+    const T wym = (in && j > 0) ? wy : T(0), wyp = (in && j + 1 < g.ny) ? wy : T(0);
+    const T dgxy = wxm + wxp + wym + wyp;
+    const bool pcol = in && base == 0;
+    int hi = 0, hj = 0;
+    if (h < TX) { hi = i0 + h; hj = j0 - 1; }
+    else if (h < 2 * TX) { hi = i0 + h - TX; hj = j0 + TY; }
+    else if (h < 2 * TX + TY) { hi = i0 - 1; hj = j0 + h - 2 * TX; }
+    else { hi = i0 + TX; hj = j0 + h - 2 * TX - TY; }
+    const bool hv = halo_thread && hi >= 0 && hi < g.nx && hj >= 0 && hj < g.ny;
+    const int hbase = hv ? hj * g.nx + hi : 0;
+    const int hcls = hv ? 9 * miss(hi, g.nx) + 3 * miss(hj, g.ny) : 0;
+    const int hslot = halo_thread ? (hj - j0 + 1) * SW + (hi - i0 + 1) : 0;
+    const bool hpcol = hv && hbase == 0;
+    T below = T(0), cur = T(0);
+    Raw a1{}, a2{}, h1{}, h2{};
+    if (in) {
+        if (k0 > 0) below = make(load(base + (k0 - 1) * g.nxy), cxy + miss(k0 - 1, g.nz), false);
+        cur = make(load(base + k0 * g.nxy), cxy + miss(k0, g.nz), pcol && k0 == 0);
+        if (k0 + 1 <= kmax) a1 = load(base + (k0 + 1) * g.nxy);
+        if (k0 + 2 <= kmax) a2 = load(base + (k0 + 2) * g.nxy);
+    }
+    if (hv) {
+        h1 = load(hbase + k0 * g.nxy);
+        if (k0 + 1 < k1) h2 = load(hbase + (k0 + 1) * g.nxy);
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int mk = miss(k, g.nz);
+        T above = T(0);
+        if (in) {
+            if (k + 1 < g.nz) above = make(a1, cxy + miss(k + 1, g.nz), false);
+            a1 = a2;
+            if (k + 3 <= kmax) a2 = load(base + (k + 3) * g.nxy);
+        }
+        T hval = T(0);
+        if (hv) {
+            hval = make(h1, hcls + mk, hpcol && k == 0);
+            h1 = h2;
+            if (k + 2 < k1) h2 = load(hbase + (k + 2) * g.nxy);
+        }
+        const int sp = (ty + 1) * SW + tx + 1;
+        ts[sp] = cur;
+        if (halo_thread) ts[hslot] = hval;
+        __syncthreads();
+        if (in) {
+            const T wzm = k > 0 ? wz : T(0), wzp = k + 1 < g.nz ? wz : T(0);
+            const T ax = (dgxy + wzm + wzp) * cur -
+                         (wxm * ts[sp - 1] + wxp * ts[sp + 1] + wym * ts[sp - SW] + wyp * ts[sp + SW] +
+                          wzm * below + wzp * above);
+            const bool pin = pcol && k == 0;
+            emit(base + k * g.nxy, cxy + mk, pin, cur, pin ? cur : ax);
+        }
+        __syncthreads();
+        below = cur;
+        cur = above;
+    }
+}
+
+__device__ __forceinline__ bool stop_ok(const SeqArgs &a, double res, double thr) {
+    return a.stop_rule == FLURSYS_STOP_REL_L2 ? res <= thr : res < thr;
+}
+
+// Residual r = b - A x (FP64) over one tile with its sums; shared by init and replace.
+template <typename V, bool MIXED>
+__device__ __forceinline__ void residual_tile(const SeqArgs &a, void *tile, double &srr, double &srz, double &smax,
+                                              bool zero_dx) {
+    V *r = static_cast<V *>(a.r);
+    const SeqGeo &g = a.g;
+    tile_sweep(
+        g, blockIdx.x, tile, [&](int c) -> double { return a.x[c]; },
+        [&](double v, int, bool pin) -> double { return pin ? 0.0 : v; },
+        [&](int c, int cls, bool pin, double, double ax) {
+            const double rr = pin ? 0.0 : -__ldg(a.rhs + c) - ax;
+            const V rv = V(rr);
+            r[c] = rv;
+            if (MIXED && zero_dx) a.dx[c] = 0.f;
+            const double rd = double(rv);
+            srr += rd * rd;
+            srz += rd * rd * (pin ? 1.0 : g.inv_diag[cls]);
+            smax = fmax(smax, fabs(rd));
+        });
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) seq_init(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kBlock / 32];
+    double srr = 0.0, srz = 0.0, smax = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.x[0] = 0.0;
+    residual_tile<V, MIXED>(a, tile, srr, srz, smax, true);
+    const double v[3] = {srr, srz, smax};
+    if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
+    double o[3];
+    reduce_finish<3>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *s = a.st;
+        const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
+        s->counter = 0;
+        s->initial_l2 = sqrt(o[0]);
+        s->initial = l2 ? s->initial_l2 : o[2];
+        s->threshold = l2 ? a.atol + a.rtol * s->initial : a.tol;
+        s->residual = s->initial;
+        s->rz_old = o[1];
+        s->beta = 0.0;
+        s->first = 1;
+        s->iterations = 0;
+        s->error = 0;
+        s->replace = 0;
+        s->pending_conv = 0;
+        const bool done = stop_ok(a, s->initial, s->threshold);
+        s->status = done ? FLURSYS_LINEAR_CONVERGED : FLURSYS_LINEAR_MAX_ITERATIONS;
+        s->done = done || a.max_iters <= 0;
+        cudaGraphSetConditional(a.h_loop, s->done ? 0u : 1u);
+    }
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) seq_dir_spmv(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kBlock / 32];
+    const CgSeqState *s = a.st;
+    const double beta = s->beta;
+    const bool first = s->first != 0;
+    const int parity = (int)(s->iterations & 1);  // d buffers alternate per iteration
+    V *r = static_cast<V *>(a.r);
+    V *dcur = static_cast<V *>(parity ? a.d1 : a.d0);
+    const V *dold = static_cast<const V *>(parity ? a.d0 : a.d1);
+    V *q = static_cast<V *>(a.q);
+    const SeqGeo &g = a.g;
+    const V vbeta = V(beta);
+    struct RawA {
+        V r, d;
+    };
+    double sdq = 0.0;
+    tile_sweep(
+        g, blockIdx.x, tile, [&](int c) -> RawA { return RawA{r[c], first ? V(0) : dold[c]}; },
+        [&](RawA v, int cls, bool pin) -> V {
+            if (pin) return V(0);
+            const V z = V(double(v.r) * g.inv_diag[cls]);
+            return first ? z : V(z + vbeta * v.d);
+        },
+        [&](int c, int, bool, V dc, V qc) {
+            dcur[c] = dc;
+            q[c] = qc;
+            sdq += double(dc) * double(qc);
+        });
+    const double v[1] = {sdq};
+    if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
+    double o[1];
+    reduce_finish<1>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        const double dq = o[0];
+        if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(w->rz_old / dq)) {
+            w->error = FLURSYS_ERR_BREAKDOWN;
+            w->done = 1;
+            w->alpha = 0.0;
+        } else {
+            w->alpha = w->rz_old / dq;
+        }
+    }
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
+    __shared__ double red[kBlock / 32];
+    const CgSeqState *s = a.st;
+    const double alpha = s->alpha;
+    const bool dead = s->error != 0;
+    const int parity = (int)(s->iterations & 1);
+    V *r = static_cast<V *>(a.r);
+    const V *dcur = static_cast<const V *>(parity ? a.d1 : a.d0);
+    const V *q = static_cast<const V *>(a.q);
+    const SeqGeo &g = a.g;
+    double srr = 0.0, srz = 0.0, smax = 0.0;
+    if (!dead) {
+        using V4 = typename std::conditional<std::is_same<V, float>::value, float4, double2>::type;
+        constexpr int W = sizeof(V4) / sizeof(V);
+        const int nrow = g.nx / W;
+        const bool vec = (g.nx % W) == 0;
+        const int nv = vec ? g.ny * g.nz * nrow : 0;
+        const int stride = gridDim.x * kBlock;
+        for (int cv = blockIdx.x * kBlock + threadIdx.x; cv < nv; cv += stride) {
+            const int row = cv / nrow;
+            const int i0 = (cv - row * nrow) * W;
+            const int c0 = cv * W;
+            const int rcls = a.row_class[row];
+            const V4 d4 = reinterpret_cast<const V4 *>(dcur)[cv];
+            const V4 q4 = reinterpret_cast<const V4 *>(q)[cv];
+            V4 r4 = reinterpret_cast<const V4 *>(r)[cv];
+            const V *dv = reinterpret_cast<const V *>(&d4);
+            const V *qv = reinterpret_cast<const V *>(&q4);
+            V *rv = reinterpret_cast<V *>(&r4);
+            if (MIXED) {
+                float4 x4 = reinterpret_cast<const float4 *>(a.dx)[cv];
+                float *xv = reinterpret_cast<float *>(&x4);
+#pragma unroll
+                for (int e = 0; e < W; ++e) xv[e] = float(double(xv[e]) + alpha * double(dv[e]));
+                reinterpret_cast<float4 *>(a.dx)[cv] = x4;
+            } else {
+                double2 *xp = reinterpret_cast<double2 *>(a.x + c0);
+                double2 x2 = *xp;
+                x2.x += (c0 == 0) ? 0.0 : alpha * double(dv[0]);
+                x2.y += alpha * double(dv[1]);
+                *xp = x2;
+            }
+            const double idg_mid = g.inv_diag[rcls];
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+                rv[e] = V(double(rv[e]) - alpha * double(qv[e]));
+                const double rd = double(rv[e]);
+                const int ie = i0 + e;
+                const double idg = (ie == 0 || ie == g.nx - 1) ? g.inv_diag[9 * miss(ie, g.nx) + rcls] : idg_mid;
+                srr += rd * rd;
+                srz += rd * rd * ((c0 + e == 0) ? 1.0 : idg);
+                smax = fmax(smax, fabs(rd));
+            }
+            reinterpret_cast<V4 *>(r)[cv] = r4;
+        }
+        const int ns = vec ? 0 : g.n;
+        for (int c = blockIdx.x * kBlock + threadIdx.x; c < ns; c += stride) {
+            const int row = c / g.nx;
+            const int i = c - row * g.nx;
+            const double dcv = double(dcur[c]);
+            if (MIXED) a.dx[c] = float(double(a.dx[c]) + alpha * dcv);
+            else if (c != 0) a.x[c] += alpha * dcv;
+            const V rv = V(double(r[c]) - alpha * double(q[c]));
+            r[c] = rv;
+            const double rd = double(rv);
+            srr += rd * rd;
+            srz += rd * rd * (c == 0 ? 1.0 : g.inv_diag[9 * miss(i, g.nx) + a.row_class[row]]);
+            smax = fmax(smax, fabs(rd));
+        }
+    }
+    const double v[3] = {srr, srz, smax};
+    if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
+    double o[3];
+    reduce_finish<3>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        if (w->error) {
+            w->done = 1;
+            cudaGraphSetConditional(a.h_replace, 0u);
+            cudaGraphSetConditional(a.h_loop, 0u);
+            return;
+        }
+        w->iterations += 1;
+        const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
+        const double res = l2 ? sqrt(o[0]) : o[2];
+        w->residual = res;
+        if (!isfinite(res)) {
+            w->error = FLURSYS_ERR_NON_FINITE;
+            w->done = 1;
+            cudaGraphSetConditional(a.h_replace, 0u);
+            cudaGraphSetConditional(a.h_loop, 0u);
+            return;
+        }
+        const bool conv = stop_ok(a, res, w->threshold);
+        const bool replace = MIXED && (conv || (w->iterations % a.replace_every) == 0);
+        if (replace) {
+            w->replace = 1;
+            w->rz_new = o[1];
+            cudaGraphSetConditional(a.h_replace, 1u);
+            return;  // the replacement launch takes the decision
+        }
+        cudaGraphSetConditional(a.h_replace, 0u);
+        if (conv) {
+            w->status = FLURSYS_LINEAR_CONVERGED;
+            w->done = 1;
+        } else if (fabs(w->rz_old) < 1.0e-30 || w->iterations >= a.max_iters) {
+            w->done = 1;
+        } else {
+            w->beta = o[1] / w->rz_old;
+            w->rz_old = o[1];
+            w->first = 0;
+        }
+        cudaGraphSetConditional(a.h_loop, w->done ? 0u : 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) seq_fold(SeqArgs a) {
+    const int stride = gridDim.x * kBlock;
+    for (int c = blockIdx.x * kBlock + threadIdx.x; c < a.g.n; c += stride) {
+        if (c == 0) { a.x[0] = 0.0; continue; }
+        a.x[c] += double(a.dx[c]);
+    }
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) seq_replace(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kBlock / 32];
+    double srr = 0.0, srz = 0.0, smax = 0.0;
+    residual_tile<V, MIXED>(a, tile, srr, srz, smax, true);
+    const double v[3] = {srr, srz, smax};
+    if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
+    double o[3];
+    reduce_finish<3>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        w->replace = 0;
+        const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
+        const double res = l2 ? sqrt(o[0]) : o[2];
+        w->residual = res;
+        if (!isfinite(res)) {
+            w->error = FLURSYS_ERR_NON_FINITE;
+            w->done = 1;
+        } else if (stop_ok(a, res, w->threshold)) {
+            w->status = FLURSYS_LINEAR_CONVERGED;
+            w->done = 1;
+        } else if (fabs(w->rz_old) < 1.0e-30 || w->iterations >= a.max_iters) {
+            w->done = 1;
+        } else {
+            w->beta = o[1] / w->rz_old;
+            w->rz_old = o[1];
+            w->first = 0;
+        }
+        cudaGraphSetConditional(a.h_loop, w->done ? 0u : 1u);
+    }
+}
+
+// Folds a pending increment (MIXED, not converged), then ||b - A x||_2.
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock) seq_final(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kBlock / 32];
+    double s_true = 0.0;
+    tile_sweep(
+        a.g, blockIdx.x, tile, [&](int c) -> double { return a.x[c]; },
+        [&](double v, int, bool pin) -> double { return pin ? 0.0 : v; },
+        [&](int c, int, bool pin, double, double ax) {
+            const double t = pin ? 0.0 : -__ldg(a.rhs + c) - ax;
+            s_true += t * t;
+        });
+    const double v[1] = {s_true};
+    if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
+    double o[1];
+    reduce_finish<1>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        a.st->counter = 0;
+        a.st->true_l2 = sqrt(o[0]);
+    }
+}
+
+// MIXED: fold the increment left over when the loop stops without a final
+// replacement (iteration limit or breakdown).
+__global__ void __launch_bounds__(kBlock) seq_fold_pending(SeqArgs a) {
+    const CgSeqState *s = a.st;
+    if (s->status == FLURSYS_LINEAR_CONVERGED) return;
+    const int stride = gridDim.x * kBlock;
+    for (int c = blockIdx.x * kBlock + threadIdx.x; c < a.g.n; c += stride) {
+        if (c == 0) { a.x[0] = 0.0; continue; }
+        a.x[c] += double(a.dx[c]);
+        a.dx[c] = 0.f;
+    }
+}
+
+cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t ndeps,
+                       const void *fn, int grid, void **args) {
+    cudaKernelNodeParams p{};
+    p.func = const_cast<void *>(fn);
+    p.gridDim = dim3(grid);
+    p.blockDim = dim3(kBlock);
+    p.sharedMemBytes = 0;
+    p.kernelParams = args;
+    p.extra = nullptr;
+    return cudaGraphAddKernelNode(node, g, deps, ndeps, &p);
+}
+
+template <typename V, bool MIXED>
+cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    plan.graph = g;
+    cudaGraphConditionalHandle hl;
+    e = cudaGraphConditionalHandleCreate(&hl, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    a.h_loop = hl;
+    // WHILE node first, so that the IF handle of its body exists before any
+    // kernel node copies the argument block.
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hl;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t n_while;
+    e = cudaGraphAddNode(&n_while, g, nullptr, 0, &wp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle hr;
+    e = cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    a.h_replace = hr;
+    void *args[] = {&a};
+    cudaGraphNode_t n_init, n_dir, n_upd, n_if, n_final;
+    e = add_kernel(g, &n_init, nullptr, 0, (const void *)seq_init<V, MIXED>, a.nblocks_stencil, args);
+    if (e == cudaSuccess) e = cudaGraphAddDependencies(g, &n_init, &n_while, 1);
+    if (e == cudaSuccess)
+        e = add_kernel(body, &n_dir, nullptr, 0, (const void *)seq_dir_spmv<V, MIXED>, a.nblocks_stencil, args);
+    if (e == cudaSuccess)
+        e = add_kernel(body, &n_upd, &n_dir, 1, (const void *)seq_update<V, MIXED>, a.nblocks_point, args);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams ip{};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hr;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    e = cudaGraphAddNode(&n_if, body, &n_upd, 1, &ip);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    if (MIXED) {
+        cudaGraphNode_t n_fold, n_rep;
+        e = add_kernel(rb, &n_fold, nullptr, 0, (const void *)seq_fold, a.nblocks_point, args);
+        if (e == cudaSuccess)
+            e = add_kernel(rb, &n_rep, &n_fold, 1, (const void *)seq_replace<V, MIXED>, a.nblocks_stencil, args);
+    } else {
+        cudaGraphNode_t n_empty;
+        e = cudaGraphAddEmptyNode(&n_empty, rb, nullptr, 0);
+    }
+    if (e != cudaSuccess) return e;
+    cudaGraphNode_t after = n_while;
+    if (MIXED) {
+        cudaGraphNode_t n_pend;
+        e = add_kernel(g, &n_pend, &n_while, 1, (const void *)seq_fold_pending, a.nblocks_point, args);
+        if (e != cudaSuccess) return e;
+        after = n_pend;
+    }
+    e = add_kernel(g, &n_final, &after, 1, (const void *)seq_final<V, MIXED>, a.nblocks_stencil, args);
+    if (e != cudaSuccess) return e;
+    return cudaGraphInstantiate(&plan.exec, g, 0);
+}
+
+}  // namespace
+
+cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precision, int device) {
+    pcg3d_seq_destroy(plan);
+    SeqArgs a{};
+    SeqGeo &g = a.g;
+    g.nx = args.nx; g.ny = args.ny; g.nz = args.nz;
+    g.nxy = args.nx * args.ny;
+    g.n = g.nxy * args.nz;
+    g.ix2 = args.ix2; g.iy2 = args.iy2; g.iz2 = args.iz2;
+    for (int t = 0; t < 27; ++t) {
+        const int mx = t / 9, my = (t / 3) % 3, mz = t % 3;
+        const double dg = (2 - mx) * g.ix2 + (2 - my) * g.iy2 + (2 - mz) * g.iz2;
+        g.inv_diag[t] = dg > 0.0 ? 1.0 / dg : 0.0;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    g.tiles_x = (g.nx + TX - 1) / TX;
+    g.tiles_y = (g.ny + TY - 1) / TY;
+    const long long cols = (long long)g.tiles_x * g.tiles_y;
+    // enough tiles for about eight waves of four blocks per SM, at least four planes each
+    const long long want_tiles = (long long)sms * 4 * 8;
+    long long chunks = std::max(1LL, std::min<long long>(g.nz, (want_tiles + cols - 1) / cols));
+    int kc = (int)std::max(4LL, (g.nz + chunks - 1) / chunks);
+    kc = std::min(kc, g.nz);
+    g.kc = kc;
+    g.chunks = (g.nz + kc - 1) / kc;
+    a.nblocks_stencil = g.tiles_x * g.tiles_y * g.chunks;
+    a.nblocks_point = std::max(1, std::min(sms * 8, (g.n / 4 + kBlock - 1) / kBlock));
+    a.x = args.x;
+    a.rhs = args.rhs;
+    a.r = args.r; a.d0 = args.d0; a.d1 = args.d1; a.q = args.q; a.dx = args.dx;
+    a.row_class = args.row_class;
+    a.stop_rule = args.stop_rule;
+    a.tol = args.tol; a.atol = args.atol; a.rtol = args.rtol;
+    a.max_iters = args.max_iters;
+    a.replace_every = args.replace_every > 0 ? args.replace_every : 50;
+    const int nb = std::max(a.nblocks_stencil, a.nblocks_point);
+    cudaError_t e = cudaMalloc(&plan.partials, sizeof(double) * 4 * nb);
+    if (e == cudaSuccess) e = cudaMalloc(&plan.state, sizeof(CgSeqState));
+    if (e == cudaSuccess) e = cudaMemset(plan.state, 0, sizeof(CgSeqState));
+    if (e != cudaSuccess) return e;
+    a.partials = plan.partials;
+    a.st = plan.state;
+    plan.precision = precision;
+    e = precision == FLURSYS_PRECISION_MIXED ? build<float, true>(plan, a) : build<double, false>(plan, a);
+    return e;
+}
+
+cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream) {
+    return cudaGraphLaunch(plan.exec, stream);
+}
+
+void pcg3d_seq_destroy(Pcg3dSeqPlan &plan) {
+    if (plan.exec) cudaGraphExecDestroy(plan.exec);
+    if (plan.graph) cudaGraphDestroy(plan.graph);
+    cudaFree(plan.partials);
+    cudaFree(plan.state);
+    plan = Pcg3dSeqPlan{};
+}
+
+}  // namespace flursys

@@ -1,0 +1,34 @@
+// pcg3d_seq.cuh — host interface of the graph-driven 3D pressure PCG.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pcg3d.cuh"
+
+namespace flursys {
+
+// Scalar state of one solve, read and written by the kernels of the graph.
+struct CgSeqState {
+    double rz_old, rz_new, alpha, beta;
+    double residual, initial, initial_l2, threshold, true_l2;
+    long long iterations;
+    int first, done, status, error, replace, pending_conv;
+    unsigned counter;  // last-block arrival counter
+    unsigned pad;
+};
+
+struct Pcg3dSeqPlan {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double *partials = nullptr;
+    CgSeqState *state = nullptr;
+    int precision = 0;
+};
+
+// Builds and instantiates the solve graph for fixed buffers (args as for
+// pcg3d_launch, barrier/result/partials unused).
+cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precision, int device);
+cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream);
+void pcg3d_seq_destroy(Pcg3dSeqPlan &plan);
+
+}  // namespace flursys

