@@ -26,6 +26,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <type_traits>
 
 #include "common.cuh"
@@ -42,7 +44,9 @@ constexpr int kBlock = TX * TY;
 
 struct SeqGeo {
     int nx, ny, nz, nxy, n;
-    int tiles_x, tiles_y, kc, chunks;
+    int tiles_x, tiles_y, kc, chunks;  // tile / direct sweeps: 32 x 8 columns
+    int tiles_yw, kcw, chunksw;        // warp sweep: 32 x (8 * kRyOperand) columns
+    int tiles_xv, tiles_yv, kcv, chunksv;  // vector sweep: (32 W) x (8 kRyVec) columns
     double ix2, iy2, iz2;
     double inv_diag[27];  // 1/diag by missing-neighbour class 9*mx + 3*my + mz
 };
@@ -62,7 +66,18 @@ struct SeqArgs {
     long long max_iters;
     int replace_every;
     int nblocks_stencil, nblocks_point;
+    int graph;   // 1: kernels run inside the solve graph and set its conditionals
+    int sweep;   // stencil scheme of the operand pass (kSweep*)
+    int nblocks_dir;  // grid of the operand pass
 };
+
+enum SweepKind : int { kSweepWarp = 0, kSweepTile = 1, kSweepDirect = 2, kSweepVec = 3 };
+constexpr int kRyVec = 2;  // rows per lane of the vectorised operand pass
+constexpr int kRyOperand = 4;  // rows per lane of the warp sweep (FP32; half of it in FP64)
+
+__device__ __forceinline__ void set_cond(const SeqArgs &a, cudaGraphConditionalHandle h, unsigned v) {
+    if (a.graph) cudaGraphSetConditional(h, v);
+}
 
 __device__ __forceinline__ int miss(int i, int n) { return (i == 0) + (i == n - 1); }
 
@@ -180,6 +195,161 @@ __device__ __forceinline__ void tile_sweep(const SeqGeo &g, int t, void *tile_me
     }
 }
 
+// Alternative sweep without shared memory: each thread marches its column
+// through the chunk with the planes below/above in registers and reads its
+// four in-plane neighbours' raw inputs directly (L1-cached), forming their
+// operand values itself. No block barrier.
+template <typename Load, typename Make, typename Emit>
+__device__ __forceinline__ void direct_sweep(const SeqGeo &g, int t, Load load, Make make, Emit emit) {
+    using Raw = decltype(load(0));
+    using T = decltype(make(load(0), 0, false));
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const T wx = T(g.ix2), wy = T(g.iy2), wz = T(g.iz2);
+    const int ch = t % g.chunks, col = t / g.chunks;
+    const int i0 = (col % g.tiles_x) * TX, j0 = (col / g.tiles_x) * TY;
+    const int k0 = ch * g.kc, k1 = min(g.nz, k0 + g.kc);
+    const int kmax = min(k1, g.nz - 1);
+    const int i = i0 + tx, j = j0 + ty;
+    if (i >= g.nx || j >= g.ny) return;
+    const int base = j * g.nx + i;
+    const int mi = miss(i, g.nx), mj = miss(j, g.ny);
+    const int cxy = 9 * mi + 3 * mj;
+    const bool hw = i > 0, he = i + 1 < g.nx, hs = j > 0, hn = j + 1 < g.ny;
+    const T wxm = hw ? wx : T(0), wxp = he ? wx : T(0), wym = hs ? wy : T(0), wyp = hn ? wy : T(0);
+    // classes of the in-plane neighbours (their own missing counts)
+    const int cw = 9 * miss(i - 1, g.nx) + 3 * mj, ce = 9 * miss(i + 1, g.nx) + 3 * mj;
+    const int cs = 9 * mi + 3 * miss(j - 1, g.ny), cn = 9 * mi + 3 * miss(j + 1, g.ny);
+    const bool pcol = base == 0;
+    T below = T(0), cur = T(0);
+    Raw a1{}, a2{};
+    if (k0 > 0) below = make(load(base + (k0 - 1) * g.nxy), cxy + miss(k0 - 1, g.nz), false);
+    cur = make(load(base + k0 * g.nxy), cxy + miss(k0, g.nz), pcol && k0 == 0);
+    if (k0 + 1 <= kmax) a1 = load(base + (k0 + 1) * g.nxy);
+    if (k0 + 2 <= kmax) a2 = load(base + (k0 + 2) * g.nxy);
+    for (int k = k0; k < k1; ++k) {
+        const int mk = miss(k, g.nz);
+        const int c = base + k * g.nxy;
+        const Raw rw = hw ? load(c - 1) : Raw{}, re = he ? load(c + 1) : Raw{};
+        const Raw rs = hs ? load(c - g.nx) : Raw{}, rn = hn ? load(c + g.nx) : Raw{};
+        T above = T(0);
+        if (k + 1 < g.nz) above = make(a1, cxy + miss(k + 1, g.nz), false);
+        a1 = a2;
+        if (k + 3 <= kmax) a2 = load(base + (k + 3) * g.nxy);
+        const bool k0p = k == 0;
+        const T vw = hw ? make(rw, cw + mk, k0p && c - 1 == 0) : T(0);
+        const T ve = he ? make(re, ce + mk, false) : T(0);
+        const T vs = hs ? make(rs, cs + mk, k0p && c - g.nx == 0) : T(0);
+        const T vn = hn ? make(rn, cn + mk, false) : T(0);
+        const T wzm = k > 0 ? wz : T(0), wzp = k + 1 < g.nz ? wz : T(0);
+        const T ax = (wxm + wxp + wym + wyp + wzm + wzp) * cur -
+                     (wxm * vw + wxp * ve + wym * vs + wyp * vn + wzm * below + wzp * above);
+        const bool pin = pcol && k0p;
+        emit(c, cxy + mk, pin, cur, pin ? cur : ax);
+        below = cur;
+        cur = above;
+    }
+}
+
+// Barrier-free sweep: warp w of the block owns rows [jw, jw + RY) of a
+// 32-column tile; lane l owns column i0 + l of those rows and marches them
+// through the chunk of planes. In-plane neighbours come from the lane's own
+// rows (y), from two halo rows it loads itself (y), and from the adjacent
+// lanes by shuffle (x; lanes 0 and 31 load the tile's x halo). The planes
+// below and above stay in registers; raw inputs are prefetched two planes
+// ahead. A block covers 32 x (8 RY) columns.
+template <int RY, typename Load, typename Make, typename Emit>
+__device__ __forceinline__ void warp_sweep(const SeqGeo &g, int t, Load load, Make make, Emit emit) {
+    using Raw = decltype(load(0));
+    using T = decltype(make(load(0), 0, false));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const T wx = T(g.ix2), wy = T(g.iy2), wz = T(g.iz2);
+    const int ch = t % g.chunksw, col = t / g.chunksw;
+    const int i0 = (col % g.tiles_x) * TX;
+    const int jw = (col / g.tiles_x) * (TY * RY) + w * RY;
+    if (jw >= g.ny) return;  // whole warp idle (uniform)
+    const int k0 = ch * g.kcw, k1 = min(g.nz, k0 + g.kcw);
+    const int kmax = min(k1, g.nz - 1);
+    const int i = i0 + lane;
+    const bool inx = i < g.nx;
+    const int ic = inx ? i : g.nx - 1;  // clamped column for address math of idle lanes
+    const int mi = miss(ic, g.nx);
+    const T wxm = (inx && i > 0) ? wx : T(0), wxp = (inx && i + 1 < g.nx) ? wx : T(0);
+    // rows of this warp: jw .. jw + RY - 1 (row m valid if jw + m < ny)
+    // halo loads: lane 0 the west column, lane 31 the east column (own rows)
+    const bool xw = lane == 0 && i0 > 0, xe = lane == 31 && i0 + TX < g.nx;
+    const int xcol = xw ? i0 - 1 : (xe ? i0 + TX : ic);
+    const int mxc = miss(xcol, g.nx);
+    const bool ys = jw > 0, yn = jw + RY < g.ny;  // south / north halo rows exist
+    T below[RY], cur[RY];
+    Raw a1[RY], a2[RY];
+    auto rowok = [&](int m) { return jw + m < g.ny; };
+    auto cell = [&](int col_i, int row, int k) { return (k * g.ny + row) * g.nx + col_i; };
+#pragma unroll
+    for (int m = 0; m < RY; ++m) {
+        below[m] = T(0);
+        cur[m] = T(0);
+        a1[m] = Raw{};
+        a2[m] = Raw{};
+        if (rowok(m)) {
+            const int row = jw + m, cls = 9 * mi + 3 * miss(row, g.ny);
+            if (k0 > 0) below[m] = make(load(cell(ic, row, k0 - 1)), cls + miss(k0 - 1, g.nz), false);
+            cur[m] = make(load(cell(ic, row, k0)), cls + miss(k0, g.nz), cell(ic, row, k0) == 0);
+            if (k0 + 1 <= kmax) a1[m] = load(cell(ic, row, k0 + 1));
+            if (k0 + 2 <= kmax) a2[m] = load(cell(ic, row, k0 + 2));
+        }
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int mk = miss(k, g.nz);
+        // in-plane halo raw inputs of plane k (L1/L2 hits: neighbours' data)
+        const Raw rs = ys ? load(cell(ic, jw - 1, k)) : Raw{};
+        const Raw rn = yn ? load(cell(ic, jw + RY, k)) : Raw{};
+        Raw rx[RY];
+#pragma unroll
+        for (int m = 0; m < RY; ++m) rx[m] = ((xw || xe) && rowok(m)) ? load(cell(xcol, jw + m, k)) : Raw{};
+        T above[RY];
+#pragma unroll
+        for (int m = 0; m < RY; ++m) {
+            above[m] = T(0);
+            if (rowok(m)) {
+                if (k + 1 < g.nz) above[m] = make(a1[m], 9 * mi + 3 * miss(jw + m, g.ny) + miss(k + 1, g.nz), false);
+                a1[m] = a2[m];
+                if (k + 3 <= kmax) a2[m] = load(cell(ic, jw + m, k + 3));
+            }
+        }
+        const T vs = ys ? make(rs, 9 * mi + 3 * miss(jw - 1, g.ny) + mk, cell(ic, jw - 1, k) == 0) : T(0);
+        const T vn = yn ? make(rn, 9 * mi + 3 * miss(jw + RY, g.ny) + mk, false) : T(0);
+        const T wzm = k > 0 ? wz : T(0), wzp = k + 1 < g.nz ? wz : T(0);
+#pragma unroll
+        for (int m = 0; m < RY; ++m) {
+            // x neighbours by shuffle; the tile edges take the loaded halo
+            const T xh = ((xw || xe) && rowok(m)) ? make(rx[m], 9 * mxc + 3 * miss(jw + m, g.ny) + mk,
+                                                          cell(xcol, jw + m, k) == 0)
+                                                   : T(0);
+            T west = __shfl_up_sync(0xffffffffu, cur[m], 1);
+            T east = __shfl_down_sync(0xffffffffu, cur[m], 1);
+            if (lane == 0) west = xh;
+            if (lane == 31) east = xh;
+            const int row = jw + m;
+            if (inx && rowok(m)) {
+                const T south = m > 0 ? cur[m > 0 ? m - 1 : 0] : vs;
+                const T north = m + 1 < RY ? cur[m + 1 < RY ? m + 1 : 0] : vn;
+                const T wym = row > 0 ? wy : T(0), wyp = row + 1 < g.ny ? wy : T(0);
+                const T ax = (wxm + wxp + wym + wyp + wzm + wzp) * cur[m] -
+                             (wxm * west + wxp * east + wym * south + wyp * north + wzm * below[m] +
+                              wzp * above[m]);
+                const int c = cell(i, row, k);
+                const bool pin = c == 0;
+                emit(c, 9 * mi + 3 * miss(row, g.ny) + mk, pin, cur[m], pin ? cur[m] : ax);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < RY; ++m) {
+            below[m] = cur[m];
+            cur[m] = above[m];
+        }
+    }
+}
+
 __device__ __forceinline__ bool stop_ok(const SeqArgs &a, double res, double thr) {
     return a.stop_rule == FLURSYS_STOP_REL_L2 ? res <= thr : res < thr;
 }
@@ -234,7 +404,7 @@ __global__ void __launch_bounds__(kBlock) seq_init(SeqArgs a) {
         const bool done = stop_ok(a, s->initial, s->threshold);
         s->status = done ? FLURSYS_LINEAR_CONVERGED : FLURSYS_LINEAR_MAX_ITERATIONS;
         s->done = done || a.max_iters <= 0;
-        cudaGraphSetConditional(a.h_loop, s->done ? 0u : 1u);
+        set_cond(a, a.h_loop, s->done ? 0u : 1u);
     }
 }
 
@@ -256,18 +426,237 @@ __global__ void __launch_bounds__(kBlock) seq_dir_spmv(SeqArgs a) {
         V r, d;
     };
     double sdq = 0.0;
-    tile_sweep(
-        g, blockIdx.x, tile, [&](int c) -> RawA { return RawA{r[c], first ? V(0) : dold[c]}; },
-        [&](RawA v, int cls, bool pin) -> V {
-            if (pin) return V(0);
-            const V z = V(double(v.r) * g.inv_diag[cls]);
-            return first ? z : V(z + vbeta * v.d);
-        },
-        [&](int c, int, bool, V dc, V qc) {
-            dcur[c] = dc;
-            q[c] = qc;
-            sdq += double(dc) * double(qc);
-        });
+    auto load_a = [&](int c) -> RawA { return RawA{r[c], first ? V(0) : dold[c]}; };
+    auto make_a = [&](RawA v, int cls, bool pin) -> V {
+        if (pin) return V(0);
+        const V z = V(double(v.r) * g.inv_diag[cls]);
+        return first ? z : V(z + vbeta * v.d);
+    };
+    auto emit_a = [&](int c, int, bool, V dc, V qc) {
+        dcur[c] = dc;
+        q[c] = qc;
+        sdq += double(dc) * double(qc);
+    };
+    if (a.sweep == kSweepWarp) warp_sweep<(sizeof(V) == 4 ? kRyOperand : kRyOperand / 2)>(g, blockIdx.x, load_a, make_a, emit_a);
+    else if (a.sweep == kSweepDirect) direct_sweep(g, blockIdx.x, load_a, make_a, emit_a);
+    else tile_sweep(g, blockIdx.x, tile, load_a, make_a, emit_a);
+    const double v[1] = {sdq};
+    if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
+    double o[1];
+    reduce_finish<1>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        const double dq = o[0];
+        if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(w->rz_old / dq)) {
+            w->error = FLURSYS_ERR_BREAKDOWN;
+            w->done = 1;
+            w->alpha = 0.0;
+        } else {
+            w->alpha = w->rz_old / dq;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Vectorised operand pass (the hot kernel): d = z + beta d_old, q = A d, d.q.
+// Warp w of a block owns rows [row0, row0 + RY) of a strip of 32*W columns;
+// lane l owns the W consecutive cells [i0 + W l, i0 + W l + W) of each row
+// (one float4 / double2 load per array per row). x neighbours: inside the
+// lane's vector, then the adjacent lanes by shuffle, and at the strip edges a
+// scalar halo loaded by lanes 0 and 31. y neighbours: the lane's own rows
+// plus one halo row below and above (prefetched with the rows). z
+// neighbours: registers, raw inputs prefetched one plane ahead. No shared
+// memory tiles and no block barriers in the plane loop.
+// Requires nx % W == 0 (checked on the host; the tile sweep serves the rest).
+// ---------------------------------------------------------------------------
+template <typename V>
+struct VecOf;
+template <>
+struct VecOf<float> {
+    using T = float4;
+    static constexpr int W = 4;
+};
+template <>
+struct VecOf<double> {
+    using T = double2;
+    static constexpr int W = 2;
+};
+
+template <typename V, bool MIXED, int RY>
+__global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
+    using VT = typename VecOf<V>::T;
+    constexpr int W = VecOf<V>::W;
+    constexpr int XW = 32 * W;
+    __shared__ double red[kBlock / 32];
+    __shared__ V idg[27];
+    const SeqGeo &g = a.g;
+    if (threadIdx.x < 27) idg[threadIdx.x] = V(g.inv_diag[threadIdx.x]);
+    __syncthreads();
+    const CgSeqState *s = a.st;
+    const bool first = s->first != 0;
+    const V beta = V(s->beta);
+    const int parity = (int)(s->iterations & 1);
+    const V *r = static_cast<const V *>(a.r);
+    V *dcur = static_cast<V *>(parity ? a.d1 : a.d0);
+    const V *dold = static_cast<const V *>(parity ? a.d0 : a.d1);
+    V *q = static_cast<V *>(a.q);
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int t = blockIdx.x;
+    const int ch = t % g.chunksv, col = t / g.chunksv;
+    const int i0 = (col % g.tiles_xv) * XW;
+    const int row0 = (col / g.tiles_xv) * (TY * RY) + wp * RY;
+    double sdq = 0.0;
+    if (row0 < g.ny) {
+        const int k0 = ch * g.kcv, k1 = min(g.nz, k0 + g.kcv);
+        const int ib = i0 + lane * W;
+        const bool inx = ib < g.nx;
+        const int ibc = inx ? ib : g.nx - W;  // idle lanes read a valid vector
+        const V wx = V(g.ix2), wy = V(g.iy2), wz = V(g.iz2);
+        // x weights of the lane's first and last element (domain walls)
+        const V wxm0 = (inx && ib > 0) ? wx : V(0);
+        const V wxpL = (inx && ib + W < g.nx) ? wx : V(0);
+        const int mx0 = miss(ibc, g.nx), mxL = miss(ibc + W - 1, g.nx);
+        const bool hw = lane == 0 && i0 > 0, he = lane == 31 && i0 + XW < g.nx;
+        const int xh = hw ? i0 - 1 : (he ? i0 + XW : 0);
+        const int mxh = miss(xh, g.nx);
+        const bool ys = row0 > 0, yn = row0 + RY < g.ny;
+        auto ld = [&](const V *p, int c) -> VT { return *reinterpret_cast<const VT *>(p + c); };
+        auto el = [](const VT &v, int e) -> V { return reinterpret_cast<const V *>(&v)[e]; };
+        auto idx = [&](int i, int row, int k) { return (k * g.ny + row) * g.nx + i; };
+        // d_new of W cells of one row from raw r and d_old vectors
+        auto make = [&](const VT &rv, const VT &dv, int row, int k, V (&out)[W]) {
+            const int cyz = 3 * miss(row, g.ny) + miss(k, g.nz);
+            const V mid = idg[cyz];
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+                V id = mid;
+                if (e == 0 && mx0) id = idg[9 * mx0 + cyz];
+                if (e == W - 1 && mxL) id = idg[9 * mxL + cyz];
+                const V z = el(rv, e) * id;
+                out[e] = first ? z : V(z + beta * el(dv, e));
+            }
+            if (k == 0 && row == 0 && ibc == 0) out[0] = V(0);  // pinned cell
+        };
+        auto make1 = [&](V rv, V dv, int i, int row, int k) -> V {
+            if (k == 0 && row == 0 && i == 0) return V(0);
+            const V z = rv * idg[9 * miss(i, g.nx) + 3 * miss(row, g.ny) + miss(k, g.nz)];
+            return first ? z : V(z + beta * dv);
+        };
+        V below[RY][W], cur[RY][W], above[RY][W];
+        VT nr[RY], nd[RY];        // raw inputs of the next plane (own rows)
+        VT sr, sd, hr, hd;        // raw inputs of the y halo rows of the next plane
+        V xr[RY], xd[RY];         // x halo scalars of the next plane
+        const VT zero{};
+        auto load_plane = [&](int k) {
+#pragma unroll
+            for (int m = 0; m < RY; ++m) {
+                const int row = row0 + m;
+                if (row < g.ny) {
+                    const int c = idx(ibc, row, k);
+                    nr[m] = ld(r, c);
+                    nd[m] = first ? zero : ld(dold, c);
+                    if (hw || he) {
+                        const int cx = idx(xh, row, k);
+                        xr[m] = r[cx];
+                        xd[m] = first ? V(0) : dold[cx];
+                    }
+                }
+            }
+            if (ys) { const int c = idx(ibc, row0 - 1, k); sr = ld(r, c); sd = first ? zero : ld(dold, c); }
+            if (yn) { const int c = idx(ibc, row0 + RY, k); hr = ld(r, c); hd = first ? zero : ld(dold, c); }
+        };
+        // prologue: planes k0-1 (below), k0 (cur); raw k0+1 in flight
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+#pragma unroll
+            for (int e = 0; e < W; ++e) below[m][e] = cur[m][e] = above[m][e] = V(0);
+        V vs[W], vn[W], vxh[RY];
+        if (k0 > 0) {
+            load_plane(k0 - 1);
+#pragma unroll
+            for (int m = 0; m < RY; ++m)
+                if (row0 + m < g.ny) make(nr[m], nd[m], row0 + m, k0 - 1, below[m]);
+        }
+        load_plane(k0);
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+            if (row0 + m < g.ny) make(nr[m], nd[m], row0 + m, k0, cur[m]);
+#pragma unroll
+        for (int e = 0; e < W; ++e) { vs[e] = V(0); vn[e] = V(0); }
+        if (ys) make(sr, sd, row0 - 1, k0, vs);
+        if (yn) make(hr, hd, row0 + RY, k0, vn);
+#pragma unroll
+        for (int m = 0; m < RY; ++m) vxh[m] = (hw || he) && row0 + m < g.ny ? make1(xr[m], xd[m], xh, row0 + m, k0) : V(0);
+        if (k0 + 1 < g.nz) load_plane(k0 + 1);
+        for (int k = k0; k < k1; ++k) {
+            // operand of plane k+1 for the own rows (its raw inputs landed during plane k-1)
+            const bool has_above = k + 1 < g.nz;
+            V vs1[W], vn1[W], vxh1[RY];
+#pragma unroll
+            for (int e = 0; e < W; ++e) { vs1[e] = V(0); vn1[e] = V(0); }
+            if (has_above) {
+#pragma unroll
+                for (int m = 0; m < RY; ++m)
+                    if (row0 + m < g.ny) make(nr[m], nd[m], row0 + m, k + 1, above[m]);
+                if (ys) make(sr, sd, row0 - 1, k + 1, vs1);
+                if (yn) make(hr, hd, row0 + RY, k + 1, vn1);
+#pragma unroll
+                for (int m = 0; m < RY; ++m)
+                    vxh1[m] = (hw || he) && row0 + m < g.ny ? make1(xr[m], xd[m], xh, row0 + m, k + 1) : V(0);
+            } else {
+#pragma unroll
+                for (int m = 0; m < RY; ++m) {
+                    vxh1[m] = V(0);
+#pragma unroll
+                    for (int e = 0; e < W; ++e) above[m][e] = V(0);
+                }
+            }
+            if (k + 2 < g.nz && k + 2 <= k1) load_plane(k + 2);  // next plane's loads in flight
+            const V wzm = k > 0 ? wz : V(0), wzp = has_above ? wz : V(0);
+#pragma unroll
+            for (int m = 0; m < RY; ++m) {
+                const int row = row0 + m;
+                // shuffles are warp-uniform: every lane takes part
+                V west = __shfl_up_sync(0xffffffffu, cur[m][W - 1], 1);
+                V east = __shfl_down_sync(0xffffffffu, cur[m][0], 1);
+                if (lane == 0) west = hw ? vxh[m] : V(0);
+                if (lane == 31) east = he ? vxh[m] : V(0);
+                if (!inx || row >= g.ny) continue;
+                const V wym = row > 0 ? wy : V(0), wyp = row + 1 < g.ny ? wy : V(0);
+                V dv[W], qv[W];
+#pragma unroll
+                for (int e = 0; e < W; ++e) {
+                    const V wxm = e == 0 ? wxm0 : wx, wxp = e == W - 1 ? wxpL : wx;
+                    const V xm = e == 0 ? west : cur[m][e - 1 < 0 ? 0 : e - 1];
+                    const V xp = e == W - 1 ? east : cur[m][e + 1 < W ? e + 1 : W - 1];
+                    const V ysv = m > 0 ? cur[m > 0 ? m - 1 : 0][e] : vs[e];
+                    const V ynv = m + 1 < RY ? cur[m + 1 < RY ? m + 1 : 0][e] : vn[e];
+                    const V c0 = cur[m][e];
+                    V ax = (wxm + wxp + wym + wyp + wzm + wzp) * c0 -
+                           (wxm * xm + wxp * xp + wym * ysv + wyp * ynv + wzm * below[m][e] + wzp * above[m][e]);
+                    if (k == 0 && row == 0 && ib + e == 0) ax = c0;  // identity row of the pinned cell
+                    dv[e] = c0;
+                    qv[e] = ax;
+                    sdq += double(c0) * double(ax);
+                }
+                const int c = idx(ib, row, k);
+                *reinterpret_cast<VT *>(dcur + c) = *reinterpret_cast<const VT *>(dv);
+                *reinterpret_cast<VT *>(q + c) = *reinterpret_cast<const VT *>(qv);
+            }
+#pragma unroll
+            for (int m = 0; m < RY; ++m) {
+                vxh[m] = vxh1[m];
+#pragma unroll
+                for (int e = 0; e < W; ++e) {
+                    below[m][e] = cur[m][e];
+                    cur[m][e] = above[m][e];
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < W; ++e) { vs[e] = vs1[e]; vn[e] = vn1[e]; }
+        }
+    }
     const double v[1] = {sdq};
     if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
     double o[1];
@@ -366,8 +755,8 @@ __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
         w->counter = 0;
         if (w->error) {
             w->done = 1;
-            cudaGraphSetConditional(a.h_replace, 0u);
-            cudaGraphSetConditional(a.h_loop, 0u);
+            set_cond(a, a.h_replace, 0u);
+            set_cond(a, a.h_loop, 0u);
             return;
         }
         w->iterations += 1;
@@ -377,8 +766,8 @@ __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
         if (!isfinite(res)) {
             w->error = FLURSYS_ERR_NON_FINITE;
             w->done = 1;
-            cudaGraphSetConditional(a.h_replace, 0u);
-            cudaGraphSetConditional(a.h_loop, 0u);
+            set_cond(a, a.h_replace, 0u);
+            set_cond(a, a.h_loop, 0u);
             return;
         }
         const bool conv = stop_ok(a, res, w->threshold);
@@ -386,10 +775,10 @@ __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
         if (replace) {
             w->replace = 1;
             w->rz_new = o[1];
-            cudaGraphSetConditional(a.h_replace, 1u);
+            set_cond(a, a.h_replace, 1u);
             return;  // the replacement launch takes the decision
         }
-        cudaGraphSetConditional(a.h_replace, 0u);
+        set_cond(a, a.h_replace, 0u);
         if (conv) {
             w->status = FLURSYS_LINEAR_CONVERGED;
             w->done = 1;
@@ -400,7 +789,7 @@ __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
             w->rz_old = o[1];
             w->first = 0;
         }
-        cudaGraphSetConditional(a.h_loop, w->done ? 0u : 1u);
+        set_cond(a, a.h_loop, w->done ? 0u : 1u);
     }
 }
 
@@ -442,7 +831,7 @@ __global__ void __launch_bounds__(kBlock) seq_replace(SeqArgs a) {
             w->rz_old = o[1];
             w->first = 0;
         }
-        cudaGraphSetConditional(a.h_loop, w->done ? 0u : 1u);
+        set_cond(a, a.h_loop, w->done ? 0u : 1u);
     }
 }
 
@@ -523,8 +912,9 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
     cudaGraphNode_t n_init, n_dir, n_upd, n_if, n_final;
     e = add_kernel(g, &n_init, nullptr, 0, (const void *)seq_init<V, MIXED>, a.nblocks_stencil, args);
     if (e == cudaSuccess) e = cudaGraphAddDependencies(g, &n_init, &n_while, 1);
-    if (e == cudaSuccess)
-        e = add_kernel(body, &n_dir, nullptr, 0, (const void *)seq_dir_spmv<V, MIXED>, a.nblocks_stencil, args);
+    const void *dir_fn = a.sweep == kSweepVec ? (const void *)seq_dir_vec<V, MIXED, kRyVec>
+                                              : (const void *)seq_dir_spmv<V, MIXED>;
+    if (e == cudaSuccess) e = add_kernel(body, &n_dir, nullptr, 0, dir_fn, a.nblocks_dir, args);
     if (e == cudaSuccess)
         e = add_kernel(body, &n_upd, &n_dir, 1, (const void *)seq_update<V, MIXED>, a.nblocks_point, args);
     if (e != cudaSuccess) return e;
@@ -572,20 +962,38 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
         const int mx = t / 9, my = (t / 3) % 3, mz = t % 3;
         const double dg = (2 - mx) * g.ix2 + (2 - my) * g.iy2 + (2 - mz) * g.iz2;
         g.inv_diag[t] = dg > 0.0 ? 1.0 / dg : 0.0;
+        // MIXED forms z = r/diag in FP32; r.z must use the same rounded
+        // Jacobi weights or the recurrences lose conjugacy.
+        if (precision == FLURSYS_PRECISION_MIXED) g.inv_diag[t] = double(float(g.inv_diag[t]));
     }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     g.tiles_x = (g.nx + TX - 1) / TX;
     g.tiles_y = (g.ny + TY - 1) / TY;
     const long long cols = (long long)g.tiles_x * g.tiles_y;
-    // enough tiles for about eight waves of four blocks per SM, at least four planes each
-    const long long want_tiles = (long long)sms * 4 * 8;
-    long long chunks = std::max(1LL, std::min<long long>(g.nz, (want_tiles + cols - 1) / cols));
-    int kc = (int)std::max(4LL, (g.nz + chunks - 1) / chunks);
-    kc = std::min(kc, g.nz);
-    g.kc = kc;
-    g.chunks = (g.nz + kc - 1) / kc;
+    // Chunk length in z: about `waves` waves of four resident blocks per SM,
+    // at least `kc_min` planes per chunk (FLURSYS_KC overrides both sweeps).
+    const char *kc_env = std::getenv("FLURSYS_KC");
+    const int kc_force = kc_env ? std::max(1, std::atoi(kc_env)) : 0;
+    const long long want_tiles = (long long)sms * 4 * 2;
+    auto chunking = [&](long long ncols, int *kc_out, int *chunks_out) {
+        long long chunks = std::max(1LL, std::min<long long>(g.nz, want_tiles / std::max(1LL, ncols)));
+        int kc = (int)((g.nz + chunks - 1) / chunks);
+        kc = std::max(kc, std::min(4, g.nz));
+        if (kc_force) kc = kc_force;
+        kc = std::min(kc, g.nz);
+        *kc_out = kc;
+        *chunks_out = (g.nz + kc - 1) / kc;
+    };
+    chunking((long long)g.tiles_x * g.tiles_y, &g.kc, &g.chunks);
     a.nblocks_stencil = g.tiles_x * g.tiles_y * g.chunks;
+    const int ryw = precision == FLURSYS_PRECISION_MIXED ? kRyOperand : kRyOperand / 2;
+    g.tiles_yw = (g.ny + TY * ryw - 1) / (TY * ryw);
+    chunking((long long)g.tiles_x * g.tiles_yw, &g.kcw, &g.chunksw);
+    const int wv = precision == FLURSYS_PRECISION_MIXED ? 4 : 2;
+    g.tiles_xv = (g.nx + 32 * wv - 1) / (32 * wv);
+    g.tiles_yv = (g.ny + TY * kRyVec - 1) / (TY * kRyVec);
+    chunking((long long)g.tiles_xv * g.tiles_yv, &g.kcv, &g.chunksv);
     a.nblocks_point = std::max(1, std::min(sms * 8, (g.n / 4 + kBlock - 1) / kBlock));
     a.x = args.x;
     a.rhs = args.rhs;
@@ -595,7 +1003,8 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.tol = args.tol; a.atol = args.atol; a.rtol = args.rtol;
     a.max_iters = args.max_iters;
     a.replace_every = args.replace_every > 0 ? args.replace_every : 50;
-    const int nb = std::max(a.nblocks_stencil, a.nblocks_point);
+    const int nb = std::max({a.nblocks_stencil, a.nblocks_point, g.tiles_x * g.tiles_yw * g.chunksw,
+                             g.tiles_xv * g.tiles_yv * g.chunksv});
     cudaError_t e = cudaMalloc(&plan.partials, sizeof(double) * 4 * nb);
     if (e == cudaSuccess) e = cudaMalloc(&plan.state, sizeof(CgSeqState));
     if (e == cudaSuccess) e = cudaMemset(plan.state, 0, sizeof(CgSeqState));
@@ -603,15 +1012,63 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.partials = plan.partials;
     a.st = plan.state;
     plan.precision = precision;
+    a.graph = 1;
+    const char *st = std::getenv("FLURSYS_STENCIL");
+    const bool vec_ok = g.nx % wv == 0;
+    a.sweep = vec_ok ? kSweepVec : kSweepTile;
+    if (st && std::strcmp(st, "direct") == 0) a.sweep = kSweepDirect;
+    if (st && std::strcmp(st, "tiled") == 0) a.sweep = kSweepTile;
+    if (st && std::strcmp(st, "warp") == 0) a.sweep = kSweepWarp;
+    a.nblocks_dir = a.sweep == kSweepWarp ? g.tiles_x * g.tiles_yw * g.chunksw
+                  : a.sweep == kSweepVec  ? g.tiles_xv * g.tiles_yv * g.chunksv
+                                          : a.nblocks_stencil;
     e = precision == FLURSYS_PRECISION_MIXED ? build<float, true>(plan, a) : build<double, false>(plan, a);
+    plan.host_args = new SeqArgs(a);
+    const char *v = std::getenv("FLURSYS_PCG_VARIANT");
+    if (v && std::strcmp(v, "host") == 0) plan.host_iterations = (int)std::min<long long>(a.max_iters, 1 << 20);
     return e;
 }
 
 cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream) {
+    if (plan.host_iterations > 0) return pcg3d_seq_run_host(plan, stream);
     return cudaGraphLaunch(plan.exec, stream);
 }
 
+// Diagnostic mode: the same kernels launched from the host for a fixed
+// number of iterations (no device loop control), so profilers that cannot
+// look inside conditional graph nodes see every launch.
+cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t st) {
+    SeqArgs a = *static_cast<const SeqArgs *>(plan.host_args);
+    a.graph = 0;
+    const bool mixed = plan.precision == FLURSYS_PRECISION_MIXED;
+    if (mixed) seq_init<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+    else seq_init<double, false><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+    for (int it = 1; it <= plan.host_iterations; ++it) {
+        if (mixed) {
+            if (a.sweep == kSweepVec) seq_dir_vec<float, true, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+            else seq_dir_spmv<float, true><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+            seq_update<float, true><<<a.nblocks_point, kBlock, 0, st>>>(a);
+            if (it % a.replace_every == 0) {
+                seq_fold<<<a.nblocks_point, kBlock, 0, st>>>(a);
+                seq_replace<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+            }
+        } else {
+            if (a.sweep == kSweepVec) seq_dir_vec<double, false, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+            else seq_dir_spmv<double, false><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+            seq_update<double, false><<<a.nblocks_point, kBlock, 0, st>>>(a);
+        }
+    }
+    if (mixed) {
+        seq_fold_pending<<<a.nblocks_point, kBlock, 0, st>>>(a);
+        seq_final<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+    } else {
+        seq_final<double, false><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 void pcg3d_seq_destroy(Pcg3dSeqPlan &plan) {
+    delete static_cast<SeqArgs *>(plan.host_args);
     if (plan.exec) cudaGraphExecDestroy(plan.exec);
     if (plan.graph) cudaGraphDestroy(plan.graph);
     cudaFree(plan.partials);

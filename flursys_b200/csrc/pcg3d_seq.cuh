@@ -23,6 +23,8 @@ struct Pcg3dSeqPlan {
     double *partials = nullptr;
     CgSeqState *state = nullptr;
     int precision = 0;
+    int host_iterations = 0;    // > 0: diagnostic host-driven mode with this many iterations
+    void *host_args = nullptr;  // argument block of the kernels
 };
 
 // Builds and instantiates the solve graph for fixed buffers (args as for
@@ -30,5 +32,6 @@ struct Pcg3dSeqPlan {
 cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precision, int device);
 cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream);
 void pcg3d_seq_destroy(Pcg3dSeqPlan &plan);
+cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t stream);
 
 }  // namespace flursys

@@ -10,6 +10,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import subprocess
 
 from . import _abi
 from .solver import BackendOptions, LidDrivenCavity3DConfig, _Handle
@@ -20,12 +21,13 @@ def main():
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--iters", type=int, default=20000, help="pressure iteration limit")
     args = ap.parse_args()
     n = args.size
     h = 1.0 / n
     nu = 1.0 / 400.0
     cfg = LidDrivenCavity3DConfig(nx=n, ny=n, nz=n, reynolds=400.0, dt=min(0.5 * h, 0.25 * h * h / (3 * nu)),
-                                  pressure_max_iters=20000, pressure_solver="pcg",
+                                  pressure_max_iters=args.iters, pressure_solver="pcg",
                                   backend=BackendOptions(precision=args.precision, stop_rule="rel-l2",
                                                          pressure_rtol=1e-8))
     hd = _Handle(cfg.to_c())
@@ -40,6 +42,12 @@ def main():
                           "phase_us_per_iteration": {k: 1000.0 * ph[i] / its for i, k in enumerate(
                               ["stencil", "pointwise", "barrier+reduce", "replacement"])}}))
     hd.close()
+    try:
+        q = subprocess.run(["nvidia-smi", "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                            "--format=csv,noheader"], capture_output=True, text=True, timeout=10).stdout.strip()
+        print(json.dumps({"clocks_after": q}))
+    except Exception:
+        pass
 
 
 if __name__ == "__main__":
