@@ -198,6 +198,11 @@ SIGNATURES = {
     "flursys_cuda_stencil_pcg": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                              C.c_double, _D, _D, C.c_int32,
                                              C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport)]),
+    # device pointers (rhs, x) and a cudaStream_t
+    "flursys_cuda_stencil_pcg_noalloc": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                                     C.c_double, _P, _P, C.c_int32,
+                                                     C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport),
+                                                     _P]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libflursys_cuda.so")

@@ -305,6 +305,36 @@ int32_t flursys_cuda_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, double dx, 
                                  int32_t precision, const FlursysLinearSolverOptions *options,
                                  FlursysLinearSolveReport *report);
 
+/* Allocation-free variant of the 3D matrix-free pressure PCG. No reference
+ * counterpart: the reference solves on the host and has no device memory.
+ *
+ * Some callers cannot let a library allocate device memory: applications
+ * whose device memory is entirely owned by their own pool allocator (a
+ * cudaMalloc would fail or fragment it), services running under a hard
+ * per-process memory cap, and latency-sensitive pipelines that cannot take
+ * the device-wide synchronisation a cudaFree implies. This entry point calls
+ * no cudaMalloc, cudaFree or other allocating routine: it solves the same
+ * pinned 7-point system as flursys_cuda_stencil_pcg (nz >= 2; A x = -rhs,
+ * x(0,0,0) = 0; stop when ||r||_2 <= atol + rtol ||r0||_2) with the same
+ * kernel, on caller-owned DEVICE buffers `rhs_device` and `x_device`
+ * (nx*ny*nz FP64 values each, 16-byte aligned; x_device holds the initial
+ * guess in and the solution out), enqueued on `stream` (NULL = the default
+ * stream); it returns after the solve, with `report` filled.
+ *
+ * Its scratch (work vectors, partial sums, barrier, result) is one
+ * file-scope device array of about 9.2 MB that every device loading the
+ * library keeps until the process exits. Limit: nx*ny*nz <= 262144 cells
+ * (64^3); larger grids are rejected with FLURSYS_ERR_INVALID_ARGUMENT and a
+ * message in flursys_cuda_global_error(). Every call shares the array and
+ * it keeps the last call's contents, so calls that overlap on the GPU (two
+ * host threads, two streams) race; run them one after another. The first
+ * call on a device looks up the array's device address with that device
+ * current; make that first call before any stream capture. */
+int32_t flursys_cuda_stencil_pcg_noalloc(int64_t nx, int64_t ny, int64_t nz, double dx, double dy, double dz,
+                                         const double *rhs_device, double *x_device, int32_t precision,
+                                         const FlursysLinearSolverOptions *options,
+                                         FlursysLinearSolveReport *report, void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
