@@ -52,18 +52,26 @@ def workload_config(n: int, precision: str):
 
 
 def pcg_bytes_per_launch(n_cells: int, iterations: int, precision: str, replace_every: int = 50) -> float:
-    """Compulsory HBM bytes of one pressure-solve launch."""
+    """Compulsory HBM bytes of one pressure solve (one graph launch).
+
+    MIXED per cell: init 24 (read x, rhs; write r, dx), each iteration 40
+    (operand pass: read r, d_old, write d, q — 4 B each; update pass: read
+    dx, d, r, q, write dx, r), each FP64 residual replacement 44 (fold: read
+    x, dx, write x; residual: read x, rhs, write r, dx), final check 16.
+    F64: init 24, each iteration 80, final 16.
+    """
     if precision == "mixed":
-        init = 24        # read x, rhs (8+8); write r, dx (4+4)
-        per_it = 40      # A: read r, d_old; write d, q (4 each); B: read dx, d, r, q; write dx, r (4 each)
-        per_rep = 44     # fold: read x 8, dx 4, write x 8; residual: read x, rhs, write r, dx
-        final = 16       # read x, rhs
         nrep = iterations // replace_every + 1
-        return float(n_cells) * (init + per_it * iterations + per_rep * nrep + final)
-    init = 32            # read x, rhs; write r (8 each) + read x halo
-    per_it = 80          # A: read r, d_old; write d, q; B: read x, d, r, q; write x, r (8 each)
-    final = 16
-    return float(n_cells) * (init - 8 + per_it * iterations + final)
+        return float(n_cells) * (24 + 40 * iterations + 44 * nrep + 16)
+    return float(n_cells) * (24 + 80 * iterations + 16)
+
+
+def launches_per_step(iterations: int, precision: str, replace_every: int = 50) -> int:
+    """Kernels of one 3D step: predictor (3), rhs, correction, diagnostics (2),
+    and the solve graph: init, operand + update per iteration, fold + replace
+    per FP64 replacement, pending fold, final check."""
+    nrep = iterations // replace_every + 1 if precision == "mixed" else 0
+    return 7 + 1 + 2 * iterations + 2 * nrep + (1 if precision == "mixed" else 0) + 1
 
 
 class ClockSampler:
@@ -270,10 +278,12 @@ def run_ours(args):
                        "true_relative_residual_max": max(true_rel), "parallelism": f"replicas{world}"},
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": hbytes,
                     "d2h_bytes_per_step": hbytes + report_bytes},
-            "gpu_launches": 8 * args.steps,
+            "gpu_launches": sum(launches_per_step(i, precision) for i in its),
             "clocks": clocks,
         }
         line["roofline"] = roofline(n_cells, its, solve_ms, precision)
+        if args.big_size and not args.no_big:
+            line["pcg_big"] = big_solve(args.big_size, precision, local)
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             steps, elapsed, cits = cpu_reference_run(n, 3, args.cpu_budget, threads)
@@ -285,6 +295,23 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def big_solve(n, precision, device):
+    """Two steps of the n^3 cavity (the 256^3 shape of the learned-FCG
+    comparison), plain PCG: pressure-solve ms, iterations and HBM roofline."""
+    from flursys_b200.solver import _Handle
+    _, c = workload_config(n, precision)
+    c.device = device
+    h = _Handle(c)
+    h.step(1)  # first step from the zero field; the second is timed
+    rep = h.step(1)
+    h.close()
+    its = int(rep.pressure_iterations)
+    r = roofline(n ** 3, [its], [rep.pressure_solve_ms], precision)
+    return {"cells": n ** 3, "pressure_iterations": its, "pressure_solve_ms": rep.pressure_solve_ms,
+            "step_ms": rep.step_ms, "true_relative_residual": rep.pressure_true_relative_residual,
+            "roofline_frac": r["frac"], "achieved_gbs": r["achieved"]}
 
 
 def roofline(n_cells, its, solve_ms, precision):
@@ -304,7 +331,8 @@ def roofline(n_cells, its, solve_ms, precision):
         traffic = per_cell_it * n_cells * (sum(its) / len(its))
     except Exception:
         pass
-    return {"bound": "hbm", "kernel": "pcg3d_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    return {"bound": "hbm", "kernel": "pressure-solve graph (seq_dir_vec + seq_update per iteration)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_src,
             "algorithmic_bytes_per_launch": bytes_total / len(its), "traffic": traffic}
 
@@ -320,6 +348,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--reference-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--big-size", type=int, default=256, help="size of the extra plain-PCG solve measurement")
+    ap.add_argument("--no-big", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

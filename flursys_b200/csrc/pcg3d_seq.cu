@@ -413,6 +413,7 @@ __global__ void __launch_bounds__(kBlock) seq_dir_spmv(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
     __shared__ double red[kBlock / 32];
     const CgSeqState *s = a.st;
+    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
     const double beta = s->beta;
     const bool first = s->first != 0;
     const int parity = (int)(s->iterations & 1);  // d buffers alternate per iteration
@@ -494,6 +495,7 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
     if (threadIdx.x < 27) idg[threadIdx.x] = V(g.inv_diag[threadIdx.x]);
     __syncthreads();
     const CgSeqState *s = a.st;
+    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
     const bool first = s->first != 0;
     const V beta = V(s->beta);
     const int parity = (int)(s->iterations & 1);
@@ -679,6 +681,7 @@ template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
     __shared__ double red[kBlock / 32];
     const CgSeqState *s = a.st;
+    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
     const double alpha = s->alpha;
     const bool dead = s->error != 0;
     const int parity = (int)(s->iterations & 1);
@@ -794,6 +797,7 @@ __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
 }
 
 __global__ void __launch_bounds__(kBlock) seq_fold(SeqArgs a) {
+    if (!a.graph && !a.st->replace) return;  // host-driven mode: no replacement due
     const int stride = gridDim.x * kBlock;
     for (int c = blockIdx.x * kBlock + threadIdx.x; c < a.g.n; c += stride) {
         if (c == 0) { a.x[0] = 0.0; continue; }
@@ -805,6 +809,7 @@ template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_replace(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
     __shared__ double red[kBlock / 32];
+    if (!a.graph && !a.st->replace) return;  // host-driven mode: no replacement due
     double srr = 0.0, srz = 0.0, smax = 0.0;
     residual_tile<V, MIXED>(a, tile, srr, srz, smax, true);
     const double v[3] = {srr, srz, smax};
@@ -1025,7 +1030,7 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     e = precision == FLURSYS_PRECISION_MIXED ? build<float, true>(plan, a) : build<double, false>(plan, a);
     plan.host_args = new SeqArgs(a);
     const char *v = std::getenv("FLURSYS_PCG_VARIANT");
-    if (v && std::strcmp(v, "host") == 0) plan.host_iterations = (int)std::min<long long>(a.max_iters, 1 << 20);
+    if (v && std::strcmp(v, "host") == 0) plan.host_iterations = 1;
     return e;
 }
 
@@ -1034,29 +1039,35 @@ cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream) {
     return cudaGraphLaunch(plan.exec, stream);
 }
 
-// Diagnostic mode: the same kernels launched from the host for a fixed
-// number of iterations (no device loop control), so profilers that cannot
-// look inside conditional graph nodes see every launch.
+// Host-driven mode (diagnostics): the same kernels launched one by one from
+// the host, so profilers that cannot look inside conditional graph nodes see
+// every launch. The kernels honour the device flags (`done`, `replace`)
+// exactly as the graph's conditional nodes do; the host checks `done` after
+// every chunk of 16 iterations.
 cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t st) {
     SeqArgs a = *static_cast<const SeqArgs *>(plan.host_args);
     a.graph = 0;
     const bool mixed = plan.precision == FLURSYS_PRECISION_MIXED;
     if (mixed) seq_init<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
     else seq_init<double, false><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
-    for (int it = 1; it <= plan.host_iterations; ++it) {
-        if (mixed) {
-            if (a.sweep == kSweepVec) seq_dir_vec<float, true, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
-            else seq_dir_spmv<float, true><<<a.nblocks_dir, kBlock, 0, st>>>(a);
-            seq_update<float, true><<<a.nblocks_point, kBlock, 0, st>>>(a);
-            if (it % a.replace_every == 0) {
+    int done = 0;
+    for (long long it = 0; it < a.max_iters && !done; it += 16) {
+        for (int j = 0; j < 16; ++j) {
+            if (mixed) {
+                if (a.sweep == kSweepVec) seq_dir_vec<float, true, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+                else seq_dir_spmv<float, true><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+                seq_update<float, true><<<a.nblocks_point, kBlock, 0, st>>>(a);
                 seq_fold<<<a.nblocks_point, kBlock, 0, st>>>(a);
                 seq_replace<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+            } else {
+                if (a.sweep == kSweepVec) seq_dir_vec<double, false, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+                else seq_dir_spmv<double, false><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+                seq_update<double, false><<<a.nblocks_point, kBlock, 0, st>>>(a);
             }
-        } else {
-            if (a.sweep == kSweepVec) seq_dir_vec<double, false, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
-            else seq_dir_spmv<double, false><<<a.nblocks_dir, kBlock, 0, st>>>(a);
-            seq_update<double, false><<<a.nblocks_point, kBlock, 0, st>>>(a);
         }
+        cudaError_t e = cudaMemcpyAsync(&done, &plan.state->done, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
     }
     if (mixed) {
         seq_fold_pending<<<a.nblocks_point, kBlock, 0, st>>>(a);

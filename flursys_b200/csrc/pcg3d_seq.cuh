@@ -23,7 +23,7 @@ struct Pcg3dSeqPlan {
     double *partials = nullptr;
     CgSeqState *state = nullptr;
     int precision = 0;
-    int host_iterations = 0;    // > 0: diagnostic host-driven mode with this many iterations
+    int host_iterations = 0;    // > 0: host-driven mode (diagnostics; FLURSYS_PCG_VARIANT=host)
     void *host_args = nullptr;  // argument block of the kernels
 };
 
