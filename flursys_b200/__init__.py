@@ -7,12 +7,12 @@ reference's solver and linear-algebra interfaces; it has no CPU fallback.
 from . import _abi
 from .cases import (BackwardStepCase, Case, CavityCase, ChannelCase, CylinderCase, SolverBoundaryOverride,
                     SolverBoundaryOverrides)
-from .solver import (BackendOptions, FieldUpdate, IncompressibleSolver, LidDrivenCavity3DConfig,
+from .solver import (BackendOptions, BatchedIncompressibleSolver, FieldUpdate, IncompressibleSolver, LidDrivenCavity3DConfig,
                      LidDrivenCavity3DSolver, RunSummary, RunSummary3D, SimulationConfig, SolverError, SolverStep,
                      TimeStepSettings)
 
 __all__ = [
-    "BackendOptions", "BackwardStepCase", "Case", "CavityCase", "ChannelCase", "CylinderCase", "FieldUpdate",
+    "BackendOptions", "BatchedIncompressibleSolver", "BackwardStepCase", "Case", "CavityCase", "ChannelCase", "CylinderCase", "FieldUpdate",
     "IncompressibleSolver", "LidDrivenCavity3DConfig", "LidDrivenCavity3DSolver", "RunSummary", "RunSummary3D",
     "SimulationConfig", "SolverBoundaryOverride", "SolverBoundaryOverrides", "SolverError", "SolverStep",
     "TimeStepSettings", "load_library",

@@ -170,6 +170,19 @@ class StepReport(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [
+        ("tile_elems", C.c_int32 * 6),
+        ("pressure_blocks_per_sm", C.c_int32),
+        ("pressure_blocks", C.c_int32),
+        ("graph_nodes", C.c_int32),
+        ("reserved", C.c_int32),
+        ("tune_ms", C.c_double),
+    ]
+
+
+BATCH_AUTOTUNE, BATCH_NO_GRAPH = 1, 2
+
 # Every extern "C" entry point of include/flursys_cuda.h: (restype, argtypes).
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
@@ -203,6 +216,12 @@ SIGNATURES = {
                                                      C.c_double, _P, _P, C.c_int32,
                                                      C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport),
                                                      _P]),
+    "flursys_cuda_batch_create": (C.c_int32, [C.POINTER(CudaConfig), C.c_int32, C.c_int32, C.POINTER(_P)]),
+    "flursys_cuda_batch_step": (C.c_int32, [_P, C.c_int64]),
+    "flursys_cuda_batch_report": (C.c_int32, [_P, C.c_int32, C.POINTER(StepReport), C.POINTER(C.c_int32)]),
+    "flursys_cuda_batch_download": (C.c_int32, [_P, C.c_int32, C.c_int32, _D, C.c_size_t]),
+    "flursys_cuda_batch_tuning": (C.c_int32, [_P, C.POINTER(BatchTuning)]),
+    "flursys_cuda_batch_destroy": (C.c_int32, [_P]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libflursys_cuda.so")

@@ -101,6 +101,8 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
 
 namespace flursys {
 
+int32_t validate_config_checked(const FlursysCudaConfig &c, std::string *msg) { return validate_config(c, msg); }
+
 void set_global_error(const std::string &msg) { g_error = msg; }
 
 int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what) {

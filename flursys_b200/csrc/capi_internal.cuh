@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "cavity3d.cuh"
 #include "common.cuh"
@@ -61,6 +62,8 @@ struct FlursysCudaHandle {
 namespace flursys {
 
 int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what);
+// SimulationConfig::validate / LidDrivenCavity3DConfig::validate of a config.
+int32_t validate_config_checked(const FlursysCudaConfig &c, std::string *msg);
 // Message returned by flursys_cuda_global_error() on this thread.
 void set_global_error(const std::string &msg);
 // Matrix-free 2D pressure PCG for flursys_cuda_stencil_pcg (nz == 1).
@@ -76,6 +79,24 @@ void on_upload2d(FlursysCudaHandle *h, int32_t id);
 int32_t init2d(FlursysCudaHandle *h);
 void free2d(FlursysCudaHandle *h);
 bool field_ptr2d(FlursysCudaHandle *h, int32_t id, double **p, size_t *n);
+
+// Host-side data of one 2D case (src/cases/mod.rs:120-227 with the
+// SolverBoundaryOverrides of src/preprocess.rs:1370-1388): boundary kinds,
+// cell flags, boundary velocity arrays and the initial field of
+// initialize_velocity (incompressible.rs:588-620).
+struct Case2dHost {
+    int kind[4];          // BoundaryKindDev per side
+    double outlet_p;      // right-side outlet pressure
+    bool project;         // pure Neumann pressure system (no outlet)
+    std::vector<uint8_t> flags;  // CellFlag bits, nx*ny
+    long long fluid;      // cells that are neither solid nor outlet
+    int ref_cell;         // first non-solid cell
+    // bu_left, bu_right, bv_bottom, bv_top, gu_bottom, gu_top, gv_left, gv_right
+    std::vector<double> bnd[8];
+    std::vector<double> u, v;    // initial face velocities
+    double max_u, max_v;  // max |u|, |v| of the initial field
+};
+void build_case2d(const FlursysCudaConfig &c, Case2dHost *out);
 int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
                   const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,
                   long long max_iters, int replace_every, cudaStream_t stream, std::string *err);

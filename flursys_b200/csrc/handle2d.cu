@@ -128,7 +128,6 @@ struct HostCase {
 
 struct Handle2D {
     Cavity2dState s{};
-    HostCase hc{};
     double current_dt = 0.0;
     double outlet_p = 0.0;
     bool project = false;
@@ -227,45 +226,40 @@ bool reached_end_time(const FlursysCudaConfig &c, double time) {
 
 }  // namespace
 
-int32_t init2d(FlursysCudaHandle *h) {
-    const FlursysCudaConfig &c = h->cfg;
-    auto *h2 = new Handle2D();
-    h->h2 = h2;
-    Cavity2dState &s = h2->s;
-    HostCase &hc = h2->hc;
+void build_case2d(const FlursysCudaConfig &c, Case2dHost *out) {
+    HostCase hc{};
     hc.c = c.case_params;
     std::memcpy(hc.ov, c.overrides, sizeof hc.ov);
     const int nx = (int)c.nx, ny = (int)c.ny;
-    s.nx = nx; s.ny = ny; s.sms = h->sms;
-    s.dx = c.case_params.length / nx;
-    s.dy = c.case_params.height / ny;
-    s.rho = c.case_params.density;
-    s.nu = c.case_params.kinematic_viscosity;
-    s.convection = c.convection;
-    for (int side = 0; side < 4; ++side) s.kind[side] = hc.kind(side);
-    hc.kind(FLURSYS_SIDE_RIGHT, &h2->outlet_p);
-    h2->project = s.kind[FLURSYS_SIDE_RIGHT] != kBkOutlet;  // pressure_reference_required (:1625-1632)
-    h2->current_dt = c.dt;
+    const double dx = c.case_params.length / nx, dy = c.case_params.height / ny;
+    Case2dHost &o = *out;
+    for (int side = 0; side < 4; ++side) o.kind[side] = hc.kind(side);
+    hc.kind(FLURSYS_SIDE_RIGHT, &o.outlet_p);
+    o.project = o.kind[FLURSYS_SIDE_RIGHT] != kBkOutlet;  // pressure_reference_required (:1625-1632)
 
     // masks and boundary data
-    std::vector<uint8_t> solid(nx * ny), flags(nx * ny);
-    long long fluid = 0;
-    int ref_cell = -1;
+    std::vector<uint8_t> solid(nx * ny);
+    o.flags.assign(nx * ny, 0);
+    o.fluid = 0;
+    o.ref_cell = -1;
     for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) solid[i + nx * j] = hc.is_solid((i + 0.5) * s.dx, (j + 0.5) * s.dy) ? 1 : 0;
+        for (int i = 0; i < nx; ++i) solid[i + nx * j] = hc.is_solid((i + 0.5) * dx, (j + 0.5) * dy) ? 1 : 0;
     for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) {
             uint8_t f = solid[i + nx * j] ? kCellSolid : 0;
-            if (i + 1 == nx && !solid[i + nx * j] && s.kind[FLURSYS_SIDE_RIGHT] == kBkOutlet) f |= kCellOutlet;
-            flags[i + nx * j] = f;
-            if (!(f & 3)) ++fluid;
-            if (!solid[i + nx * j] && ref_cell < 0) ref_cell = i + nx * j;
+            if (i + 1 == nx && !solid[i + nx * j] && o.kind[FLURSYS_SIDE_RIGHT] == kBkOutlet) f |= kCellOutlet;
+            o.flags[i + nx * j] = f;
+            if (!(f & 3)) ++o.fluid;
+            if (!solid[i + nx * j] && o.ref_cell < 0) o.ref_cell = i + nx * j;
         }
-    std::vector<double> bul(ny), bur(ny), bvb(nx), bvt(nx), gub(nx + 1), gut(nx + 1), gvl(ny + 1), gvr(ny + 1);
+    std::vector<double> &bul = o.bnd[0], &bur = o.bnd[1], &bvb = o.bnd[2], &bvt = o.bnd[3];
+    std::vector<double> &gub = o.bnd[4], &gut = o.bnd[5], &gvl = o.bnd[6], &gvr = o.bnd[7];
+    bul.assign(ny, 0.0); bur.assign(ny, 0.0); bvb.assign(nx, 0.0); bvt.assign(nx, 0.0);
+    gub.assign(nx + 1, 0.0); gut.assign(nx + 1, 0.0); gvl.assign(ny + 1, 0.0); gvr.assign(ny + 1, 0.0);
     double a, b;
     for (int j = 0; j < ny; ++j) {
-        hc.velocity(FLURSYS_SIDE_LEFT, (j + 0.5) * s.dy, &a, &b); bul[j] = a;
-        hc.velocity(FLURSYS_SIDE_RIGHT, (j + 0.5) * s.dy, &a, &b); bur[j] = a;
+        hc.velocity(FLURSYS_SIDE_LEFT, (j + 0.5) * dy, &a, &b); bul[j] = a;
+        hc.velocity(FLURSYS_SIDE_RIGHT, (j + 0.5) * dy, &a, &b); bur[j] = a;
     }
     for (int i = 0; i < nx; ++i) {
         hc.velocity(FLURSYS_SIDE_BOTTOM, 0.0, &a, &b); bvb[i] = b;
@@ -276,29 +270,57 @@ int32_t init2d(FlursysCudaHandle *h) {
         hc.velocity(FLURSYS_SIDE_TOP, hc.c.height, &a, &b); gut[i] = a;
     }
     for (int j = 0; j <= ny; ++j) {
-        hc.velocity(FLURSYS_SIDE_LEFT, j * s.dy, &a, &b); gvl[j] = b;
-        hc.velocity(FLURSYS_SIDE_RIGHT, j * s.dy, &a, &b); gvr[j] = b;
+        hc.velocity(FLURSYS_SIDE_LEFT, j * dy, &a, &b); gvl[j] = b;
+        hc.velocity(FLURSYS_SIDE_RIGHT, j * dy, &a, &b); gvr[j] = b;
     }
     // initialize_velocity (:588-620)
-    std::vector<double> u((nx + 1) * ny), v(nx * (ny + 1));
+    std::vector<double> &u = o.u, &v = o.v;
+    u.assign((size_t)(nx + 1) * ny, 0.0);
+    v.assign((size_t)nx * (ny + 1), 0.0);
     auto sol = [&](int i, int j) { return solid[i + nx * j] != 0; };
     for (int j = 0; j < ny; ++j)
         for (int i = 0; i <= nx; ++i) {
-            hc.initial_velocity(i * s.dx, (j + 0.5) * s.dy, &a, &b);
+            hc.initial_velocity(i * dx, (j + 0.5) * dy, &a, &b);
             const bool open = i == 0 ? !sol(0, j) : (i == nx ? !sol(nx - 1, j) : !sol(i - 1, j) && !sol(i, j));
             u[i + (nx + 1) * j] = open ? a : 0.0;
         }
     for (int j = 0; j <= ny; ++j)
         for (int i = 0; i < nx; ++i) {
-            hc.initial_velocity((i + 0.5) * s.dx, j * s.dy, &a, &b);
+            hc.initial_velocity((i + 0.5) * dx, j * dy, &a, &b);
             const bool open = j == 0 ? !sol(i, 0) : (j == ny ? !sol(i, ny - 1) : !sol(i, j - 1) && !sol(i, j));
             v[i + nx * j] = open ? b : 0.0;
         }
-    host_boundaries(hc, nx, ny, s.dx, s.dy, solid, u, v);
-    h2->last_max_u = 0.0;
-    h2->last_max_v = 0.0;
-    for (double x : u) h2->last_max_u = std::max(h2->last_max_u, std::fabs(x));
-    for (double x : v) h2->last_max_v = std::max(h2->last_max_v, std::fabs(x));
+    host_boundaries(hc, nx, ny, dx, dy, solid, u, v);
+    o.max_u = 0.0;
+    o.max_v = 0.0;
+    for (double x : u) o.max_u = std::max(o.max_u, std::fabs(x));
+    for (double x : v) o.max_v = std::max(o.max_v, std::fabs(x));
+}
+
+int32_t init2d(FlursysCudaHandle *h) {
+    const FlursysCudaConfig &c = h->cfg;
+    auto *h2 = new Handle2D();
+    h->h2 = h2;
+    Cavity2dState &s = h2->s;
+    Case2dHost cs;
+    build_case2d(c, &cs);
+    const int nx = (int)c.nx, ny = (int)c.ny;
+    s.nx = nx; s.ny = ny; s.sms = h->sms;
+    s.dx = c.case_params.length / nx;
+    s.dy = c.case_params.height / ny;
+    s.rho = c.case_params.density;
+    s.nu = c.case_params.kinematic_viscosity;
+    s.convection = c.convection;
+    for (int side = 0; side < 4; ++side) s.kind[side] = cs.kind[side];
+    h2->outlet_p = cs.outlet_p;
+    h2->project = cs.project;
+    h2->current_dt = c.dt;
+    h2->last_max_u = cs.max_u;
+    h2->last_max_v = cs.max_v;
+    const std::vector<uint8_t> &flags = cs.flags;
+    const std::vector<double> &u = cs.u, &v = cs.v;
+    const long long fluid = cs.fluid;
+    const int ref_cell = cs.ref_cell;
 
     cudaError_t e = cudaSuccess;
     const size_t nc = (size_t)nx * ny, nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
@@ -308,10 +330,9 @@ int32_t init2d(FlursysCudaHandle *h) {
     s.p = dalloc(h2, nc, &e); s.rhs = dalloc(h2, nc, &e); s.pold = dalloc(h2, nc, &e);
     s.uc = dalloc(h2, nc, &e); s.vc = dalloc(h2, nc, &e); s.speed = dalloc(h2, nc, &e); s.vort = dalloc(h2, nc, &e);
     double *bd[8];
-    const std::vector<double> *bh[8] = {&bul, &bur, &bvb, &bvt, &gub, &gut, &gvl, &gvr};
     for (int k = 0; k < 8; ++k) {
-        bd[k] = dalloc(h2, bh[k]->size(), &e);
-        if (e == cudaSuccess) e = cudaMemcpy(bd[k], bh[k]->data(), bh[k]->size() * sizeof(double), cudaMemcpyHostToDevice);
+        bd[k] = dalloc(h2, cs.bnd[k].size(), &e);
+        if (e == cudaSuccess) e = cudaMemcpy(bd[k], cs.bnd[k].data(), cs.bnd[k].size() * sizeof(double), cudaMemcpyHostToDevice);
     }
     s.bu_left = bd[0]; s.bu_right = bd[1]; s.bv_bottom = bd[2]; s.bv_top = bd[3];
     s.gu_bottom = bd[4]; s.gu_top = bd[5]; s.gv_left = bd[6]; s.gv_right = bd[7];

@@ -445,14 +445,23 @@ cudaError_t pcg2d_max_grid(int precision, int device, int *grid) {
 int pcg2d_block_size() { return kBlock; }
 int pcg2d_num_partials() { return kParts; }
 
+// cudaLaunchKernelEx with the cooperative attribute: valid on a stream and
+// inside stream capture (the batched solver records it in its step graph).
 cudaError_t pcg2d_launch(const Pcg2dInstance *inst_dev, int ninst, int total_blocks, int precision,
                          cudaStream_t stream) {
-    void *params[] = {(void *)&inst_dev, &ninst};
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(total_blocks);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (precision == FLURSYS_PRECISION_MIXED)
-        return cudaLaunchCooperativeKernel((const void *)pcg2d_kernel<float, true>, dim3(total_blocks),
-                                           dim3(kBlock), params, 0, stream);
-    return cudaLaunchCooperativeKernel((const void *)pcg2d_kernel<double, false>, dim3(total_blocks), dim3(kBlock),
-                                       params, 0, stream);
+        return cudaLaunchKernelEx(&cfg, pcg2d_kernel<float, true>, inst_dev, ninst);
+    return cudaLaunchKernelEx(&cfg, pcg2d_kernel<double, false>, inst_dev, ninst);
 }
 
 }  // namespace flursys

@@ -408,3 +408,78 @@ class IncompressibleSolver:
 
     def close(self) -> None:
         self._h.close()
+
+
+class BatchedIncompressibleSolver:
+    """Many independent IncompressibleSolver instances (2D, projection
+    coupling) of uneven size advanced together on one device.
+
+    No reference counterpart: each instance computes what
+    ``IncompressibleSolver`` (src/solver/incompressible.rs:294-746) computes
+    for its config. ``advance(n)`` steps every instance that is still active;
+    an instance whose time reached t_end, or whose step failed, stops and
+    reports its status through ``status(i)``.
+    """
+
+    def __init__(self, configs, autotune: bool = True, use_graph: bool = True):
+        if not configs:
+            raise SolverError("a batch needs at least one config", _abi.ERR_INVALID_ARGUMENT)
+        self.lib = _abi.load()
+        self.configs = list(configs)
+        arr = (_abi.CudaConfig * len(self.configs))()
+        for i, c in enumerate(self.configs):
+            arr[i] = c.to_c() if hasattr(c, "to_c") else c
+        flags = (_abi.BATCH_AUTOTUNE if autotune else 0) | (0 if use_graph else _abi.BATCH_NO_GRAPH)
+        h = C.c_void_p()
+        _check(self.lib, None, self.lib.flursys_cuda_batch_create(arr, len(self.configs), flags, C.byref(h)))
+        self.h = h
+
+    def __len__(self) -> int:
+        return len(self.configs)
+
+    def advance(self, nsteps: int = 1) -> None:
+        _check(self.lib, None, self.lib.flursys_cuda_batch_step(self.h, int(nsteps)))
+
+    def report(self, i: int) -> _abi.StepReport:
+        rep = _abi.StepReport()
+        st = C.c_int32()
+        _check(self.lib, None, self.lib.flursys_cuda_batch_report(self.h, i, C.byref(rep), C.byref(st)))
+        return rep
+
+    def status(self, i: int) -> int:
+        rep = _abi.StepReport()
+        st = C.c_int32()
+        _check(self.lib, None, self.lib.flursys_cuda_batch_report(self.h, i, C.byref(rep), C.byref(st)))
+        return int(st.value)
+
+    def step_report(self, i: int) -> SolverStep:
+        return SolverStep.from_report(self.report(i))
+
+    def field(self, i: int, name: str) -> np.ndarray:
+        cfg = self.configs[i]
+        nx, ny = cfg.nx, cfg.ny
+        fid = {"u": _abi.FIELD_U, "v": _abi.FIELD_V, "pressure": _abi.FIELD_PRESSURE, "rhs": _abi.FIELD_RHS,
+               "u_star": _abi.FIELD_U_STAR, "v_star": _abi.FIELD_V_STAR, "speed": _abi.FIELD_SPEED,
+               "vorticity": _abi.FIELD_VORTICITY, "u_cell": _abi.FIELD_U_CELL,
+               "v_cell": _abi.FIELD_V_CELL}[name]
+        n = {"u": (nx + 1) * ny, "v": nx * (ny + 1), "u_star": (nx + 1) * ny, "v_star": nx * (ny + 1)}.get(name, nx * ny)
+        out = np.empty(n, dtype=np.float64)
+        _check(self.lib, None, self.lib.flursys_cuda_batch_download(self.h, i, fid, _abi.dptr(out), n))
+        return out
+
+    def tuning(self) -> dict:
+        t = _abi.BatchTuning()
+        _check(self.lib, None, self.lib.flursys_cuda_batch_tuning(self.h, C.byref(t)))
+        return {"tile_elems": list(t.tile_elems), "pressure_blocks_per_sm": t.pressure_blocks_per_sm,
+                "pressure_blocks": t.pressure_blocks, "graph_nodes": t.graph_nodes, "tune_ms": t.tune_ms}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.flursys_cuda_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -335,6 +335,58 @@ int32_t flursys_cuda_stencil_pcg_noalloc(int64_t nx, int64_t ny, int64_t nz, dou
                                          const FlursysLinearSolverOptions *options,
                                          FlursysLinearSolveReport *report, void *stream);
 
+/* ---- Batched 2D solvers ---------------------------------------------------
+ * Many independent 2D projection solvers (one IncompressibleSolver,
+ * src/solver/incompressible.rs:294-746, per config) of uneven size advanced
+ * together on one device. No reference counterpart: the reference runs one
+ * solver per process; each instance here computes what that solver computes.
+ *
+ * Every config must be 2D, projection coupling, pressure solver PCG or SOR,
+ * and all configs must share one `precision`. Each instance keeps its own
+ * dt control (fixed dt, or adaptive_time_step :2308-2336), its own t_end and
+ * its own pressure-solver settings. One step of the batch is one captured
+ * CUDA graph: per instance the dt rule, momentum predictor, boundaries,
+ * pressure right-hand side, pressure solve (one cooperative launch over all
+ * instances, blocks shared out in proportion to cells x iterations of the
+ * previous step), correction and diagnostics. An instance that reaches t_end
+ * or fails stops stepping; the others go on. */
+typedef struct FlursysBatchHandle FlursysBatchHandle;
+
+enum FlursysBatchFlags {
+    FLURSYS_BATCH_AUTOTUNE = 1, /* time candidate tile sizes and pressure grids at create */
+    FLURSYS_BATCH_NO_GRAPH = 2  /* enqueue the kernels of each step directly (no graph) */
+};
+
+/* Tuned launch parameters (flursys_cuda_batch_tuning). */
+typedef struct FlursysBatchTuning {
+    int32_t tile_elems[6];      /* elements per tile: predict, boundaries, rhs, correct, boundaries, post */
+    int32_t pressure_blocks_per_sm;
+    int32_t pressure_blocks;    /* blocks of the cooperative pressure launch */
+    int32_t graph_nodes;        /* kernel nodes of one step's graph (0 without a graph) */
+    int32_t reserved;
+    double tune_ms;             /* host time spent tuning at create */
+} FlursysBatchTuning;
+
+int32_t flursys_cuda_batch_create(const FlursysCudaConfig *configs, int32_t count, int32_t flags,
+                                  FlursysBatchHandle **out);
+/* Advances every active instance by `nsteps` steps (instances that stop
+ * early stay put) and returns after the last one. FLURSYS_OK unless the
+ * device failed (FLURSYS_ERR_CUDA, FLURSYS_ERR_TIMEOUT); per-instance
+ * outcomes come from flursys_cuda_batch_report. */
+int32_t flursys_cuda_batch_step(FlursysBatchHandle *h, int64_t nsteps);
+/* Report of the last step `instance` took (SolverStep, :211-229) and its
+ * status: FLURSYS_OK while it steps, FLURSYS_ERR_REACHED_END_TIME once its
+ * time reached t_end, or the error that stopped it. step_ms is the mean
+ * device time of one batch step over the last flursys_cuda_batch_step call;
+ * pressure_solve_ms is 0 (the solve is shared by all instances). */
+int32_t flursys_cuda_batch_report(FlursysBatchHandle *h, int32_t instance, FlursysStepReport *report,
+                                  int32_t *instance_status);
+/* Copies field `field_id` (FlursysFieldId, 2D fields) of one instance. */
+int32_t flursys_cuda_batch_download(FlursysBatchHandle *h, int32_t instance, int32_t field_id, double *host,
+                                    size_t n);
+int32_t flursys_cuda_batch_tuning(const FlursysBatchHandle *h, FlursysBatchTuning *out);
+int32_t flursys_cuda_batch_destroy(FlursysBatchHandle *h);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
