@@ -326,8 +326,10 @@ def roofline(n_cells, its, solve_ms, precision):
     achieved = bytes_total / secs / 1e9
     traffic = None
     try:
-        t = json.load(open(TRAFFIC_FILE))
-        per_cell_it = t[precision]["dram_bytes_per_cell_iteration"]
+        t = json.load(open(TRAFFIC_FILE))[precision]
+        by_size = {int(k): v for k, v in t.get("by_size", {}).items()}
+        n = round(n_cells ** (1.0 / 3.0))
+        per_cell_it = by_size[min(by_size, key=lambda s: abs(s - n))] if by_size else t["dram_bytes_per_cell_iteration"]
         traffic = per_cell_it * n_cells * (sum(its) / len(its))
     except Exception:
         pass
