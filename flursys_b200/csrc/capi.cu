@@ -72,7 +72,8 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
     for (int s = 0; s < 4; ++s)
         if (c.overrides[s].kind < FLURSYS_BOUNDARY_CASE_DEFAULT || c.overrides[s].kind > FLURSYS_BOUNDARY_PRESSURE_OUTLET) { *msg = "unknown boundary override kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }
     if (c.nx < 4 || c.ny < 4) { *msg = "nx and ny must be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
-    if (c.nx > (1 << 20) || c.ny > (1 << 20)) { *msg = "grid dimension too large"; return FLURSYS_ERR_INVALID_CONFIG; }
+    // Device indices are 32-bit: the face arrays must stay below 2^31 entries.
+    if (c.nx > (1 << 20) || c.ny > (1 << 20) || (c.nx + 1) * (c.ny + 1) >= (1LL << 31)) { *msg = "grid dimension too large"; return FLURSYS_ERR_INVALID_CONFIG; }
     if (!fin_pos(c.dt)) { *msg = "dt must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
     if (!std::isfinite(c.t_end) || c.t_end < 0.0) { *msg = "t_end must be finite and non-negative"; return FLURSYS_ERR_INVALID_CONFIG; }
     if (c.coupling == FLURSYS_COUPLING_PROJECTION && c.t_end == 0.0) { *msg = "t_end must be positive for projection coupling"; return FLURSYS_ERR_INVALID_CONFIG; }

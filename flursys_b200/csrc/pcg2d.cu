@@ -38,17 +38,37 @@ namespace {
 constexpr int kBlock = 256;
 constexpr int kParts = 8;
 
-__device__ __forceinline__ bool solid(const uint8_t *f, long long c) { return (f[c] & kCellSolid) != 0; }
-__device__ __forceinline__ bool ident(const uint8_t *f, long long c) { return (f[c] & 3) != 0; }
+__device__ __forceinline__ bool solid(const uint8_t *f, int c) { return (f[c] & kCellSolid) != 0; }
+__device__ __forceinline__ bool ident(const uint8_t *f, int c) { return (f[c] & 3) != 0; }
 
 struct Ctx {
     Pcg2dInstance in;
     int lb;  // block index within the instance
-    long long n, c_begin, c_end;
+    int n, c_begin, c_end;
+    int step_i, step_j;  // kBlock cells = step_j rows + step_i columns
 };
 
+// A thread's walk over the cells of its block: c advances by kBlock and
+// (i, j) follow without a division per cell.
+struct CellIter {
+    int c, i, j;
+};
+__device__ __forceinline__ CellIter first_cell(const Ctx &k) {
+    const int c = k.c_begin + (int)threadIdx.x;
+    return CellIter{c, c % k.in.nx, c / k.in.nx};
+}
+__device__ __forceinline__ void next_cell(const Ctx &k, CellIter &it) {
+    it.c += kBlock;
+    it.i += k.step_i;
+    it.j += k.step_j;
+    if (it.i >= k.in.nx) {
+        it.i -= k.in.nx;
+        ++it.j;
+    }
+}
+
 // Diagonal of a fluid row.
-__device__ __forceinline__ double diag2(const Ctx &k, long long c, int i, int j) {
+__device__ __forceinline__ double diag2(const Ctx &k, int c, int i, int j) {
     const uint8_t *f = k.in.flags;
     double d = 0.0;
     if (i + 1 < k.in.nx && !solid(f, c + 1)) d += k.in.idx2;
@@ -60,7 +80,7 @@ __device__ __forceinline__ double diag2(const Ctx &k, long long c, int i, int j)
 
 // (A v)_c for a fluid row with `val(nb)` giving the operand.
 template <typename T, typename F>
-__device__ __forceinline__ T apply_row(const Ctx &k, long long c, int i, int j, T vc, F val) {
+__device__ __forceinline__ T apply_row(const Ctx &k, int c, int i, int j, T vc, F val) {
     const uint8_t *f = k.in.flags;
     const T wx = T(k.in.idx2), wy = T(k.in.idy2);
     T dg = T(0), s = T(0);
@@ -106,7 +126,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     const double cnt = in.count_fluid > 0 ? double(in.count_fluid) : 1.0;
     const unsigned nb = in.nblocks;
     const int nx = in.nx;
-    auto bval = [&](long long c) -> double {  // b of the system (before projection)
+    auto bval = [&](int c) -> double {  // b of the system (before projection)
         const uint8_t fc = f[c];
         if (fc & kCellOutlet) return in.outlet_pressure;
         if (fc & kCellSolid) return 0.0;
@@ -122,7 +142,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     // ---- I1: identity rows take their fixed values; sums of x and b ----
     {
         double sx = 0.0, sb = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+        for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
             const uint8_t fc = f[c];
             if (fc & 3) {
                 x[c] = (fc & kCellOutlet) ? in.outlet_pressure : 0.0;
@@ -138,7 +158,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     double mx = proj ? read_sum(k, 0, red) / cnt : 0.0;
     mb = proj ? read_sum(k, 1, red) / cnt : 0.0;
     if (proj) {
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
+        for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
             if (!ident(f, c)) x[c] -= mx;
         if (!grid_sync(in.barrier, nb)) return;
     }
@@ -146,11 +166,11 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     // ---- r = b' - A x (FP64), projected; residual; z; r.z ----
     auto residual_pass = [&]() -> bool {
         double sr = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-            const int j = int(c / nx), i = int(c - (long long)j * nx);
+        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+            const int c = it.c, i = it.i, j = it.j;
             double rv = 0.0;
             if (!ident(f, c)) {
-                rv = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](long long m) { return x[m]; });
+                rv = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](int m) { return x[m]; });
                 sr += rv;
             }
             r[c] = V(rv);
@@ -160,8 +180,8 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         if (!grid_sync(in.barrier, nb)) return false;
         const double mr = proj ? read_sum(k, 0, red) / cnt : 0.0;
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-            const int j = int(c / nx), i = int(c - (long long)j * nx);
+        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+            const int c = it.c, i = it.i, j = it.j;
             double rv = double(r[c]);
             double zv = rv;
             if (!ident(f, c)) {
@@ -210,14 +230,14 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         V *dcur = dbuf[it & 1];
         const V *dold = dbuf[(it + 1) & 1];
         // ---- pass 1: direction + stencil ----
-        auto dn = [&](long long m) -> V {
+        auto dn = [&](int m) -> V {
             if (ident(f, m)) return V(0);
             const double zm = double(z[m]) - mz;
             return first ? V(zm) : V(zm + beta * (double(dold[m]) - md_old));
         };
         double s_dq = 0.0, s_q = 0.0, s_d = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-            const int j = int(c / nx), i = int(c - (long long)j * nx);
+        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+            const int c = it.c, i = it.i, j = it.j;
             const V dc = dn(c);
             V qc = dc;
             if (!ident(f, c)) {
@@ -244,7 +264,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         double mr = 0.0;
         if (proj) {
             double s_x = 0.0, s_r = 0.0;
-            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+            for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
                 if (ident(f, c)) continue;
                 const double dc = double(dcur[c]) - md;
                 const double xv = x[c] + alpha * dc;
@@ -262,8 +282,8 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         // ---- pass 3: projection, residual, z, r.z ----
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-            const int j = int(c / nx), i = int(c - (long long)j * nx);
+        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+            const int c = it.c, i = it.i, j = it.j;
             double rv;
             double zv;
             if (ident(f, c)) {
@@ -316,10 +336,10 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     // ---- final FP64 check ||b' - A x||_2 over fluid rows ----
     if (!grid_sync(in.barrier, nb)) return;
     double s_true = 0.0;
-    for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+    for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+        const int c = it.c, i = it.i, j = it.j;
         if (ident(f, c)) continue;
-        const int j = int(c / nx), i = int(c - (long long)j * nx);
-        const double t = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](long long m) { return x[m]; });
+        const double t = bval(c) - mb - apply_row<double>(k, c, i, j, x[c], [&](int m) { return x[m]; });
         s_true += t * t;
     }
     {
@@ -353,8 +373,8 @@ __device__ void sor_instance(Ctx &k, double *red) {
     for (long long it = 0; it < in.max_iters; ++it) {
         its = it + 1;
         for (int color = 0; color < 2; ++color) {
-            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-                const int j = int(c / nx), i = int(c - (long long)j * nx);
+            for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+                const int c = it.c, i = it.i, j = it.j;
                 if (((i + j) & 1) != color) continue;
                 const uint8_t fc = f[c];
                 if (fc & kCellSolid) { p[c] = 0.0; continue; }
@@ -374,14 +394,14 @@ __device__ void sor_instance(Ctx &k, double *red) {
         if (in.project && in.ref_cell >= 0) {
             const double pr = p[in.ref_cell];
             if (!grid_sync(in.barrier, nb)) return;
-            for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
+            for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
                 if (!solid(f, c)) p[c] -= pr;
             if (!grid_sync(in.barrier, nb)) return;
         }
         double m = 0.0;
-        for (long long c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+            const int c = it.c, i = it.i, j = it.j;
             if (ident(f, c)) continue;
-            const int j = int(c / nx), i = int(c - (long long)j * nx);
             const double p0 = p[c];
             const double pe = (i + 1 < nx && !solid(f, c + 1)) ? p[c + 1] : p0;
             const double pw = (i > 0 && !solid(f, c - 1)) ? p[c - 1] : p0;
@@ -410,7 +430,7 @@ __device__ void sor_instance(Ctx &k, double *red) {
 }
 
 template <typename V, bool MIXED>
-__global__ void __launch_bounds__(kBlock) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
+__global__ void __launch_bounds__(kBlock, 4) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
     __shared__ double red[kBlock / 32];
     int id = 0;
     for (int t = 0; t < ninst; ++t)
@@ -419,10 +439,12 @@ __global__ void __launch_bounds__(kBlock) pcg2d_kernel(const Pcg2dInstance *__re
     k.in = insts[id];
     k.lb = (int)blockIdx.x - k.in.block0;
     if (k.lb >= k.in.nblocks) return;  // spare block of the launch
-    k.n = (long long)k.in.nx * k.in.ny;
-    const long long chunk = (k.n + k.in.nblocks - 1) / k.in.nblocks;
-    k.c_begin = (long long)k.lb * chunk;
+    k.n = k.in.nx * k.in.ny;
+    const int chunk = (k.n + k.in.nblocks - 1) / k.in.nblocks;
+    k.c_begin = k.lb * chunk;
     k.c_end = k.c_begin + chunk < k.n ? k.c_begin + chunk : k.n;
+    k.step_j = kBlock / k.in.nx;
+    k.step_i = kBlock - k.step_j * k.in.nx;
     if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red);
     else pcg_instance<V, MIXED>(k, red);
 }
