@@ -182,6 +182,20 @@ class BatchTuning(C.Structure):
 
 
 BATCH_AUTOTUNE, BATCH_NO_GRAPH = 1, 2
+FCG_LOSS_ENERGY, FCG_LOSS_RESIDUAL = 0, 1
+
+
+class FcgReport(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("fallback", C.c_int32),
+        ("fcg_iterations", C.c_int64),
+        ("pcg_iterations", C.c_int64),
+        ("initial_residual", C.c_double),
+        ("final_residual", C.c_double),
+        ("relative_residual", C.c_double),
+        ("net_ms", C.c_double),
+    ]
 
 # Every extern "C" entry point of include/flursys_cuda.h: (restype, argtypes).
 _P = C.c_void_p
@@ -216,6 +230,20 @@ SIGNATURES = {
                                                      C.c_double, _P, _P, C.c_int32,
                                                      C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport),
                                                      _P]),
+    "flursys_cuda_fcgnet_param_count": (C.c_int64, []),
+    "flursys_cuda_fcgnet_create": (C.c_int32, [C.POINTER(C.c_float), C.POINTER(_P)]),
+    "flursys_cuda_fcgnet_load": (C.c_int32, [C.c_char_p, C.POINTER(_P)]),
+    "flursys_cuda_fcgnet_set_params": (C.c_int32, [_P, _P, _P]),
+    "flursys_cuda_fcgnet_get_params": (C.c_int32, [_P, C.POINTER(C.c_float), C.c_int64]),
+    "flursys_cuda_fcgnet_apply": (C.c_int32, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P, _P]),
+    "flursys_cuda_fcgnet_train_sample": (C.c_int32, [_P, C.c_int64, C.c_int64, C.c_int64, _P, _P, C.c_double,
+                                                     C.c_int32, _P, _P, _P]),
+    "flursys_cuda_fcgnet_adam": (C.c_int32, [_P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float,
+                                             C.c_int64, C.c_float, _P]),
+    "flursys_cuda_fcgnet_destroy": (C.c_int32, [_P]),
+    "flursys_cuda_stencil_fcg": (C.c_int32, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                             C.c_double, _D, _D, C.POINTER(LinearSolverOptions),
+                                             C.POINTER(FcgReport)]),
     "flursys_cuda_batch_create": (C.c_int32, [C.POINTER(CudaConfig), C.c_int32, C.c_int32, C.POINTER(_P)]),
     "flursys_cuda_batch_step": (C.c_int32, [_P, C.c_int64]),
     "flursys_cuda_batch_report": (C.c_int32, [_P, C.c_int32, C.POINTER(StepReport), C.POINTER(C.c_int32)]),

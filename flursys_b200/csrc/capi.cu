@@ -68,6 +68,7 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
         return FLURSYS_OK;
     }
     if (c.dimension != 2) { *msg = "dimension must be 2 or 3"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.pressure_solver == FLURSYS_PRESSURE_FCG) { *msg = "the learned FCG pressure solver is 3D only"; return FLURSYS_ERR_UNSUPPORTED; }
     if (c.case_params.kind < FLURSYS_CASE_CAVITY || c.case_params.kind > FLURSYS_CASE_CHANNEL) { *msg = "unknown case kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }
     for (int s = 0; s < 4; ++s)
         if (c.overrides[s].kind < FLURSYS_BOUNDARY_CASE_DEFAULT || c.overrides[s].kind > FLURSYS_BOUNDARY_PRESSURE_OUTLET) { *msg = "unknown boundary override kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }

@@ -57,6 +57,9 @@ struct FlursysCudaHandle {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // 2D state
     flursys::Handle2D *h2 = nullptr;
+    // 3D learned-preconditioner FCG (pressure_solver == FLURSYS_PRESSURE_FCG)
+    FlursysFcgNet *fcg_net = nullptr;
+    FlursysFcgReport fcg_report{};
 };
 
 namespace flursys {
@@ -102,6 +105,15 @@ int32_t run_pcg3d(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy
                   long long max_iters, int replace_every, cudaStream_t stream, std::string *err);
 // Maps a finished PcgResultDev to a status and message.
 int32_t pcg_result_status(const PcgResultDev &r, std::string *err);
+// Learned-preconditioner FCG on device buffers x (FP64, in/out) and rhs
+// (A x = -rhs on the pinned 3D system); fallback Jacobi-PCG in
+// `precision_fallback`.
+int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
+                  const double *rhs, double atol, double rtol, long long max_iters, int precision_fallback,
+                  cudaStream_t st, FlursysFcgReport *rep, std::string *err);
+int32_t fcgnet_read_file(const char *path, std::vector<float> *out, std::string *err);
+int32_t fcgnet_create(const float *host_params, FlursysFcgNet **out, std::string *err);
+void fcgnet_destroy(FlursysFcgNet *net);
 // Fills the argument block of a 3D pressure solve on the workspace buffers.
 Pcg3dArgs make_pcg3d_args(PcgWorkspace &ws, int nx, int ny, int nz, double dx, double dy, double dz, double *x,
                           const double *rhs, int precision, int stop_rule, double tol, double atol, double rtol,

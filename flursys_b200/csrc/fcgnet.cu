@@ -1,0 +1,706 @@
+// fcgnet.cu — kernels of the learned FCG preconditioner (fcgnet.cuh):
+// forward, backward and Adam, hand-written for sm_100a.
+//
+//   conv_tc<CIN, COUT, MODE>  3x3x3 convolution as an implicit GEMM on the
+//       tensor cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation):
+//       M = 16 voxels along x per warp, N = COUT, K = 27 taps x CIN. A block
+//       covers 16 x 8 voxels of one z plane; for each of the three input
+//       planes it stages the 18 x 10 halo tile and the 9 taps' weights in
+//       shared memory (rows padded by 8 BF16 so the fragment loads hit 32
+//       distinct banks). MODE fuses the input transform into the staging:
+//       PLAIN reads the tensor, POOL averages 2x2x2 cells of the finer level,
+//       UPADD adds the nearest-neighbour upsampled coarser tensor to a skip
+//       tensor — with the same FP32 sums and BF16 rounding as the separate
+//       pool / up_add kernels, so fused and unfused paths agree bit for bit.
+//   conv_first  1 -> 16 channels (FP32 input, CUDA cores)
+//   conv_last   16 -> 1 channel (FP32 output, CUDA cores, staged tile)
+//   wgrad       dW[co][tap][ci] += sum_v dY[v][co] X[v + tap][ci] (CUDA cores,
+//               FP32, atomics per voxel chunk)
+// The data gradient of a layer is the forward convolution with the
+// transposed, flipped weights (NetWeights::bwd), so conv_tc serves both.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "fcgnet.cuh"
+
+namespace flursys {
+
+namespace {
+
+constexpr int kTX = 16, kTY = 8;              // conv tile: 16 x 8 voxels of one plane
+constexpr int kHX = kTX + 2, kHY = kTY + 2;   // with the 1-cell halo
+constexpr int kConvThreads = 32 * kTY;        // one warp per tile row
+constexpr int kPad = 8;                       // BF16 padding of a staged row
+
+enum StageMode { kPlain = 0, kPool = 1, kUpAdd = 2 };
+
+__device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
+__device__ __forceinline__ uint16_t f2bf(float f) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(f);
+    return *reinterpret_cast<const uint16_t *>(&h);
+}
+
+// Eight channels of one voxel of a stage source, as FP32.
+struct Src {
+    const uint16_t *in;      // PLAIN: the tensor; POOL: the finer tensor; UPADD: the skip tensor
+    const uint16_t *coarse;  // UPADD: the coarser tensor
+};
+
+// 2x2x2 mean of the finer level (dims 2nx, 2ny, 2nz), channels k8*8..+7.
+template <int C>
+__device__ __forceinline__ void pool8(const uint16_t *fine, int x, int y, int z, int nx, int ny, int k8, float v[8]) {
+    const int fx = 2 * nx, fy = 2 * ny;
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = 0.f;
+    #pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const long long vox = ((long long)(2 * z + (a >> 2)) * fy + (2 * y + ((a >> 1) & 1))) * fx + (2 * x + (a & 1));
+        const uint4 q = *reinterpret_cast<const uint4 *>(fine + vox * C + k8 * 8);
+        const uint16_t *h = reinterpret_cast<const uint16_t *>(&q);
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] += bf2f(h[c]);
+    }
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] *= 0.125f;
+}
+
+// up(coarse) + skip at (x, y, z), channels k8*8..+7.
+template <int C>
+__device__ __forceinline__ void upadd8(const uint16_t *coarse, const uint16_t *skip, int x, int y, int z, int nx,
+                                       int ny, int k8, float v[8]) {
+    const int cx = nx >> 1, cy = ny >> 1;
+    const long long cv = ((long long)(z >> 1) * cy + (y >> 1)) * cx + (x >> 1);
+    const long long fv = ((long long)z * ny + y) * nx + x;
+    const uint4 a = *reinterpret_cast<const uint4 *>(coarse + cv * C + k8 * 8);
+    const uint4 b = *reinterpret_cast<const uint4 *>(skip + fv * C + k8 * 8);
+    const uint16_t *ha = reinterpret_cast<const uint16_t *>(&a);
+    const uint16_t *hb = reinterpret_cast<const uint16_t *>(&b);
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) v[c] = bf2f(ha[c]) + bf2f(hb[c]);
+}
+
+// Eight BF16 channels of voxel (x, y, z) of the staged input (zero outside).
+template <int C, int MODE>
+__device__ __forceinline__ uint4 load8(const Src &s, int x, int y, int z, int nx, int ny, int nz, int k8) {
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return make_uint4(0, 0, 0, 0);
+    if (MODE == kPlain) return *reinterpret_cast<const uint4 *>(s.in + (((long long)z * ny + y) * nx + x) * C + k8 * 8);
+    float v[8];
+    if (MODE == kPool) pool8<C>(s.in, x, y, z, nx, ny, k8, v);
+    else upadd8<C>(s.coarse, s.in, x, y, z, nx, ny, k8, v);
+    uint4 q;
+    uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) h[c] = f2bf(v[c]);
+    return q;
+}
+
+// Stages the 18 x 10 halo tile of plane z (row stride C + kPad).
+template <int C, int MODE>
+__device__ __forceinline__ void stage_tile(uint16_t *sIn, const Src &s, int x0, int y0, int z, int nx, int ny, int nz) {
+    constexpr int K8 = C / 8;
+    for (int idx = threadIdx.x; idx < kHY * kHX * K8; idx += blockDim.x) {
+        const int k8 = idx % K8, cell = idx / K8;
+        const int cx = cell % kHX, cy = cell / kHX;
+        const uint4 q = load8<C, MODE>(s, x0 - 1 + cx, y0 - 1 + cy, z, nx, ny, nz, k8);
+        *reinterpret_cast<uint4 *>(sIn + (cy * kHX + cx) * (C + kPad) + k8 * 8) = q;
+    }
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int CIN, int COUT>
+constexpr int conv_smem_bytes() {
+    return (kHY * kHX * (CIN + kPad) + 9 * COUT * (CIN + kPad)) * 2;
+}
+
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kConvThreads) conv_tc(Src src, const uint16_t *__restrict__ W, uint16_t *out, int nx,
+                                                        int ny, int nz) {
+    extern __shared__ __align__(16) uint16_t smem[];
+    uint16_t *sIn = smem;
+    uint16_t *sW = smem + kHY * kHX * (CIN + kPad);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tig = lane & 3;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z = blockIdx.z;
+    float acc[COUT / 8][4];
+    #pragma unroll
+    for (int n = 0; n < COUT / 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+
+    for (int dz = 0; dz < 3; ++dz) {
+        __syncthreads();
+        stage_tile<CIN, MODE>(sIn, src, x0, y0, z + dz - 1, nx, ny, nz);
+        constexpr int K8 = CIN / 8;
+        for (int idx = threadIdx.x; idx < 9 * COUT * K8; idx += blockDim.x) {
+            const int k8 = idx % K8, rest = idx / K8;
+            const int co = rest % COUT, t9 = rest / COUT;
+            const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + dz * 9 + t9) * CIN + k8 * 8);
+            *reinterpret_cast<uint4 *>(sW + (t9 * COUT + co) * (CIN + kPad) + k8 * 8) = q;
+        }
+        __syncthreads();
+        #pragma unroll 1
+        for (int t9 = 0; t9 < 9; ++t9) {
+            const int dy = t9 / 3, dx = t9 % 3;  // halo-relative offsets 0..2
+            const uint16_t *rowA = sIn + ((warp + dy) * kHX + dx) * (CIN + kPad);
+            const uint16_t *wt = sW + t9 * COUT * (CIN + kPad);
+            #pragma unroll
+            for (int kc = 0; kc < CIN; kc += 16) {
+                const uint32_t a0 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + tig * 2);
+                const uint32_t a1 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + tig * 2);
+                const uint32_t a2 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + 8 + tig * 2);
+                const uint32_t a3 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + 8 + tig * 2);
+                #pragma unroll
+                for (int n = 0; n < COUT / 8; ++n) {
+                    const uint16_t *wb = wt + (n * 8 + g) * (CIN + kPad) + kc + tig * 2;
+                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
+                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
+                    mma_bf16(acc[n], a0, a1, a2, a3, b0, b1);
+                }
+            }
+        }
+    }
+    const int y = y0 + warp;
+    if (y >= ny) return;
+    #pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int x = x0 + g + 8 * h;
+        if (x >= nx) continue;
+        uint16_t *o = out + (((long long)z * ny + y) * nx + x) * COUT;
+        #pragma unroll
+        for (int n = 0; n < COUT / 8; ++n) {
+            const uint32_t pk = uint32_t(f2bf(acc[n][2 * h])) | (uint32_t(f2bf(acc[n][2 * h + 1])) << 16);
+            *reinterpret_cast<uint32_t *>(o + n * 8 + tig * 2) = pk;
+        }
+    }
+}
+
+// 1 -> 16 channels: out[v][co] = sum_tap W[co][tap] * scale * in[v + tap].
+// scale = *scale_ptr (input normalisation) or 1 when scale_ptr is null.
+__global__ void __launch_bounds__(256) conv_first(const float *__restrict__ in, const float *__restrict__ W,
+                                                  const double *scale_ptr, uint16_t *out, float *scaled_copy, int nx,
+                                                  int ny, int nz) {
+    __shared__ float sw[16 * 27];
+    for (int i = threadIdx.x; i < 16 * 27; i += blockDim.x) sw[i] = W[i];
+    __syncthreads();
+    const float scale = scale_ptr ? float(scale_ptr[0]) : 1.f;
+    const long long n = (long long)nx * ny * nz;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const int x = int(v % nx);
+        const long long t = v / nx;
+        const int y = int(t % ny), z = int(t / ny);
+        float acc[16];
+        #pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+        #pragma unroll
+        for (int tap = 0; tap < 27; ++tap) {
+            const int xx = x + tap % 3 - 1, yy = y + (tap / 3) % 3 - 1, zz = z + tap / 9 - 1;
+            if (xx < 0 || yy < 0 || zz < 0 || xx >= nx || yy >= ny || zz >= nz) continue;
+            const float r = in[((long long)zz * ny + yy) * nx + xx] * scale;
+            #pragma unroll
+            for (int c = 0; c < 16; ++c) acc[c] = fmaf(sw[c * 27 + tap], r, acc[c]);
+        }
+        uint4 q[2];
+        uint16_t *h = reinterpret_cast<uint16_t *>(q);
+        #pragma unroll
+        for (int c = 0; c < 16; ++c) h[c] = f2bf(acc[c]);
+        uint4 *o = reinterpret_cast<uint4 *>(out + v * 16);
+        o[0] = q[0];
+        o[1] = q[1];
+        if (scaled_copy) scaled_copy[v] = in[v] * scale;
+    }
+}
+
+// 16 -> 1 channel with an FP32 output: out[v] = out_scale * sum W[tap][ci] x[v+tap][ci].
+// out_scale = h2 / scale (input normalisation undone), or 1 without scale_ptr.
+// The pinned cell 0 is written as 0 when pin0 is set.
+template <int MODE>
+__global__ void __launch_bounds__(kTX * kTY) conv_last(Src src, const float *__restrict__ W, const double *scale_ptr,
+                                                       double h2, float *out, int nx, int ny, int nz, int pin0) {
+    __shared__ __align__(16) uint16_t sIn[3][kHY * kHX * (16 + kPad)];
+    __shared__ float sw[27 * 16];
+    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) sw[i] = W[i];
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z = blockIdx.z;
+    for (int p = 0; p < 3; ++p) stage_tile<16, MODE>(sIn[p], src, x0, y0, z + p - 1, nx, ny, nz);
+    __syncthreads();
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= nx || y >= ny) return;
+    float acc = 0.f;
+    #pragma unroll 1
+    for (int tap = 0; tap < 27; ++tap) {
+        const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
+        const uint16_t *c = sIn[dz] + ((ty + dy) * kHX + tx + dx) * (16 + kPad);
+        #pragma unroll
+        for (int k = 0; k < 16; ++k) acc = fmaf(sw[tap * 16 + k], bf2f(c[k]), acc);
+    }
+    double s = 1.0;
+    if (scale_ptr) s = scale_ptr[0] > 0.0 ? h2 / scale_ptr[0] : 0.0;
+    const long long v = ((long long)z * ny + y) * nx + x;
+    out[v] = (pin0 && v == 0) ? 0.f : float(double(acc) * s);
+}
+
+// Mean (factor 0.125) or sum (factor 1) of 2x2x2 fine cells into the coarse level.
+template <int C>
+__global__ void pool_kernel(const uint16_t *fine, uint16_t *coarse, int cx, int cy, int cz, float factor) {
+    const long long n = (long long)cx * cy * cz * (C / 8);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int k8 = int(i % (C / 8));
+        const long long v = i / (C / 8);
+        const int x = int(v % cx);
+        const long long t = v / cx;
+        const int y = int(t % cy), z = int(t / cy);
+        float s[8];
+        pool8<C>(fine, x, y, z, cx, cy, k8, s);  // s = mean
+        uint4 q;
+        uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) h[c] = f2bf(factor == 0.125f ? s[c] : s[c] * 8.f * factor);
+        *reinterpret_cast<uint4 *>(coarse + v * C + k8 * 8) = q;
+    }
+}
+
+// out = up(coarse) + skip, or (accumulate) skip += factor * up(coarse) in place.
+template <int C>
+__global__ void upadd_kernel(const uint16_t *coarse, const uint16_t *skip, uint16_t *out, int nx, int ny, int nz,
+                             float factor, int accumulate) {
+    const long long n = (long long)nx * ny * nz * (C / 8);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int k8 = int(i % (C / 8));
+        const long long v = i / (C / 8);
+        const int x = int(v % nx);
+        const long long t = v / nx;
+        const int y = int(t % ny), z = int(t / ny);
+        float s[8];
+        if (!accumulate) {
+            upadd8<C>(coarse, skip, x, y, z, nx, ny, k8, s);
+        } else {
+            const long long cv = ((long long)(z >> 1) * (ny >> 1) + (y >> 1)) * (nx >> 1) + (x >> 1);
+            const uint4 a = *reinterpret_cast<const uint4 *>(coarse + cv * C + k8 * 8);
+            const uint4 b = *reinterpret_cast<const uint4 *>(skip + v * C + k8 * 8);
+            const uint16_t *ha = reinterpret_cast<const uint16_t *>(&a);
+            const uint16_t *hb = reinterpret_cast<const uint16_t *>(&b);
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) s[c] = bf2f(hb[c]) + factor * bf2f(ha[c]);
+        }
+        uint4 q;
+        uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) h[c] = f2bf(s[c]);
+        *reinterpret_cast<uint4 *>(out + v * C + k8 * 8) = q;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ float ld(const T *p, long long i);
+template <>
+__device__ __forceinline__ float ld<float>(const float *p, long long i) { return p[i]; }
+template <>
+__device__ __forceinline__ float ld<uint16_t>(const uint16_t *p, long long i) { return bf2f(p[i]); }
+
+constexpr int kWgradChunk = 1024;
+
+// dW[co][tap][ci] += sum over a chunk of voxels v of dY[v][co] * X[v + tap][ci].
+template <typename TX, typename TY>
+__global__ void __launch_bounds__(256) wgrad_kernel(const TX *X, const TY *dY, float *dW, int cin, int cout, int nx,
+                                                    int ny, int nz) {
+    const int per = 27 * cin;
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= cout * per) return;
+    const int co = o / per, rem = o - co * per, tap = rem / cin, ci = rem - tap * cin;
+    const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+    const long long n = (long long)nx * ny * nz;
+    const long long v0 = (long long)blockIdx.y * kWgradChunk;
+    const long long v1 = v0 + kWgradChunk < n ? v0 + kWgradChunk : n;
+    int x = int(v0 % nx);
+    long long t = v0 / nx;
+    int y = int(t % ny), z = int(t / ny);
+    float acc = 0.f;
+    for (long long v = v0; v < v1; ++v) {
+        const int xx = x + dx, yy = y + dy, zz = z + dz;
+        if (xx >= 0 && yy >= 0 && zz >= 0 && xx < nx && yy < ny && zz < nz)
+            acc = fmaf(ld(dY, v * cout + co), ld(X, (((long long)zz * ny + yy) * nx + xx) * cin + ci), acc);
+        if (++x == nx) {
+            x = 0;
+            if (++y == ny) { y = 0; ++z; }
+        }
+    }
+    atomicAdd(dW + o, acc);
+}
+
+// Energy-norm loss of e = out - p_hat on the unit-spacing Neumann operator L:
+// gout = 2 L e / norm, loss += e . L e / norm.
+__device__ __forceinline__ float neumann_apply(const float *v, int x, int y, int z, int nx, int ny, int nz) {
+    const long long c = ((long long)z * ny + y) * nx + x;
+    const long long sy = nx, sz = (long long)nx * ny;
+    const float e = v[c];
+    float q = 0.f;
+    if (x > 0) q += e - v[c - 1];
+    if (x + 1 < nx) q += e - v[c + 1];
+    if (y > 0) q += e - v[c - sy];
+    if (y + 1 < ny) q += e - v[c + sy];
+    if (z > 0) q += e - v[c - sz];
+    if (z + 1 < nz) q += e - v[c + sz];
+    return q;
+}
+
+// e = out - p_hat into err_out (the loss kernels read e at the neighbours).
+__global__ void __launch_bounds__(256) loss_err(const float *out, const float *p_hat, float *err_out, long long n) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        err_out[v] = out[v] - p_hat[v];
+}
+
+__global__ void __launch_bounds__(256) loss_kernel(const float *e, float *gout, double inv_norm, double *loss, int nx,
+                                                   int ny, int nz) {
+    __shared__ double red[8];
+    const long long n = (long long)nx * ny * nz;
+    double part = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const int x = int(v % nx);
+        const long long t = v / nx;
+        const int y = int(t % ny), z = int(t / ny);
+        const float q = neumann_apply(e, x, y, z, nx, ny, nz);
+        gout[v] = float(2.0 * double(q) * inv_norm);
+        part += double(e[v]) * double(q);
+    }
+    part = block_sum<256>(part, red);
+    if (threadIdx.x == 0) atomicAdd(loss, part * inv_norm);
+}
+
+// Residual-norm loss, first pass: q = L e into lq, loss += q.q / norm.
+__global__ void __launch_bounds__(256) loss_res_kernel(const float *e, float *lq, double inv_norm, double *loss, int nx,
+                                                       int ny, int nz) {
+    __shared__ double red[8];
+    const long long n = (long long)nx * ny * nz;
+    double part = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const int x = int(v % nx);
+        const long long t = v / nx;
+        const int y = int(t % ny), z = int(t / ny);
+        const float q = neumann_apply(e, x, y, z, nx, ny, nz);
+        lq[v] = q;
+        part += double(q) * double(q);
+    }
+    part = block_sum<256>(part, red);
+    if (threadIdx.x == 0) atomicAdd(loss, part * inv_norm);
+}
+
+// Residual-norm loss, second pass: gout = 2 L q / norm (L is symmetric).
+__global__ void __launch_bounds__(256) loss_res_grad(const float *lq, float *gout, double inv_norm, int nx, int ny,
+                                                     int nz) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const int x = int(v % nx);
+        const long long t = v / nx;
+        const int y = int(t % ny), z = int(t / ny);
+        gout[v] = float(2.0 * double(neumann_apply(lq, x, y, z, nx, ny, nz)) * inv_norm);
+    }
+}
+
+// Sum of squares of r into per-block partials; the finalizer turns the total
+// into the normalisation scale 1 / rms(r) (0 for r = 0).
+__global__ void __launch_bounds__(256) sumsq_kernel(const float *r, long long n, double *partials) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double x = r[i];
+        s += x * x;
+    }
+    s = block_sum<256>(s, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+__global__ void __launch_bounds__(256) scale_kernel(const double *partials, int np, long long n, double *scale) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum<256>(s, red);
+    if (threadIdx.x == 0) scale[0] = s > 0.0 ? sqrt(double(n) / s) : 0.0;
+}
+
+__global__ void pack_kernel(const float *master, uint16_t *fwd, uint16_t *bwd, float *f32, long long total) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int cins[kNetLayers] = {1, 16, 32, 64, 64, 32, 16};   // kNetCin
+        const int couts[kNetLayers] = {16, 32, 64, 64, 32, 16, 1};  // kNetCout
+        int layer = 0;
+        long long off = 0;
+        while (layer < kNetLayers - 1 && i >= off + 27LL * cins[layer] * couts[layer]) {
+            off += 27LL * cins[layer] * couts[layer];
+            ++layer;
+        }
+        const int cin = cins[layer], cout = couts[layer];
+        const long long loc = i - off;
+        const int co = int(loc / (27 * cin)), rem = int(loc % (27 * cin)), tap = rem / cin, ci = rem % cin;
+        const float w = master[i];
+        fwd[i] = f2bf(w);
+        bwd[off + ((long long)ci * 27 + (26 - tap)) * cout + co] = f2bf(w);
+        if (layer == 0) f32[co * 27 + tap] = w;                      // c1 as [16][27]
+        if (layer == kNetLayers - 1) {
+            f32[432 + tap * 16 + ci] = w;                            // c7 as [27][16]
+            f32[864 + ci * 27 + (26 - tap)] = w;                     // c7 transposed as [16][27]
+        }
+    }
+}
+
+__global__ void adam_kernel(float *w, const float *g, float *m, float *v, long long n, float lr, float b1, float b2,
+                            float eps, float c1, float c2, float gs) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i] * gs;
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+int grid_1d(long long n, int per = 256) { return (int)std::max<long long>(1, std::min<long long>((n + per - 1) / per, 148LL * 16)); }
+
+template <int CIN, int COUT, int MODE>
+cudaError_t launch_conv(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
+    constexpr int smem = conv_smem_bytes<CIN, COUT>();
+    static bool configured = false;  // per instantiation; set once per process
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(conv_tc<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
+    conv_tc<CIN, COUT, MODE><<<grid, kConvThreads, smem, st>>>(s, W, out, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+template <int C>
+cudaError_t launch_pool(const uint16_t *fine, uint16_t *coarse, int cx, int cy, int cz, float factor, cudaStream_t st) {
+    pool_kernel<C><<<grid_1d((long long)cx * cy * cz * (C / 8)), 256, 0, st>>>(fine, coarse, cx, cy, cz, factor);
+    return cudaGetLastError();
+}
+cudaError_t pool_any(int c, const uint16_t *fine, uint16_t *coarse, int cx, int cy, int cz, float factor, cudaStream_t st) {
+    switch (c) {
+        case 16: return launch_pool<16>(fine, coarse, cx, cy, cz, factor, st);
+        case 32: return launch_pool<32>(fine, coarse, cx, cy, cz, factor, st);
+        default: return launch_pool<64>(fine, coarse, cx, cy, cz, factor, st);
+    }
+}
+template <int C>
+cudaError_t launch_upadd(const uint16_t *coarse, const uint16_t *skip, uint16_t *out, int nx, int ny, int nz,
+                         float factor, int acc, cudaStream_t st) {
+    upadd_kernel<C><<<grid_1d((long long)nx * ny * nz * (C / 8)), 256, 0, st>>>(coarse, skip, out, nx, ny, nz, factor, acc);
+    return cudaGetLastError();
+}
+cudaError_t upadd_any(int c, const uint16_t *coarse, const uint16_t *skip, uint16_t *out, int nx, int ny, int nz,
+                      float factor, int acc, cudaStream_t st) {
+    switch (c) {
+        case 16: return launch_upadd<16>(coarse, skip, out, nx, ny, nz, factor, acc, st);
+        case 32: return launch_upadd<32>(coarse, skip, out, nx, ny, nz, factor, acc, st);
+        default: return launch_upadd<64>(coarse, skip, out, nx, ny, nz, factor, acc, st);
+    }
+}
+
+template <typename TX, typename TY>
+cudaError_t launch_wgrad(const TX *X, const TY *dY, float *dW, int cin, int cout, int nx, int ny, int nz,
+                         cudaStream_t st) {
+    const long long n = (long long)nx * ny * nz;
+    dim3 grid((cout * 27 * cin + 255) / 256, (unsigned)((n + kWgradChunk - 1) / kWgradChunk));
+    wgrad_kernel<TX, TY><<<grid, 256, 0, st>>>(X, dY, dW, cin, cout, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+size_t al(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+long long net_param_offset(int layer) {
+    long long off = 0;
+    for (int l = 0; l < layer; ++l) off += 27LL * kNetCin[l] * kNetCout[l];
+    return off;
+}
+long long net_param_count() { return net_param_offset(kNetLayers); }
+
+cudaError_t NetWorkspace::ensure(int nx_, int ny_, int nz_, bool training_) {
+    const long long v1 = (long long)nx_ * ny_ * nz_, v2 = v1 / 8, v3 = v1 / 64, v4 = v1 / 512;
+    // element counts (BF16) of every tensor, in declaration order
+    const long long sizes[24] = {
+        v1 * 16, v2 * 16, v2 * 32, v3 * 32, v3 * 64, v4 * 64, v4 * 64,   // a1 x2 a2 x3 a3 x4 a4
+        v3 * 64, v3 * 32, v2 * 32, v2 * 16, v1 * 16,                    // x5 b3 x6 b2 x7
+        v1 * 16, v2 * 32, v3 * 64, v4 * 64, v3 * 32, v2 * 16,           // g7 g6 g5 g4 g3 g2
+        v2 * 16, v3 * 32, v4 * 64, 0, 0, 0};                            // gb2 gb3 ga4
+    const int ntensor = training_ ? 21 : 12;
+    size_t need = 0;
+    for (int i = 0; i < ntensor; ++i) need += al(size_t(sizes[i]) * 2);
+    const int np = 1024;
+    need += al(size_t(v1) * 4) * (training_ ? 3 : 0) + al(8 * 8) + al(size_t(np) * 8);
+    if (base && need <= bytes && nx_ == nx && ny_ == ny && nz_ == nz && training == training_) return cudaSuccess;
+    if (!base || need > bytes) {
+        release();
+        cudaError_t e = cudaMalloc(&base, need);
+        if (e != cudaSuccess) {
+            base = nullptr;
+            return e;
+        }
+        bytes = need;
+    }
+    nx = nx_; ny = ny_; nz = nz_;
+    training = training_;
+    char *p = static_cast<char *>(base);
+    uint16_t **slots[21] = {&a1, &x2, &a2, &x3, &a3, &x4, &a4, &x5, &b3, &x6, &b2, &x7,
+                            &g7, &g6, &g5, &g4, &g3, &g2, &gb2, &gb3, &ga4};
+    for (int i = 0; i < 21; ++i) *slots[i] = nullptr;
+    for (int i = 0; i < ntensor; ++i) {
+        *slots[i] = reinterpret_cast<uint16_t *>(p);
+        p += al(size_t(sizes[i]) * 2);
+    }
+    ga3 = g5; ga2 = g6; ga1 = g7;  // skip-path gradients accumulate in place
+    out32 = gout = lq = nullptr;
+    if (training_) {
+        out32 = reinterpret_cast<float *>(p); p += al(size_t(v1) * 4);
+        lq = reinterpret_cast<float *>(p); p += al(size_t(v1) * 4);
+        gout = reinterpret_cast<float *>(p); p += al(size_t(v1) * 4);
+    }
+    scalars = reinterpret_cast<double *>(p); p += al(8 * 8);
+    partials = reinterpret_cast<double *>(p);
+    npartials = np;
+    return cudaSuccess;
+}
+
+void NetWorkspace::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    bytes = 0;
+    nx = ny = nz = 0;
+}
+
+cudaError_t NetWeights::allocate() {
+    const long long n = net_param_count();
+    cudaError_t e = cudaMalloc(&fwd, n * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&bwd, n * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&fwd_f32, 1296 * sizeof(float));
+    return e;
+}
+
+void NetWeights::release() {
+    if (fwd) cudaFree(fwd);
+    if (bwd) cudaFree(bwd);
+    if (fwd_f32) cudaFree(fwd_f32);
+    fwd = bwd = nullptr;
+    fwd_f32 = nullptr;
+}
+
+cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st) {
+    const long long n = net_param_count();
+    pack_kernel<<<grid_1d(n), 256, 0, st>>>(master, w.fwd, w.bwd, w.fwd_f32, n);
+    return cudaGetLastError();
+}
+
+cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int nz, double h2, const float *r, float *z,
+                      cudaStream_t st) {
+    if (nx % 8 || ny % 8 || nz % 8) return cudaErrorInvalidValue;
+    cudaError_t e = ws.ensure(nx, ny, nz, false);
+    if (e != cudaSuccess) return e;
+    const long long n = (long long)nx * ny * nz;
+    const int np = std::min(ws.npartials, grid_1d(n));
+    sumsq_kernel<<<np, 256, 0, st>>>(r, n, ws.partials);
+    scale_kernel<<<1, 256, 0, st>>>(ws.partials, np, n, ws.scalars);
+    conv_first<<<grid_1d(n), 256, 0, st>>>(r, w.fwd_f32, ws.scalars, ws.a1, nullptr, nx, ny, nz);
+    e = cudaGetLastError();
+    const int n2x = nx / 2, n2y = ny / 2, n2z = nz / 2, n3x = nx / 4, n3y = ny / 4, n3z = nz / 4;
+    const int n4x = nx / 8, n4y = ny / 8, n4z = nz / 8;
+    const uint16_t *W = w.fwd;
+    if (e == cudaSuccess) e = launch_conv<16, 32, kPool>(Src{ws.a1, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
+    if (e == cudaSuccess) e = launch_conv<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) {
+        dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
+        conv_last<kUpAdd><<<grid, kTX * kTY, 0, st>>>(Src{ws.a1, ws.b2}, w.fwd_f32 + 432, ws.scalars, h2, z, nx, ny, nz, 0);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t net_train_sample(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int nz, const float *b_hat,
+                             const float *p_hat, double norm, int loss_kind, float *grad, double *loss,
+                             cudaStream_t st) {
+    if (nx % 8 || ny % 8 || nz % 8) return cudaErrorInvalidValue;
+    cudaError_t e = ws.ensure(nx, ny, nz, true);
+    if (e != cudaSuccess) return e;
+    const long long n = (long long)nx * ny * nz;
+    const int n2x = nx / 2, n2y = ny / 2, n2z = nz / 2, n3x = nx / 4, n3y = ny / 4, n3z = nz / 4;
+    const int n4x = nx / 8, n4y = ny / 8, n4z = nz / 8;
+    const uint16_t *W = w.fwd, *Wb = w.bwd;
+    auto off = [](int l) { return net_param_offset(l); };
+    // ---- forward, every input tensor materialised ----
+    conv_first<<<grid_1d(n), 256, 0, st>>>(b_hat, w.fwd_f32, nullptr, ws.a1, nullptr, nx, ny, nz);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = pool_any(16, ws.a1, ws.x2, n2x, n2y, n2z, 0.125f, st);
+    if (e == cudaSuccess) e = launch_conv<16, 32, kPlain>(Src{ws.x2, nullptr}, W + off(1), ws.a2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = pool_any(32, ws.a2, ws.x3, n3x, n3y, n3z, 0.125f, st);
+    if (e == cudaSuccess) e = launch_conv<32, 64, kPlain>(Src{ws.x3, nullptr}, W + off(2), ws.a3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = pool_any(64, ws.a3, ws.x4, n4x, n4y, n4z, 0.125f, st);
+    if (e == cudaSuccess) e = launch_conv<64, 64, kPlain>(Src{ws.x4, nullptr}, W + off(3), ws.a4, n4x, n4y, n4z, st);
+    if (e == cudaSuccess) e = upadd_any(64, ws.a4, ws.a3, ws.x5, n3x, n3y, n3z, 1.f, 0, st);
+    if (e == cudaSuccess) e = launch_conv<64, 32, kPlain>(Src{ws.x5, nullptr}, W + off(4), ws.b3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = upadd_any(32, ws.b3, ws.a2, ws.x6, n2x, n2y, n2z, 1.f, 0, st);
+    if (e == cudaSuccess) e = launch_conv<32, 16, kPlain>(Src{ws.x6, nullptr}, W + off(5), ws.b2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = upadd_any(16, ws.b2, ws.a1, ws.x7, nx, ny, nz, 1.f, 0, st);
+    if (e == cudaSuccess) {
+        dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
+        conv_last<kPlain><<<grid, kTX * kTY, 0, st>>>(Src{ws.x7, nullptr}, w.fwd_f32 + 432, nullptr, 1.0, ws.out32, nx,
+                                                      ny, nz, 0);
+        e = cudaGetLastError();
+    }
+    // ---- loss and dL/d(output) ----
+    if (e == cudaSuccess) {
+        loss_err<<<grid_1d(n), 256, 0, st>>>(ws.out32, p_hat, ws.out32, n);  // out32 := e
+        if (loss_kind == kNetLossResidual) {
+            loss_res_kernel<<<grid_1d(n), 256, 0, st>>>(ws.out32, ws.lq, 1.0 / norm, loss, nx, ny, nz);
+            loss_res_grad<<<grid_1d(n), 256, 0, st>>>(ws.lq, ws.gout, 1.0 / norm, nx, ny, nz);
+        } else {
+            loss_kernel<<<grid_1d(n), 256, 0, st>>>(ws.out32, ws.gout, 1.0 / norm, loss, nx, ny, nz);
+        }
+        e = cudaGetLastError();
+    }
+    // ---- backward: weight gradient of each layer, then its data gradient ----
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, float>(ws.x7, ws.gout, grad + off(6), 16, 1, nx, ny, nz, st);
+    if (e == cudaSuccess) {
+        conv_first<<<grid_1d(n), 256, 0, st>>>(ws.gout, w.fwd_f32 + 864, nullptr, ws.g7, nullptr, nx, ny, nz);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = pool_any(16, ws.g7, ws.gb2, n2x, n2y, n2z, 1.f, st);
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, uint16_t>(ws.x6, ws.gb2, grad + off(5), 32, 16, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv<16, 32, kPlain>(Src{ws.gb2, nullptr}, Wb + off(5), ws.g6, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = pool_any(32, ws.g6, ws.gb3, n3x, n3y, n3z, 1.f, st);
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, uint16_t>(ws.x5, ws.gb3, grad + off(4), 64, 32, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv<32, 64, kPlain>(Src{ws.gb3, nullptr}, Wb + off(4), ws.g5, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = pool_any(64, ws.g5, ws.ga4, n4x, n4y, n4z, 1.f, st);
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, uint16_t>(ws.x4, ws.ga4, grad + off(3), 64, 64, n4x, n4y, n4z, st);
+    if (e == cudaSuccess) e = launch_conv<64, 64, kPlain>(Src{ws.ga4, nullptr}, Wb + off(3), ws.g4, n4x, n4y, n4z, st);
+    if (e == cudaSuccess) e = upadd_any(64, ws.g4, ws.ga3, ws.ga3, n3x, n3y, n3z, 0.125f, 1, st);
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, uint16_t>(ws.x3, ws.ga3, grad + off(2), 32, 64, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv<64, 32, kPlain>(Src{ws.ga3, nullptr}, Wb + off(2), ws.g3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = upadd_any(32, ws.g3, ws.ga2, ws.ga2, n2x, n2y, n2z, 0.125f, 1, st);
+    if (e == cudaSuccess) e = launch_wgrad<uint16_t, uint16_t>(ws.x2, ws.ga2, grad + off(1), 16, 32, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv<32, 16, kPlain>(Src{ws.ga2, nullptr}, Wb + off(1), ws.g2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = upadd_any(16, ws.g2, ws.ga1, ws.ga1, nx, ny, nz, 0.125f, 1, st);
+    if (e == cudaSuccess) e = launch_wgrad<float, uint16_t>(b_hat, ws.ga1, grad + off(0), 1, 16, nx, ny, nz, st);
+    return e;
+}
+
+cudaError_t net_adam(float *w, const float *g, float *m, float *v, long long n, float lr, float beta1, float beta2,
+                     float eps, long long t, float grad_scale, cudaStream_t st) {
+    const float c1 = 1.f - powf(beta1, float(t)), c2 = 1.f - powf(beta2, float(t));
+    adam_kernel<<<grid_1d(n), 256, 0, st>>>(w, g, m, v, n, lr, beta1, beta2, eps, c1, c2, grad_scale);
+    return cudaGetLastError();
+}
+
+}  // namespace flursys

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "capi_internal.cuh"
 #include "sor.cuh"
@@ -55,6 +56,21 @@ static int32_t init3d(FlursysCudaHandle *h) {
     if (e == cudaSuccess) e = h->pcg.allocate3d((int)c.nx, (int)c.ny, (int)c.nz, c.precision, h->device, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "allocating 3D solver workspace");
+    if (c.pressure_solver == FLURSYS_PRESSURE_FCG) {
+        if (!c.fcg_weights_path || !c.fcg_weights_path[0]) {
+            h->err = "pressure_solver fcg needs fcg_weights_path (a trained network)";
+            return FLURSYS_ERR_INVALID_CONFIG;
+        }
+        if (c.nx % 8 || c.ny % 8 || c.nz % 8) {
+            h->err = "the learned FCG needs nx, ny and nz divisible by 8";
+            return FLURSYS_ERR_UNSUPPORTED;
+        }
+        std::vector<float> params;
+        int32_t st = fcgnet_read_file(c.fcg_weights_path, &params, &h->err);
+        if (!st) st = fcgnet_create(params.data(), &h->fcg_net, &h->err);
+        if (st) return st;
+        return FLURSYS_OK;
+    }
     // The graph-driven PCG is the default; FLURSYS_PCG_VARIANT=persistent
     // selects the single cooperative kernel instead.
     const char *variant = std::getenv("FLURSYS_PCG_VARIANT");
@@ -98,6 +114,8 @@ void handle_free(FlursysCudaHandle *h) {
     if (h->h_diag3) cudaFreeHost(h->h_diag3);
     h->pcg.free_all();
     pcg3d_seq_destroy(h->seq);
+    if (h->fcg_net) fcgnet_destroy(h->fcg_net);
+    h->fcg_net = nullptr;
     if (h->h_seq) cudaFreeHost(h->h_seq);
     for (auto &ev : h->ev)
         if (ev) cudaEventDestroy(ev);
@@ -116,7 +134,22 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "3D predictor");
     int32_t status;
     const bool sor = c.pressure_solver == FLURSYS_PRESSURE_SOR;
-    if (sor) {
+    const bool fcg = c.pressure_solver == FLURSYS_PRESSURE_FCG;
+    if (fcg) {
+        status = fcg_solve(h->fcg_net, s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.p, s.rhs, c.pressure_atol,
+                           c.pressure_rtol, c.pressure_max_iters, c.precision, st, &h->fcg_report, &h->err);
+        if (!status) {
+            const FlursysFcgReport &f = h->fcg_report;
+            PcgResultDev &m = *h->pcg.h_result;
+            std::memset(&m, 0, sizeof m);
+            m.status = f.status;
+            m.iterations = f.fcg_iterations + f.pcg_iterations;
+            m.initial = f.initial_residual;
+            m.residual = f.final_residual;
+            m.true_l2 = f.final_residual;
+            m.initial_l2 = f.initial_residual;
+        }
+    } else if (sor) {
         status = run_sor3d(h->pcg, s.nx, s.ny, s.nz, s.dx, s.dy, s.dz, s.p, s.rhs, c.pressure_omega,
                            c.pressure_tolerance, c.pressure_max_iters, st, &h->err);
     } else if (h->use_seq) {
@@ -134,15 +167,15 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (e == cudaSuccess) e = cavity3d_diagnostics(s, h->diag3, st);
     if (e == cudaSuccess) e = cudaEventRecord(h->ev[3], st);
     if (e == cudaSuccess) {
-        if (h->use_seq && !sor)
+        if (h->use_seq && !sor && !fcg)
             e = cudaMemcpyAsync(h->h_seq, h->seq.state, sizeof(CgSeqState), cudaMemcpyDeviceToHost, st);
-        else
+        else if (!fcg)
             e = cudaMemcpyAsync(h->pcg.h_result, h->pcg.result, sizeof(PcgResultDev), cudaMemcpyDeviceToHost, st);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h->h_diag3, h->diag3, sizeof(Diag3Dev), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(&h->err, e, "3D step");
-    if (h->use_seq && !sor) {
+    if (h->use_seq && !sor && !fcg) {
         const CgSeqState &q = *h->h_seq;
         PcgResultDev &m = *h->pcg.h_result;  // the shared result record
         m.error = q.error;
@@ -186,6 +219,7 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     rep->pressure_solve_ms = ms_p;
     rep->step_ms = ms_step;
     rep->pressure_status = r.status;
+    rep->fcg_fallback = fcg ? h->fcg_report.fallback : 0;
     return FLURSYS_OK;
 }
 

@@ -63,6 +63,8 @@ class BackendOptions:
         cfg.pressure_rtol = self.pressure_rtol
         cfg.residual_replacement_every = self.residual_replacement_every
         cfg.device = self.device
+        if self.fcg_weights_path:
+            cfg.fcg_weights_path = os.fsencode(self.fcg_weights_path)
 
 
 # --------------------------------------------------------------------------

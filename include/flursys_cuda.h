@@ -335,6 +335,64 @@ int32_t flursys_cuda_stencil_pcg_noalloc(int64_t nx, int64_t ny, int64_t nz, dou
                                          const FlursysLinearSolverOptions *options,
                                          FlursysLinearSolveReport *report, void *stream);
 
+/* ---- Learned preconditioner and flexible CG (3D pinned pressure system) ----
+ * No reference counterpart: the reference's pressure solvers are SOR and
+ * Jacobi-PCG (src/linear/solver.rs, src/solver/incompressible_3d.rs:293-332).
+ * The network is a linear 4-level 3x3x3 convolutional encoder-decoder
+ * (channels 16/32/64/64, BF16 activations, FP32 accumulation) applied to
+ * the residual; its FP32 parameters are laid out layer after layer as
+ * W[co][tap][ci] (flursys_cuda_fcgnet_param_count() floats). Grids must have
+ * nx, ny, nz divisible by 8. Every buffer argument named *_device is device
+ * memory; `stream` is a cudaStream_t (NULL = default stream). */
+typedef struct FlursysFcgNet FlursysFcgNet;
+
+typedef struct FlursysFcgReport {
+    int32_t status;           /* FlursysLinearStatus of the whole solve */
+    int32_t fallback;         /* 1 when the Jacobi-PCG fallback finished the solve */
+    int64_t fcg_iterations;
+    int64_t pcg_iterations;   /* fallback iterations */
+    double initial_residual;  /* ||b - A x0||_2 */
+    double final_residual;    /* FP64 ||b - A x||_2 of the returned solution */
+    double relative_residual;
+    double net_ms;            /* device time spent applying the network */
+} FlursysFcgReport;
+
+int64_t flursys_cuda_fcgnet_param_count(void);
+/* params: host FP32 parameters, or NULL for zeros. */
+int32_t flursys_cuda_fcgnet_create(const float *params, FlursysFcgNet **out);
+/* Weights file: "FLNT", uint32 version 1, uint32 layer count 7, (cin, cout)
+ * int32 pairs, int64 parameter count, FP32 parameters, little endian. */
+int32_t flursys_cuda_fcgnet_load(const char *path, FlursysFcgNet **out);
+int32_t flursys_cuda_fcgnet_set_params(FlursysFcgNet *net, const float *params_device, void *stream);
+int32_t flursys_cuda_fcgnet_get_params(const FlursysFcgNet *net, float *host, int64_t count);
+/* z = M(r) on an nx*ny*nz grid with cell spacing factor h2 (h^2 of A^-1). */
+int32_t flursys_cuda_fcgnet_apply(FlursysFcgNet *net, int64_t nx, int64_t ny, int64_t nz, double h2,
+                                  const float *r_device, float *z_device, void *stream);
+/* Training losses of e = net(b_hat) - p_hat on the unit-spacing pure-Neumann
+ * 7-point operator L (out-of-range neighbours dropped), with L p_hat = b_hat
+ * and sum(b_hat) = 0 (the FCG solves the pinned system in this compatible
+ * Neumann form):
+ *   ENERGY    (e . L e) / norm, norm = p_hat . b_hat
+ *   RESIDUAL  |L e|^2 / norm,   norm = b_hat . b_hat  (= |L net(b_hat) - b_hat|^2 / |b_hat|^2) */
+enum FlursysFcgLoss { FLURSYS_FCG_LOSS_ENERGY = 0, FLURSYS_FCG_LOSS_RESIDUAL = 1 };
+/* One training sample: forward on b_hat, loss, backward; adds dLoss/dparams
+ * into grad_device and the loss into *loss_device (one double). */
+int32_t flursys_cuda_fcgnet_train_sample(FlursysFcgNet *net, int64_t nx, int64_t ny, int64_t nz,
+                                         const float *b_hat_device, const float *p_hat_device, double norm,
+                                         int32_t loss_kind, float *grad_device, double *loss_device, void *stream);
+/* Adam step on FP32 parameters (bias-corrected, step t >= 1). */
+int32_t flursys_cuda_fcgnet_adam(float *params_device, const float *grad_device, float *m_device, float *v_device,
+                                 int64_t n, float lr, float beta1, float beta2, float eps, int64_t t,
+                                 float grad_scale, void *stream);
+int32_t flursys_cuda_fcgnet_destroy(FlursysFcgNet *net);
+/* Learned-preconditioner FCG on the pinned 3D system of
+ * flursys_cuda_stencil_pcg (host buffers): stops when ||b - A x||_2 <= atol
+ * + rtol ||b - A x0||_2 (FP64), Jacobi-PCG finishing the solve when FCG
+ * stalls. options->max_iterations caps the FCG iterations. */
+int32_t flursys_cuda_stencil_fcg(FlursysFcgNet *net, int64_t nx, int64_t ny, int64_t nz, double dx, double dy,
+                                 double dz, const double *rhs, double *x_inout,
+                                 const FlursysLinearSolverOptions *options, FlursysFcgReport *report);
+
 /* ---- Batched 2D solvers ---------------------------------------------------
  * Many independent 2D projection solvers (one IncompressibleSolver,
  * src/solver/incompressible.rs:294-746, per config) of uneven size advanced
