@@ -259,8 +259,8 @@ int32_t flursys_cuda_create(const FlursysCudaConfig *cfg, FlursysCudaHandle **ou
     if (st) { g_error = msg; return st; }
     auto *h = new FlursysCudaHandle();
     h->cfg = *cfg;
-    h->cfg.fcg_weights_path = nullptr;  // the path is read during create only
     st = handle_init(h, cfg);
+    h->cfg.fcg_weights_path = nullptr;  // the path is read during create only
     if (st) {
         g_error = h->err;
         handle_free(h);

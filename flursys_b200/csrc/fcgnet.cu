@@ -12,8 +12,10 @@
 //       UPADD adds the nearest-neighbour upsampled coarser tensor to a skip
 //       tensor — with the same FP32 sums and BF16 rounding as the separate
 //       pool / up_add kernels, so fused and unfused paths agree bit for bit.
-//   conv_first  1 -> 16 channels (FP32 input, CUDA cores)
-//   conv_last   16 -> 1 channel (FP32 output, CUDA cores, staged tile)
+//   conv_first  1 -> 16 channels (FP32 input, CUDA cores; training)
+//   conv_last   16 -> 1 channel (FP32 output, CUDA cores, staged tile; training)
+//   net_in_fused / net_out_fused  the full-resolution layers of inference,
+//               collapsed by linearity into composite stencils (see below)
 //   wgrad       dW[co][tap][ci] += sum_v dY[v][co] X[v + tap][ci] (CUDA cores,
 //               FP32, atomics per voxel chunk)
 // The data gradient of a layer is the forward convolution with the
@@ -125,6 +127,99 @@ constexpr int conv_smem_bytes() {
     return (kHY * kHX * (CIN + kPad) + 9 * COUT * (CIN + kPad)) * 2;
 }
 
+// The 9 taps of one staged input plane (sIn: 18 x 10 halo tile, sW: the 9
+// taps' weights [t9][COUT][CIN + kPad]) accumulated into this warp's row of
+// 16 voxels x COUT channels.
+template <int CIN, int COUT>
+__device__ __forceinline__ void mma_plane(const uint16_t *sIn, const uint16_t *sW, float (&acc)[COUT / 8][4], int warp,
+                                          int g, int tig) {
+    #pragma unroll 1
+    for (int t9 = 0; t9 < 9; ++t9) {
+        const int dy = t9 / 3, dx = t9 % 3;  // halo-relative offsets 0..2
+        const uint16_t *rowA = sIn + ((warp + dy) * kHX + dx) * (CIN + kPad);
+        const uint16_t *wt = sW + t9 * COUT * (CIN + kPad);
+        #pragma unroll
+        for (int kc = 0; kc < CIN; kc += 16) {
+            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + tig * 2);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + tig * 2);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + 8 + tig * 2);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + 8 + tig * 2);
+            #pragma unroll
+            for (int n = 0; n < COUT / 8; ++n) {
+                const uint16_t *wb = wt + (n * 8 + g) * (CIN + kPad) + kc + tig * 2;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
+                mma_bf16(acc[n], a0, a1, a2, a3, b0, b1);
+            }
+        }
+    }
+}
+
+// Stores this warp's row of 16 voxels x COUT channels of plane z as BF16.
+template <int COUT>
+__device__ __forceinline__ void store_row(const float (&acc)[COUT / 8][4], uint16_t *out, int x0, int y, int z, int nx,
+                                          int ny, int g, int tig) {
+    if (y >= ny) return;
+    #pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int x = x0 + g + 8 * h;
+        if (x >= nx) continue;
+        uint16_t *o = out + (((long long)z * ny + y) * nx + x) * COUT;
+        #pragma unroll
+        for (int n = 0; n < COUT / 8; ++n) {
+            const uint32_t pk = uint32_t(f2bf(acc[n][2 * h])) | (uint32_t(f2bf(acc[n][2 * h + 1])) << 16);
+            *reinterpret_cast<uint32_t *>(o + n * 8 + tig * 2) = pk;
+        }
+    }
+}
+
+// Shared memory of conv_tc_z: all 27 taps' weights and a ring of 3 planes.
+template <int CIN, int COUT>
+constexpr int conv_z_smem_bytes() {
+    return (3 * kHY * kHX * (CIN + kPad) + 27 * COUT * (CIN + kPad)) * 2;
+}
+
+// The same convolution marching along z: a block owns a 16 x 8 column of kz
+// planes, stages the weights of all 27 taps once, and keeps the last three
+// input planes in a ring, so each input plane (and its pool / up-add
+// transform) is staged once per block instead of three times, and the
+// weights once instead of three times per plane.
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kConvThreads) conv_tc_z(Src src, const uint16_t *__restrict__ W, uint16_t *out,
+                                                          int nx, int ny, int nz, int kz) {
+    extern __shared__ __align__(16) uint16_t smem[];
+    constexpr int kPlane = kHY * kHX * (CIN + kPad);
+    uint16_t *sIn = smem;              // [3][kPlane]
+    uint16_t *sW = smem + 3 * kPlane;  // [27][COUT][CIN + kPad]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tig = lane & 3;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kz;
+    const int z1 = min(z0 + kz, nz);
+    constexpr int K8 = CIN / 8;
+    for (int idx = threadIdx.x; idx < 27 * COUT * K8; idx += blockDim.x) {
+        const int k8 = idx % K8, rest = idx / K8;
+        const int co = rest % COUT, t27 = rest / COUT;
+        const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + t27) * CIN + k8 * 8);
+        *reinterpret_cast<uint4 *>(sW + (t27 * COUT + co) * (CIN + kPad) + k8 * 8) = q;
+    }
+    // ring slot of plane z: (z - z0 + 1) mod 3
+    stage_tile<CIN, MODE>(sIn, src, x0, y0, z0 - 1, nx, ny, nz);
+    stage_tile<CIN, MODE>(sIn + kPlane, src, x0, y0, z0, nx, ny, nz);
+    for (int z = z0; z < z1; ++z) {
+        stage_tile<CIN, MODE>(sIn + ((z - z0 + 2) % 3) * kPlane, src, x0, y0, z + 1, nx, ny, nz);
+        __syncthreads();
+        float acc[COUT / 8][4];
+        #pragma unroll
+        for (int n = 0; n < COUT / 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+        #pragma unroll 1
+        for (int dz = 0; dz < 3; ++dz)
+            mma_plane<CIN, COUT>(sIn + ((z - z0 + dz) % 3) * kPlane, sW + dz * 9 * COUT * (CIN + kPad), acc, warp, g,
+                                 tig);
+        store_row<COUT>(acc, out, x0, y0 + warp, z, nx, ny, g, tig);
+        __syncthreads();  // the slot of plane z - 1 is staged next
+    }
+}
+
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kConvThreads) conv_tc(Src src, const uint16_t *__restrict__ W, uint16_t *out, int nx,
                                                         int ny, int nz) {
@@ -149,40 +244,9 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc(Src src, const uint16_t 
             *reinterpret_cast<uint4 *>(sW + (t9 * COUT + co) * (CIN + kPad) + k8 * 8) = q;
         }
         __syncthreads();
-        #pragma unroll 1
-        for (int t9 = 0; t9 < 9; ++t9) {
-            const int dy = t9 / 3, dx = t9 % 3;  // halo-relative offsets 0..2
-            const uint16_t *rowA = sIn + ((warp + dy) * kHX + dx) * (CIN + kPad);
-            const uint16_t *wt = sW + t9 * COUT * (CIN + kPad);
-            #pragma unroll
-            for (int kc = 0; kc < CIN; kc += 16) {
-                const uint32_t a0 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + tig * 2);
-                const uint32_t a1 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + tig * 2);
-                const uint32_t a2 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + 8 + tig * 2);
-                const uint32_t a3 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + 8 + tig * 2);
-                #pragma unroll
-                for (int n = 0; n < COUT / 8; ++n) {
-                    const uint16_t *wb = wt + (n * 8 + g) * (CIN + kPad) + kc + tig * 2;
-                    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
-                    const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
-                    mma_bf16(acc[n], a0, a1, a2, a3, b0, b1);
-                }
-            }
-        }
+        mma_plane<CIN, COUT>(sIn, sW, acc, warp, g, tig);
     }
-    const int y = y0 + warp;
-    if (y >= ny) return;
-    #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int x = x0 + g + 8 * h;
-        if (x >= nx) continue;
-        uint16_t *o = out + (((long long)z * ny + y) * nx + x) * COUT;
-        #pragma unroll
-        for (int n = 0; n < COUT / 8; ++n) {
-            const uint32_t pk = uint32_t(f2bf(acc[n][2 * h])) | (uint32_t(f2bf(acc[n][2 * h + 1])) << 16);
-            *reinterpret_cast<uint32_t *>(o + n * 8 + tig * 2) = pk;
-        }
-    }
+    store_row<COUT>(acc, out, x0, y0 + warp, z, nx, ny, g, tig);
 }
 
 // 1 -> 16 channels: out[v][co] = sum_tap W[co][tap] * scale * in[v + tap].
@@ -451,6 +515,159 @@ __global__ void pack_kernel(const float *master, uint16_t *fwd, uint16_t *bwd, f
     }
 }
 
+// ---- fused full-resolution layers of the inference path ----------------
+// The network is linear, so its full-resolution work collapses:
+//   x2  = pool(c1 r)          = K2 * r, a 4x4x4 stencil of stride 2 (16 outputs)
+//   out = c7(up(b2) + c1 r)   = sum over 8 coarse cells of Wp * b2
+//                               + (c7 o c1) r, a 5x5x5 stencil on r
+// c7 zero-pads its input a1 = c1 r (not r), so the composite stencil of a
+// cell drops the c7 taps that leave the domain: one 5x5x5 stencil per
+// boundary class (low boundary / interior / high boundary on each axis,
+// 27 classes). With r zero outside the domain every cell then takes the
+// same 125-tap path, exactly as the unfused layers compute it (up to FP32
+// instead of BF16 rounding of the intermediate a1 and x7).
+// up() is nearest-neighbour, so the 27 taps of c7 on up(b2) reach 2x2x2
+// coarse cells, with weights Wp that depend on the parity of the fine cell;
+// a fine tap leaves the domain exactly when its coarse cell does.
+constexpr int kFusedK2 = 0;                         // [16][64], offsets -1..2 from 2V
+constexpr int kFusedK125 = kFusedK2 + 16 * 64;      // [27 classes][125], offsets -2..2
+constexpr int kFusedWp = kFusedK125 + 27 * 125;     // [8 parities][8 coarse cells][16]
+constexpr int kFusedCount = kFusedWp + 8 * 8 * 16;
+
+__global__ void pack_fused(const float *master, long long off_first, long long off_last, float *fz) {
+    const float *W1 = master + off_first;  // [16][27][1]
+    const float *W7 = master + off_last;   // [1][27][16]
+    for (int i = threadIdx.x; i < kFusedCount; i += blockDim.x) {
+        double acc = 0.0;
+        if (i < kFusedK125) {  // K2[c][o], o = (oz*4 + oy)*4 + ox
+            const int c = i / 64, o = i % 64;
+            const int ox = o % 4 - 1, oy = (o / 4) % 4 - 1, oz = o / 16 - 1;
+            for (int a = 0; a < 8; ++a)
+                for (int t = 0; t < 27; ++t) {
+                    const int dx = t % 3 - 1 + (a & 1), dy = (t / 3) % 3 - 1 + ((a >> 1) & 1), dz = t / 9 - 1 + (a >> 2);
+                    if (dx == ox && dy == oy && dz == oz) acc += W1[c * 27 + t];
+                }
+            acc *= 0.125;
+        } else if (i < kFusedWp) {  // K125[class][o]; class axis value 0 low, 1 interior, 2 high
+            const int k = i - kFusedK125, cls = k / 125, o = k % 125;
+            const int ox = o % 5 - 2, oy = (o / 5) % 5 - 2, oz = o / 25 - 2;
+            const int clx = cls % 3, cly = (cls / 3) % 3, clz = cls / 9;
+            for (int t7 = 0; t7 < 27; ++t7) {
+                const int ax = t7 % 3 - 1, ay = (t7 / 3) % 3 - 1, az = t7 / 9 - 1;
+                if ((clx == 0 && ax < 0) || (clx == 2 && ax > 0) || (cly == 0 && ay < 0) || (cly == 2 && ay > 0) ||
+                    (clz == 0 && az < 0) || (clz == 2 && az > 0))
+                    continue;  // this c7 tap leaves the domain
+                const int bx = ox - ax, by = oy - ay, bz = oz - az;  // the c1 tap
+                if (bx < -1 || bx > 1 || by < -1 || by > 1 || bz < -1 || bz > 1) continue;
+                const int t1 = (bz + 1) * 9 + (by + 1) * 3 + (bx + 1);
+                for (int ci = 0; ci < 16; ++ci) acc += double(W7[t7 * 16 + ci]) * W1[ci * 27 + t1];
+            }
+        } else {  // Wp[par][c8][ci]
+            const int k = i - kFusedWp, par = k / 128, c8 = (k / 16) % 8, ci = k % 16;
+            for (int t7 = 0; t7 < 27; ++t7) {
+                bool hit = true;
+                for (int ax = 0; ax < 3; ++ax) {
+                    const int p = (par >> ax) & 1, d = (ax == 0 ? t7 % 3 : ax == 1 ? (t7 / 3) % 3 : t7 / 9) - 1;
+                    const int f = p + d;                                       // fine offset from 2V, -1..2
+                    const int cc = (f >= 0 ? f / 2 : -1) - (p == 0 ? -1 : 0);  // coarse cell 0 or 1
+                    if (cc != ((c8 >> ax) & 1)) hit = false;
+                }
+                if (hit) acc += W7[t7 * 16 + ci];
+            }
+        }
+        fz[i] = float(acc);
+    }
+}
+
+// x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz).
+__global__ void __launch_bounds__(256) net_in_fused(const float *__restrict__ r, const float *__restrict__ fz,
+                                                    const double *scale_ptr, uint16_t *x2, int cx, int cy, int cz) {
+    __shared__ float k2[64][16];
+    for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x) k2[i % 64][i / 64] = fz[kFusedK2 + i];
+    __syncthreads();
+    const float scale = float(scale_ptr[0]);
+    const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
+    const long long n = (long long)cx * cy * cz;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        const int X = int(v % cx);
+        const long long t = v / cx;
+        const int Y = int(t % cy), Z = int(t / cy);
+        float acc[16];
+        #pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+        #pragma unroll 4
+        for (int o = 0; o < 64; ++o) {
+            const int x = 2 * X + (o & 3) - 1, y = 2 * Y + ((o >> 2) & 3) - 1, z = 2 * Z + (o >> 4) - 1;
+            if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) continue;
+            const float rv = __ldg(r + ((long long)z * ny + y) * nx + x);
+            #pragma unroll
+            for (int c = 0; c < 16; ++c) acc[c] = fmaf(k2[o][c], rv, acc[c]);
+        }
+        uint4 q[2];
+        uint16_t *h = reinterpret_cast<uint16_t *>(q);
+        #pragma unroll
+        for (int c = 0; c < 16; ++c) h[c] = f2bf(acc[c] * scale);
+        uint4 *o4 = reinterpret_cast<uint4 *>(x2 + v * 16);
+        o4[0] = q[0];
+        o4[1] = q[1];
+    }
+}
+
+// z = (sum over 8 coarse cells of Wp * b2 + scale * K125[class] * r) * h2 / scale.
+constexpr int kOutTX = 32, kOutTY = 8;
+__global__ void __launch_bounds__(kOutTX * kOutTY) net_out_fused(const float *__restrict__ r,
+                                                                 const uint16_t *__restrict__ b2,
+                                                                 const float *__restrict__ fz, const double *scale_ptr,
+                                                                 double h2, float *out, int nx, int ny, int nz) {
+    __shared__ float tile[5][kOutTY + 4][kOutTX + 4];
+    __shared__ float k125[27 * 125];
+    __shared__ float wp[8 * 8 * 16];
+    for (int i = threadIdx.x; i < 27 * 125; i += blockDim.x) k125[i] = fz[kFusedK125 + i];
+    for (int i = threadIdx.x; i < 8 * 8 * 16; i += blockDim.x) wp[i] = fz[kFusedWp + i];
+    const int x0 = blockIdx.x * kOutTX, y0 = blockIdx.y * kOutTY, z = blockIdx.z;
+    for (int i = threadIdx.x; i < 5 * (kOutTY + 4) * (kOutTX + 4); i += blockDim.x) {
+        const int tx = i % (kOutTX + 4), ty = (i / (kOutTX + 4)) % (kOutTY + 4), tz = i / ((kOutTX + 4) * (kOutTY + 4));
+        const int x = x0 + tx - 2, y = y0 + ty - 2, zz = z + tz - 2;
+        tile[tz][ty][tx] = (x >= 0 && y >= 0 && zz >= 0 && x < nx && y < ny && zz < nz)
+                               ? __ldg(r + ((long long)zz * ny + y) * nx + x) : 0.f;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % kOutTX, ty = threadIdx.x / kOutTX;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= nx || y >= ny) return;
+    const int cls = (x == 0 ? 0 : x + 1 == nx ? 2 : 1) + 3 * (y == 0 ? 0 : y + 1 == ny ? 2 : 1) +
+                    9 * (z == 0 ? 0 : z + 1 == nz ? 2 : 1);
+    const float *k = k125 + cls * 125;
+    float skip = 0.f;
+    #pragma unroll
+    for (int dz = 0; dz < 5; ++dz)
+        #pragma unroll
+        for (int dy = 0; dy < 5; ++dy)
+            #pragma unroll
+            for (int dx = 0; dx < 5; ++dx) skip = fmaf(k[dz * 25 + dy * 5 + dx], tile[dz][ty + dy][tx + dx], skip);
+    const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
+    const int px = x & 1, py = y & 1, pz = z & 1, par = px | (py << 1) | (pz << 2);
+    const int bxs = (x >> 1) - (px == 0), bys = (y >> 1) - (py == 0), bzs = (z >> 1) - (pz == 0);
+    float up = 0.f;
+    #pragma unroll
+    for (int c8 = 0; c8 < 8; ++c8) {
+        const int X = bxs + (c8 & 1), Y = bys + ((c8 >> 1) & 1), Z = bzs + (c8 >> 2);
+        if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
+        const uint4 *src = reinterpret_cast<const uint4 *>(b2 + (((long long)Z * cy + Y) * cx + X) * 16);
+        const uint4 qa = __ldg(src), qb = __ldg(src + 1);
+        const uint16_t *ha = reinterpret_cast<const uint16_t *>(&qa);
+        const uint16_t *hb = reinterpret_cast<const uint16_t *>(&qb);
+        const float *w = wp + (par * 8 + c8) * 16;
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) up = fmaf(w[j], bf2f(ha[j]), up);
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) up = fmaf(w[8 + j], bf2f(hb[j]), up);
+    }
+    const double s = scale_ptr[0];
+    const long long v = ((long long)z * ny + y) * nx + x;
+    out[v] = s > 0.0 ? float((double(up) + s * double(skip)) * (h2 / s)) : 0.f;
+}
+
 __global__ void adam_kernel(float *w, const float *g, float *m, float *v, long long n, float lr, float b1, float b2,
                             float eps, float c1, float c2, float gs) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -465,14 +682,39 @@ __global__ void adam_kernel(float *w, const float *g, float *m, float *v, long l
 
 int grid_1d(long long n, int per = 256) { return (int)std::max<long long>(1, std::min<long long>((n + per - 1) / per, 148LL * 16)); }
 
+// Planes per block of conv_tc_z: the largest of 8, 4, 2 that still gives
+// about two blocks per SM, else 1.
+int conv_planes(int nx, int ny, int nz) {
+    const long long xy = (long long)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY);
+    for (int kz = 8; kz > 1; kz /= 2)
+        if (xy * ((nz + kz - 1) / kz) >= 2 * 148) return kz;
+    return 1;
+}
+
 template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
+    constexpr int zsmem = conv_z_smem_bytes<CIN, COUT>();
+    static int configured = 0;  // per instantiation: 1 plane kernel, 2 z-marching kernel
+    // measured on B200: marching pays where the ring and weights leave room
+    // for several blocks per SM (the 128^3-level layers of a 256^3 grid);
+    // at 160 KB (one block per SM) the plane kernel is faster
+    if (zsmem <= 100 * 1024) {
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(conv_tc_z<CIN, COUT, MODE>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, zsmem);
+            if (e != cudaSuccess) return e;
+            configured = 2;
+        }
+        const int kz = conv_planes(nx, ny, nz);
+        dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, (nz + kz - 1) / kz);
+        conv_tc_z<CIN, COUT, MODE><<<grid, kConvThreads, zsmem, st>>>(s, W, out, nx, ny, nz, kz);
+        return cudaGetLastError();
+    }
     constexpr int smem = conv_smem_bytes<CIN, COUT>();
-    static bool configured = false;  // per instantiation; set once per process
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(conv_tc<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured = 1;
     }
     dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
     conv_tc<CIN, COUT, MODE><<<grid, kConvThreads, smem, st>>>(s, W, out, nx, ny, nz);
@@ -529,11 +771,14 @@ long long net_param_count() { return net_param_offset(kNetLayers); }
 cudaError_t NetWorkspace::ensure(int nx_, int ny_, int nz_, bool training_) {
     const long long v1 = (long long)nx_ * ny_ * nz_, v2 = v1 / 8, v3 = v1 / 64, v4 = v1 / 512;
     // element counts (BF16) of every tensor, in declaration order
+    // (inference fuses the full-resolution layers and the pool / up-add
+    // inputs, so it keeps x2, a2, a3, a4, b3 and b2 only)
+    const long long tr = training_ ? 1 : 0;
     const long long sizes[24] = {
-        v1 * 16, v2 * 16, v2 * 32, v3 * 32, v3 * 64, v4 * 64, v4 * 64,   // a1 x2 a2 x3 a3 x4 a4
-        v3 * 64, v3 * 32, v2 * 32, v2 * 16, v1 * 16,                    // x5 b3 x6 b2 x7
-        v1 * 16, v2 * 32, v3 * 64, v4 * 64, v3 * 32, v2 * 16,           // g7 g6 g5 g4 g3 g2
-        v2 * 16, v3 * 32, v4 * 64, 0, 0, 0};                            // gb2 gb3 ga4
+        tr * v1 * 16, v2 * 16, v2 * 32, tr * v3 * 32, v3 * 64, tr * v4 * 64, v4 * 64,  // a1 x2 a2 x3 a3 x4 a4
+        tr * v3 * 64, v3 * 32, tr * v2 * 32, v2 * 16, tr * v1 * 16,                    // x5 b3 x6 b2 x7
+        v1 * 16, v2 * 32, v3 * 64, v4 * 64, v3 * 32, v2 * 16,                          // g7 g6 g5 g4 g3 g2
+        v2 * 16, v3 * 32, v4 * 64, 0, 0, 0};                                           // gb2 gb3 ga4
     const int ntensor = training_ ? 21 : 12;
     size_t need = 0;
     for (int i = 0; i < ntensor; ++i) need += al(size_t(sizes[i]) * 2);
@@ -556,6 +801,7 @@ cudaError_t NetWorkspace::ensure(int nx_, int ny_, int nz_, bool training_) {
                             &g7, &g6, &g5, &g4, &g3, &g2, &gb2, &gb3, &ga4};
     for (int i = 0; i < 21; ++i) *slots[i] = nullptr;
     for (int i = 0; i < ntensor; ++i) {
+        if (sizes[i] == 0) continue;
         *slots[i] = reinterpret_cast<uint16_t *>(p);
         p += al(size_t(sizes[i]) * 2);
     }
@@ -584,6 +830,7 @@ cudaError_t NetWeights::allocate() {
     cudaError_t e = cudaMalloc(&fwd, n * 2);
     if (e == cudaSuccess) e = cudaMalloc(&bwd, n * 2);
     if (e == cudaSuccess) e = cudaMalloc(&fwd_f32, 1296 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&fused, kFusedCount * sizeof(float));
     return e;
 }
 
@@ -591,13 +838,15 @@ void NetWeights::release() {
     if (fwd) cudaFree(fwd);
     if (bwd) cudaFree(bwd);
     if (fwd_f32) cudaFree(fwd_f32);
+    if (fused) cudaFree(fused);
     fwd = bwd = nullptr;
-    fwd_f32 = nullptr;
+    fwd_f32 = fused = nullptr;
 }
 
 cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st) {
     const long long n = net_param_count();
     pack_kernel<<<grid_1d(n), 256, 0, st>>>(master, w.fwd, w.bwd, w.fwd_f32, n);
+    pack_fused<<<1, 256, 0, st>>>(master, net_param_offset(0), net_param_offset(kNetLayers - 1), w.fused);
     return cudaGetLastError();
 }
 
@@ -610,19 +859,19 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     const int np = std::min(ws.npartials, grid_1d(n));
     sumsq_kernel<<<np, 256, 0, st>>>(r, n, ws.partials);
     scale_kernel<<<1, 256, 0, st>>>(ws.partials, np, n, ws.scalars);
-    conv_first<<<grid_1d(n), 256, 0, st>>>(r, w.fwd_f32, ws.scalars, ws.a1, nullptr, nx, ny, nz);
-    e = cudaGetLastError();
     const int n2x = nx / 2, n2y = ny / 2, n2z = nz / 2, n3x = nx / 4, n3y = ny / 4, n3z = nz / 4;
     const int n4x = nx / 8, n4y = ny / 8, n4z = nz / 8;
+    net_in_fused<<<grid_1d((long long)n2x * n2y * n2z), 256, 0, st>>>(r, w.fused, ws.scalars, ws.x2, n2x, n2y, n2z);
+    e = cudaGetLastError();
     const uint16_t *W = w.fwd;
-    if (e == cudaSuccess) e = launch_conv<16, 32, kPool>(Src{ws.a1, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv<16, 32, kPlain>(Src{ws.x2, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
     if (e == cudaSuccess) e = launch_conv<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
     if (e == cudaSuccess) e = launch_conv<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
     if (e == cudaSuccess) e = launch_conv<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
     if (e == cudaSuccess) e = launch_conv<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
     if (e == cudaSuccess) {
-        dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
-        conv_last<kUpAdd><<<grid, kTX * kTY, 0, st>>>(Src{ws.a1, ws.b2}, w.fwd_f32 + 432, ws.scalars, h2, z, nx, ny, nz, 0);
+        dim3 grid((nx + kOutTX - 1) / kOutTX, (ny + kOutTY - 1) / kOutTY, nz);
+        net_out_fused<<<grid, kOutTX * kOutTY, 0, st>>>(r, ws.b2, w.fused, ws.scalars, h2, z, nx, ny, nz);
         e = cudaGetLastError();
     }
     return e;

@@ -58,6 +58,7 @@ struct NetWeights {
     uint16_t *fwd = nullptr;   // W[co][tap][ci]
     uint16_t *bwd = nullptr;   // W'[ci][26 - tap][co]
     float *fwd_f32 = nullptr;  // FP32 copies of c1, c7 (CUDA-core layers) and their transposes
+    float *fused = nullptr;    // FP32 composite stencils of the fused full-resolution layers
     cudaError_t allocate();
     void release();
 };

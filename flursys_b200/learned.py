@@ -291,7 +291,7 @@ def _diag_unit(n: int) -> np.ndarray:
 
 
 def fcg_iterate_pairs(net: "FcgNet", systems, iterations: int = 24, snapshots=(2, 6, 12, 24),
-                      device: str = "cuda") -> List[Pair]:
+                      device: str = "cuda", max_systems: int = 40) -> List[Pair]:
     """Pairs from the flexible CG's own iterates with the current network:
     at iteration k the preconditioner's network sees r1 = r_k - A z0 (z0 the
     pre-smoothing of r_k), whose exact solution is e_k - z0 with e_k = p - x_k.
@@ -300,6 +300,8 @@ def fcg_iterate_pairs(net: "FcgNet", systems, iterations: int = 24, snapshots=(2
     network."""
     import torch
     out = []
+    if len(systems) > max_systems:  # an even spread over the kept systems
+        systems = [systems[int(i)] for i in np.linspace(0, len(systems) - 1, max_systems)]
     for n, b, p in systems:
         h2 = (1.0 / n) ** 2
         dA = _diag_unit(n) / h2
@@ -401,8 +403,8 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--traj64", type=int, default=20)
-    ap.add_argument("--traj128", type=int, default=8)
+    ap.add_argument("--traj64", type=int, default=25)
+    ap.add_argument("--traj128", type=int, default=15)
     ap.add_argument("--steps", type=int, default=25, help="steps per trajectory (pairs per step: 1 + residual iters)")
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--lr", type=float, default=2e-3)
