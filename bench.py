@@ -15,6 +15,9 @@ Arms:
   default            the CUDA backend (libflursys_cuda.so)
   --impl reference   the reference CPU path restated in C++ (oracle/), all
                      host threads, bounded sample of the same workload.
+Extra lines on the same JSON object (rank 0): the 256^3 plain-PCG solve and
+the learned-FCG solve at the same stop rule (pcg_big, fcg_big), the batched
+2D cavities (batch2d) and the 2D 128^2 cavity (cavity2d_128).
 Multi-GPU (torchrun): replicas only — every rank advances its own cavity; no
 collective is on the data path.
 """
@@ -284,6 +287,10 @@ def run_ours(args):
         line["roofline"] = roofline(n_cells, its, solve_ms, precision)
         if args.big_size and not args.no_big:
             line["pcg_big"] = big_solve(args.big_size, precision, local)
+            line["fcg_big"] = fcg_solve(args.big_size, precision, local, line["pcg_big"])
+        if not args.no_extra:
+            line["batch2d"] = batch2d_run(local)
+            line["cavity2d_128"] = cavity2d_run(local)
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             steps, elapsed, cits = cpu_reference_run(n, 3, args.cpu_budget, threads)
@@ -298,8 +305,8 @@ def run_ours(args):
 
 
 def big_solve(n, precision, device):
-    """Two steps of the n^3 cavity (the 256^3 shape of the learned-FCG
-    comparison), plain PCG: pressure-solve ms, iterations and HBM roofline."""
+    """Two steps of the n^3 cavity, plain PCG: pressure-solve ms, iterations
+    and HBM roofline of the second (warm-started) solve."""
     from flursys_b200.solver import _Handle
     _, c = workload_config(n, precision)
     c.device = device
@@ -312,6 +319,113 @@ def big_solve(n, precision, device):
     return {"cells": n ** 3, "pressure_iterations": its, "pressure_solve_ms": rep.pressure_solve_ms,
             "step_ms": rep.step_ms, "true_relative_residual": rep.pressure_true_relative_residual,
             "roofline_frac": r["frac"], "achieved_gbs": r["achieved"]}
+
+
+def fcg_solve(n, precision, device, pcg):
+    """The same two steps with the learned-preconditioner FCG (trained weights
+    shipped in flursys_b200/weights): pressure-solve ms at the same stop rule
+    (FP64 ||b - A x||_2 <= 1e-8 ||b - A x0||_2), against the plain PCG."""
+    import os as _os
+    from flursys_b200.learned import DEFAULT_WEIGHTS
+    from flursys_b200.solver import _Handle
+    if not _os.path.exists(DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained weights file"}
+    _, c = workload_config(n, precision)
+    c.device = device
+    c.pressure_solver = 2  # FLURSYS_PRESSURE_FCG
+    c.fcg_weights_path = _os.fsencode(DEFAULT_WEIGHTS)
+    h = _Handle(c)
+    h.step(1)
+    rep = h.step(1)
+    h.close()
+    out = {"cells": n ** 3, "pressure_iterations": int(rep.pressure_iterations),
+           "pressure_solve_ms": rep.pressure_solve_ms, "fallback": int(rep.fcg_fallback),
+           "true_relative_residual": rep.pressure_true_relative_residual,
+           "iterations_ratio_pcg_over_fcg": pcg["pressure_iterations"] / max(1, int(rep.pressure_iterations)),
+           "speedup_vs_pcg": pcg["pressure_solve_ms"] / rep.pressure_solve_ms}
+    return out
+
+
+def batch2d_run(device, instances=64, steps=5, warmup=2, seed=2024):
+    """Config of the batched solver: 64 independent 2D cavities, sides drawn
+    from U{64..512}, Re from U[100, 2000], adaptive dt (CFL 0.5, diffusion
+    0.25), upwind, mixed precision, PCG to 1e-8 relative L2; aggregate
+    cell-steps/s of whole batch steps (one graph launch each)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from flursys_b200 import _abi
+    from flursys_b200.solver import BatchedIncompressibleSolver
+    lib = _abi.load()
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(64, 513, size=instances)
+    res = rng.uniform(100.0, 2000.0, size=instances)
+    cfgs = []
+    for n, re in zip(sides, res):
+        c = _abi.CudaConfig()
+        lib.flursys_cuda_default_config(2, C.byref(c))
+        c.nx = c.ny = int(n)
+        c.case_params.kinematic_viscosity = 1.0 / re
+        c.case_params.reynolds = re
+        c.adaptive = 1
+        c.dt = 1e-3
+        c.target_cfl, c.target_diffusion_number = 0.5, 0.25
+        c.t_end = 1e9
+        c.stop_rule = _abi.STOP_REL_L2
+        c.pressure_atol, c.pressure_rtol = 0.0, 1e-8
+        c.pressure_max_iters = 50000
+        c.precision = _abi.PRECISION_MIXED
+        c.residual_replacement_every = 50
+        c.device = device
+        cfgs.append(c)
+    cells = int((sides.astype(np.int64) ** 2).sum())
+    b = BatchedIncompressibleSolver(cfgs, autotune=True)
+    b.advance(warmup)
+    torch.cuda.synchronize(device)
+    b.advance(steps)
+    reps = [b.report(i) for i in range(instances)]
+    ms = reps[0].step_ms
+    its = [int(r.pressure_iterations) for r in reps]
+    status = sorted({b.status(i) for i in range(instances)})
+    tuning = b.tuning()
+    b.close()
+    return {"instances": instances, "cells": cells, "sides": [int(sides.min()), int(sides.max())],
+            "steps": steps, "ms_per_step": ms, "cell_steps_per_s": cells / (ms / 1000.0),
+            "pressure_iterations_min_max": [min(its), max(its)], "status": status, "tuning": tuning}
+
+
+def cavity2d_run(device, n=128, steps=1000):
+    """2D cavity 128^2, Re 100, upwind, adaptive dt (CFL 0.5, diffusion 0.25),
+    PCG to 1e-8 relative L2, f64, 1000 steps from the zero field:
+    cell-steps/s (host-timed: the 2D handle reads its diagnostics back every
+    step, as advance() returns a SolverStep)."""
+    import ctypes as C
+    from flursys_b200 import _abi
+    from flursys_b200.solver import _Handle
+    lib = _abi.load()
+    c = _abi.CudaConfig()
+    lib.flursys_cuda_default_config(2, C.byref(c))
+    c.nx = c.ny = n
+    c.case_params.reynolds = 100.0
+    c.case_params.kinematic_viscosity = 0.01
+    c.adaptive = 1
+    c.dt = 1e-3
+    c.target_cfl, c.target_diffusion_number = 0.5, 0.25
+    c.t_end = 1e9
+    c.max_steps = steps
+    c.stop_rule = _abi.STOP_REL_L2
+    c.pressure_atol, c.pressure_rtol = 0.0, 1e-8
+    c.pressure_max_iters = 50000
+    c.precision = _abi.PRECISION_F64
+    c.device = device
+    h = _Handle(c)
+    h.step(3)
+    t0 = time.perf_counter()
+    rep = h.step(steps)
+    secs = time.perf_counter() - t0
+    h.close()
+    return {"cells": n * n, "steps": steps, "seconds": secs, "cell_steps_per_s": n * n * steps / secs,
+            "last_pressure_iterations": int(rep.pressure_iterations), "last_dt": rep.time_step}
 
 
 def roofline(n_cells, its, solve_ms, precision):
@@ -352,6 +466,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--big-size", type=int, default=256, help="size of the extra plain-PCG solve measurement")
     ap.add_argument("--no-big", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched-2D and 2D-cavity sub-measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -32,6 +32,10 @@ struct GridBarrier {
 // Every wait is bounded: on timeout the error word is set and the caller is
 // told to leave its loop. Returns false when the barrier failed.
 __device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
+    if (nblocks == 1u) {  // one block: a block barrier orders its global accesses
+        __syncthreads();
+        return true;
+    }
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -365,7 +366,12 @@ int32_t init2d(FlursysCudaHandle *h) {
     in.ref_cell = ref_cell;
     in.count_fluid = fluid;
     in.block0 = 0;
-    in.nblocks = h->pcg.grid;
+    // Small grids are latency bound: three grid barriers per iteration cost
+    // more than the work, so the solve gets one block per 512 cells
+    // (FLURSYS_2D_CELLS_PER_BLOCK overrides), at most the co-resident grid.
+    long long per_block = 512;
+    if (const char *env = std::getenv("FLURSYS_2D_CELLS_PER_BLOCK")) per_block = std::max(1LL, std::atoll(env));
+    in.nblocks = (int)std::max(1LL, std::min<long long>(h->pcg.grid, ((long long)nc + per_block - 1) / per_block));
     in.partials = h->pcg.partials;
     in.barrier = h->pcg.barrier;
     in.result = h->pcg.result;
