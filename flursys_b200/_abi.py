@@ -181,6 +181,41 @@ class BatchTuning(C.Structure):
     ]
 
 
+class SimpleConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("reserved", C.c_int32),
+        ("nx", C.c_int64),
+        ("ny", C.c_int64),
+        ("length", C.c_double),
+        ("height", C.c_double),
+        ("kinematic_viscosity", C.c_double),
+        ("inlet_peak_velocity", C.c_double),
+        ("outlet_pressure", C.c_double),
+        ("max_outer_iterations", C.c_int64),
+        ("continuity_tolerance", C.c_double),
+        ("velocity_relaxation", C.c_double),
+        ("pressure_relaxation", C.c_double),
+        ("momentum_solver", LinearSolverOptions),
+        ("pressure_solver", LinearSolverOptions),
+    ]
+
+
+class SimpleReport(C.Structure):
+    _fields_ = [
+        ("converged", C.c_int32),
+        ("reserved", C.c_int32),
+        ("outer_iterations", C.c_int64),
+        ("initial_continuity_rms", C.c_double),
+        ("final_continuity_rms", C.c_double),
+        ("momentum", LinearSolveReport * 3),
+        ("pressure", LinearSolveReport),
+        ("total_inflow", C.c_double),
+        ("total_outflow", C.c_double),
+        ("solve_ms", C.c_double),
+    ]
+
+
 BATCH_AUTOTUNE, BATCH_NO_GRAPH = 1, 2
 FCG_LOSS_ENERGY, FCG_LOSS_RESIDUAL = 0, 1
 
@@ -244,6 +279,9 @@ SIGNATURES = {
     "flursys_cuda_stencil_fcg": (C.c_int32, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                              C.c_double, _D, _D, C.POINTER(LinearSolverOptions),
                                              C.POINTER(FcgReport)]),
+    "flursys_cuda_simple_default_config": (C.c_int32, [C.POINTER(SimpleConfig)]),
+    "flursys_cuda_simple_channel": (C.c_int32, [C.POINTER(SimpleConfig), _D, _D, _D, _D, _D,
+                                                C.POINTER(SimpleReport)]),
     "flursys_cuda_batch_create": (C.c_int32, [C.POINTER(CudaConfig), C.c_int32, C.c_int32, C.POINTER(_P)]),
     "flursys_cuda_batch_step": (C.c_int32, [_P, C.c_int64]),
     "flursys_cuda_batch_report": (C.c_int32, [_P, C.c_int32, C.POINTER(StepReport), C.POINTER(C.c_int32)]),

@@ -483,7 +483,113 @@ int32_t csr_solve(int method, int64_t n, int64_t nnz, const int64_t *ro, const i
     return status;
 }
 
+// 1/diag of each row (ascending columns); error bit on a missing or zero diagonal.
+__global__ void jacobi_inverse_kernel(int n, const int *ro, const int *ci, const double *va, double *inv,
+                                      CsrResultDev *res) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        bool found = false;
+        for (int e = ro[r]; e < ro[r + 1]; ++e)
+            if (ci[e] == r) { d = va[e]; found = true; break; }
+        if (!found || d == 0.0) {
+            atomicCAS(&res->error, 0, found ? FLURSYS_ERR_ZERO_DIAGONAL : FLURSYS_ERR_MISSING_DIAGONAL);
+            inv[r] = 0.0;
+        } else {
+            inv[r] = 1.0 / d;
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t CsrDeviceWork::ensure(int n_, int device) {
+    if (vec && n_ <= n) return cudaSuccess;
+    release();
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, krylov_kernel, kBlock, 0);
+    if (e != cudaSuccess) return e;
+    grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm, ((long long)n_ + kBlock * 4 - 1) / (kBlock * 4)));
+    e = cudaMalloc(&vec, sizeof(double) * 10 * (size_t)std::max(n_, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&partials, sizeof(double) * kParts * (size_t)grid);
+    if (e == cudaSuccess) e = cudaMalloc(&inv_diag, sizeof(double) * (size_t)std::max(n_, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&bar, sizeof(GridBarrier));
+    if (e == cudaSuccess) e = cudaMalloc(&res, 2 * sizeof(CsrResultDev));   // [0] solve, [1] Jacobi set-up
+    if (e == cudaSuccess) e = cudaMallocHost(&hres, 2 * sizeof(CsrResultDev));
+    if (e == cudaSuccess) n = n_;
+    return e;
+}
+
+void CsrDeviceWork::release() {
+    cudaFree(vec); cudaFree(partials); cudaFree(inv_diag); cudaFree(bar); cudaFree(res);
+    if (hres) cudaFreeHost(hres);
+    vec = partials = inv_diag = nullptr;
+    bar = nullptr;
+    res = hres = nullptr;
+    n = grid = 0;
+}
+
+cudaError_t csr_device_launch(int method, int n, const int *ro, const int *ci, const double *va, const double *b,
+                              double *x, double atol, double rtol, long long max_iters, CsrDeviceWork &w,
+                              cudaStream_t st) {
+    KrylovArgs k{};
+    double *v = w.vec;
+    k.r = v; k.z = v + (size_t)n; k.d0 = v + 2 * (size_t)n; k.d1 = v + 3 * (size_t)n; k.q = v + 4 * (size_t)n;
+    k.rh = v + 5 * (size_t)n; k.p = v + 6 * (size_t)n; k.v = v + 7 * (size_t)n; k.s = v + 8 * (size_t)n;
+    k.t = v + 9 * (size_t)n;
+    k.partials = w.partials;
+    k.bar = w.bar;
+    k.res = w.res;
+    k.atol = atol;
+    k.rtol = rtol;
+    k.max_iters = max_iters;
+    k.method = method;
+    k.a = CsrDev{n, ro, ci, va, method == 1 ? w.inv_diag : nullptr};
+    k.b = b;
+    k.x = x;
+    cudaError_t e = cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.res, 0xff, sizeof(CsrResultDev), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.res + 1, 0, sizeof(CsrResultDev), st);
+    if (e == cudaSuccess && method == 1) {
+        jacobi_inverse_kernel<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(n, ro, ci, va, w.inv_diag, w.res + 1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        void *params[] = {&k};
+        e = cudaLaunchCooperativeKernel((const void *)krylov_kernel, dim3(w.grid), dim3(kBlock), params, 0, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w.hres, w.res, 2 * sizeof(CsrResultDev), cudaMemcpyDeviceToHost, st);
+    return e;
+}
+
+int32_t csr_device_status(const CsrResultDev *rr, FlursysLinearSolveReport *rep, std::string *err) {
+    const CsrResultDev &r = rr[0];
+    if (rr[1].error == FLURSYS_ERR_MISSING_DIAGONAL || rr[1].error == FLURSYS_ERR_ZERO_DIAGONAL) {
+        *err = rr[1].error == FLURSYS_ERR_ZERO_DIAGONAL ? "zero diagonal entry" : "missing diagonal entry";
+        return rr[1].error;
+    }
+    if (r.device_error & kDevErrBarrierTimeout) {
+        *err = "CSR solve: a device grid barrier timed out";
+        return FLURSYS_ERR_TIMEOUT;
+    }
+    if (r.error == FLURSYS_ERR_NON_FINITE) {
+        *err = "non-finite solver value";
+        return FLURSYS_ERR_NON_FINITE;
+    }
+    if (r.error == FLURSYS_ERR_BREAKDOWN) {
+        *err = "iterative solver breakdown";
+        return FLURSYS_ERR_BREAKDOWN;
+    }
+    if (rep) {
+        rep->status = r.status;
+        rep->reserved = 0;
+        rep->iterations = r.iterations;
+        rep->initial_residual = r.initial;
+        rep->final_residual = r.final_residual;
+        rep->relative_residual = r.initial == 0.0 ? 0.0 : r.final_residual / r.initial;
+    }
+    return FLURSYS_OK;
+}
 
 }  // namespace flursys
 

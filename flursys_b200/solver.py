@@ -485,3 +485,60 @@ class BatchedIncompressibleSolver:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class ChannelSimpleConfig:
+    """The steady plane-channel case of solve_incompressible
+    (src/unstructured_incompressible.rs:368-482) on nx x ny uniform quads,
+    with IncompressibleSolverOptions defaults (:38-49). Re is on the mean
+    velocity (2/3 of the parabolic peak) and the height, as
+    src/project.rs:497-509 defines it."""
+    nx: int = 2048
+    ny: int = 512
+    length: float = 8.0
+    height: float = 1.0
+    reynolds: float = 200.0
+    inlet_peak_velocity: float = 1.0
+    outlet_pressure: float = 0.0
+    max_outer_iterations: int = 200
+    continuity_tolerance: float = 1.0e-10
+    velocity_relaxation: float = 0.7
+    pressure_relaxation: float = 0.3
+    momentum_solver: tuple = (1.0e-10, 1.0e-8, 1000)   # (atol, rtol, max_iterations)
+    pressure_solver: tuple = (1.0e-10, 1.0e-8, 1000)
+
+    def kinematic_viscosity(self) -> float:
+        return (2.0 / 3.0) * self.inlet_peak_velocity * self.height / self.reynolds
+
+    def to_c(self) -> _abi.SimpleConfig:
+        lib = _abi.load()
+        c = _abi.SimpleConfig()
+        _check(lib, None, lib.flursys_cuda_simple_default_config(C.byref(c)))
+        c.nx, c.ny = self.nx, self.ny
+        c.length, c.height = self.length, self.height
+        c.kinematic_viscosity = self.kinematic_viscosity()
+        c.inlet_peak_velocity = self.inlet_peak_velocity
+        c.outlet_pressure = self.outlet_pressure
+        c.max_outer_iterations = self.max_outer_iterations
+        c.continuity_tolerance = self.continuity_tolerance
+        c.velocity_relaxation = self.velocity_relaxation
+        c.pressure_relaxation = self.pressure_relaxation
+        c.momentum_solver = _abi.LinearSolverOptions(*self.momentum_solver)
+        c.pressure_solver = _abi.LinearSolverOptions(*self.pressure_solver)
+        return c
+
+
+def solve_simple_channel(cfg) -> dict:
+    """flursys_cuda_simple_channel: cell velocity, pressure, face fluxes
+    (+x x-faces then +y y-faces), continuity history and the report."""
+    lib = _abi.load()
+    c = cfg.to_c() if hasattr(cfg, "to_c") else cfg
+    n = c.nx * c.ny
+    u, v, p = np.zeros(n), np.zeros(n), np.zeros(n)
+    flux = np.zeros((c.nx + 1) * c.ny + c.nx * (c.ny + 1))
+    hist = np.zeros(c.max_outer_iterations + 1)
+    rep = _abi.SimpleReport()
+    _check(lib, None, lib.flursys_cuda_simple_channel(C.byref(c), _abi.dptr(u), _abi.dptr(v), _abi.dptr(p),
+                                                      _abi.dptr(flux), _abi.dptr(hist), C.byref(rep)))
+    return {"u": u, "v": v, "p": p, "flux": flux, "history": hist[:rep.outer_iterations + 1], "report": rep}

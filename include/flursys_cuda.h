@@ -393,6 +393,58 @@ int32_t flursys_cuda_stencil_fcg(FlursysFcgNet *net, int64_t nx, int64_t ny, int
                                  double dz, const double *rhs, double *x_inout,
                                  const FlursysLinearSolverOptions *options, FlursysFcgReport *report);
 
+/* ---- Steady collocated SIMPLE channel -------------------------------------
+ * solve_incompressible (src/unstructured_incompressible.rs:368-482) with
+ * solve_simple (src/simple.rs:148-314) on a plane channel of nx x ny uniform
+ * quads (unit depth): inlet on the left (fixed velocity), no-slip walls at
+ * the bottom and top, pressure outlet on the right. Kinematic pressure (the
+ * SIMPLE core uses unit density). Each outer iteration assembles the
+ * momentum systems to CSR and solves them with BiCGSTAB, forms the
+ * Rhie-Chow face flux, assembles the pressure-correction system to CSR and
+ * solves it with Jacobi-PCG, and corrects pressure, velocity and face flux;
+ * it stops when the RMS of the integrated cell continuity imbalance is at
+ * most continuity_tolerance. The inlet profile is parabolic, u = peak 4 y
+ * (H - y) / H^2 at each face centre: a per-face fixed velocity where the
+ * reference's VelocityInlet holds one vector per patch. */
+typedef struct FlursysSimpleConfig {
+    uint32_t abi_version;
+    int32_t reserved;
+    int64_t nx, ny;
+    double length, height;
+    double kinematic_viscosity;
+    double inlet_peak_velocity;
+    double outlet_pressure;
+    int64_t max_outer_iterations;          /* IncompressibleSolverOptions defaults: 200 */
+    double continuity_tolerance;           /* 1e-10 */
+    double velocity_relaxation;            /* 0.7 */
+    double pressure_relaxation;            /* 0.3 */
+    FlursysLinearSolverOptions momentum_solver;  /* LinearSolverOptions::default() */
+    FlursysLinearSolverOptions pressure_solver;
+} FlursysSimpleConfig;
+
+typedef struct FlursysSimpleReport {     /* IncompressibleSolveReport / SimpleReport */
+    int32_t converged;
+    int32_t reserved;
+    int64_t outer_iterations;
+    double initial_continuity_rms;
+    double final_continuity_rms;
+    FlursysLinearSolveReport momentum[3];  /* x, y, z systems of the last outer iteration */
+    FlursysLinearSolveReport pressure;     /* pressure correction of the last outer iteration */
+    double total_inflow, total_outflow;    /* boundary flux sums (inflow negative) */
+    double solve_ms;                       /* device time of the whole solve */
+} FlursysSimpleReport;
+
+int32_t flursys_cuda_simple_default_config(FlursysSimpleConfig *cfg);
+/* Host outputs (any may be NULL): cell velocity components and pressure
+ * (nx*ny, x fastest), face fluxes ((nx+1)*ny x-faces then nx*(ny+1)
+ * y-faces, each positive along +x / +y), and the continuity RMS history
+ * (max_outer_iterations + 1 values: the initial one, then one per outer
+ * iteration). Errors mirror SimpleError: a linear solve that does not
+ * converge is FLURSYS_ERR_BREAKDOWN with the message naming it. */
+int32_t flursys_cuda_simple_channel(const FlursysSimpleConfig *cfg, double *velocity_x, double *velocity_y,
+                                    double *pressure, double *face_flux, double *continuity_history,
+                                    FlursysSimpleReport *report);
+
 /* ---- Batched 2D solvers ---------------------------------------------------
  * Many independent 2D projection solvers (one IncompressibleSolver,
  * src/solver/incompressible.rs:294-746, per config) of uneven size advanced

@@ -68,6 +68,8 @@ def load() -> C.CDLL:
         "orc_stencil_pcg": (C.c_int32, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, _D,
                                         _D, C.POINTER(_abi.LinearSolverOptions),
                                         C.POINTER(_abi.LinearSolveReport)]),
+        "orc_simple_channel": (C.c_int32, [C.POINTER(_abi.SimpleConfig), _D, _D, _D, _D, _D,
+                                           C.POINTER(_abi.SimpleReport)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -208,3 +210,35 @@ def stencil_pcg(nx, ny, nz, dx, dy, dz, rhs, x0, options):
     rep = _abi.LinearSolveReport()
     st = lib.orc_stencil_pcg(nx, ny, nz, dx, dy, dz, _abi.dptr(b), _abi.dptr(x), C.byref(options), C.byref(rep))
     return st, x, rep
+
+
+def simple_default_config(nx=64, ny=8, length=8.0, height=1.0, reynolds=200.0, peak=1.0):
+    """Channel config with the IncompressibleSolverOptions defaults
+    (unstructured_incompressible.rs:38-49); Re on the mean velocity 2/3 peak
+    and the height, as project.rs:497-509 defines it."""
+    c = _abi.SimpleConfig()
+    c.abi_version = _abi.ABI_VERSION
+    c.nx, c.ny = nx, ny
+    c.length, c.height = length, height
+    c.kinematic_viscosity = (2.0 / 3.0) * peak * height / reynolds
+    c.inlet_peak_velocity = peak
+    c.outlet_pressure = 0.0
+    c.max_outer_iterations = 200
+    c.continuity_tolerance = 1e-10
+    c.velocity_relaxation, c.pressure_relaxation = 0.7, 0.3
+    c.momentum_solver = _abi.LinearSolverOptions(1e-10, 1e-8, 1000)
+    c.pressure_solver = _abi.LinearSolverOptions(1e-10, 1e-8, 1000)
+    return c
+
+
+def simple_channel(cfg):
+    """orc_simple_channel: (status, u, v, p, face_flux, history, report)."""
+    lib = load()
+    n = cfg.nx * cfg.ny
+    u, v, p = np.zeros(n), np.zeros(n), np.zeros(n)
+    flux = np.zeros((cfg.nx + 1) * cfg.ny + cfg.nx * (cfg.ny + 1))
+    hist = np.zeros(cfg.max_outer_iterations + 1)
+    rep = _abi.SimpleReport()
+    st = lib.orc_simple_channel(C.byref(cfg), _abi.dptr(u), _abi.dptr(v), _abi.dptr(p), _abi.dptr(flux),
+                                _abi.dptr(hist), C.byref(rep))
+    return st, u, v, p, flux, hist[:rep.outer_iterations + 1], rep

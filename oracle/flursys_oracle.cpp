@@ -13,6 +13,7 @@
 #include "flursys_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1863,3 +1864,460 @@ int32_t orc_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, double dx, double dy
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Steady collocated SIMPLE (src/simple.rs, src/momentum.rs, src/numerics.rs,
+// src/unstructured_incompressible.rs) on a general face-based mesh, here
+// built for the uniform quad channel. FP64, serial, reference loop order.
+// ===========================================================================
+namespace {
+
+struct V3 {
+    double x = 0.0, y = 0.0, z = 0.0;
+};
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator*(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+enum Patch : int { kInternal = -1, kInlet = 0, kOutlet = 1, kBottom = 2, kTop = 3 };
+
+// UnstructuredMesh (src/mesh.rs:201-230) for a 2D quad grid with unit depth:
+// face area vector = edge rotated outward from the owner, |S| = edge length,
+// cell volume = cell area (mesh.rs:563-616).
+struct FvMesh {
+    int64_t nx = 0, ny = 0;
+    std::vector<V3> cc;               // cell centres
+    std::vector<double> vol;
+    std::vector<int64_t> owner, neigh;  // neigh -1 on boundary faces
+    std::vector<V3> area, fc;
+    std::vector<int> patch;
+    std::vector<std::vector<int64_t>> cell_faces;
+    int64_t ncells() const { return (int64_t)cc.size(); }
+    int64_t nfaces() const { return (int64_t)owner.size(); }
+};
+
+FvMesh channel_mesh(int64_t nx, int64_t ny, double L, double H) {
+    FvMesh m;
+    m.nx = nx;
+    m.ny = ny;
+    const double dx = L / nx, dy = H / ny;
+    m.cc.resize(nx * ny);
+    m.vol.assign(nx * ny, dx * dy);
+    m.cell_faces.resize(nx * ny);
+    for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i) m.cc[i + nx * j] = {(i + 0.5) * dx, (j + 0.5) * dy, 0.0};
+    auto add = [&](int64_t o, int64_t n, V3 s, V3 c, int p) {
+        m.owner.push_back(o);
+        m.neigh.push_back(n);
+        m.area.push_back(s);
+        m.fc.push_back(c);
+        m.patch.push_back(p);
+        const int64_t f = m.nfaces() - 1;
+        m.cell_faces[o].push_back(f);
+        if (n >= 0) m.cell_faces[n].push_back(f);
+    };
+    for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i + 1 < nx; ++i)
+            add(i + nx * j, i + 1 + nx * j, {dy, 0, 0}, {(i + 1) * dx, (j + 0.5) * dy, 0}, kInternal);
+    for (int64_t j = 0; j + 1 < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i)
+            add(i + nx * j, i + nx * (j + 1), {0, dx, 0}, {(i + 0.5) * dx, (j + 1) * dy, 0}, kInternal);
+    for (int64_t j = 0; j < ny; ++j) add(nx * j, -1, {-dy, 0, 0}, {0.0, (j + 0.5) * dy, 0}, kInlet);
+    for (int64_t j = 0; j < ny; ++j) add(nx - 1 + nx * j, -1, {dy, 0, 0}, {L, (j + 0.5) * dy, 0}, kOutlet);
+    for (int64_t i = 0; i < nx; ++i) add(i, -1, {0, -dx, 0}, {(i + 0.5) * dx, 0.0, 0}, kBottom);
+    for (int64_t i = 0; i < nx; ++i) add(i + nx * (ny - 1), -1, {0, dx, 0}, {(i + 0.5) * dx, H, 0}, kTop);
+    return m;
+}
+
+// ScalarBoundaryCondition per face (numerics.rs): fixed value or zero gradient.
+struct ScalarBc {
+    std::vector<int> fixed;  // 1 FixedValue, 0 ZeroGradient (boundary faces)
+    std::vector<double> value;
+};
+
+// weight (numerics.rs:294-303)
+double iweight(const FvMesh &m, int64_t f) {
+    const V3 d = m.cc[m.neigh[f]] - m.cc[m.owner[f]];
+    return dot(m.fc[f] - m.cc[m.owner[f]], d) / dot(d, d);
+}
+
+// LeastSquaresGradientStencil::new (numerics.rs:106-200), 2D.
+struct LsEq {
+    V3 coef;
+    int64_t nb;   // neighbour cell, or -1 for a fixed boundary value
+    double value;
+};
+struct LsStencil {
+    std::vector<std::vector<LsEq>> eqs;
+    std::vector<std::array<double, 9>> inv;
+};
+
+int32_t ls_stencil(const FvMesh &m, const ScalarBc &bc, LsStencil *out) {
+    out->eqs.assign(m.ncells(), {});
+    out->inv.assign(m.ncells(), {});
+    for (int64_t c = 0; c < m.ncells(); ++c) {
+        double nm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t f : m.cell_faces[c]) {
+            V3 off;
+            LsEq e{};
+            if (m.neigh[f] >= 0) {
+                const int64_t nb = m.owner[f] == c ? m.neigh[f] : m.owner[f];
+                off = m.cc[nb] - m.cc[c];
+                e.nb = nb;
+            } else {
+                if (!bc.fixed[f]) continue;  // zero gradient: no equation in 2D
+                off = m.fc[f] - m.cc[c];
+                e.nb = -1;
+                e.value = bc.value[f];
+            }
+            const double w = 1.0 / dot(off, off);
+            const V3 rc = off * w;
+            nm[0] += rc.x * off.x; nm[1] += rc.x * off.y; nm[2] += rc.x * off.z;
+            nm[3] += rc.y * off.x; nm[4] += rc.y * off.y; nm[5] += rc.y * off.z;
+            nm[6] += rc.z * off.x; nm[7] += rc.z * off.y; nm[8] += rc.z * off.z;
+            e.coef = rc;
+            out->eqs[c].push_back(e);
+        }
+        // inverse_normal_matrix, TwoD (numerics.rs:236-254)
+        const double det = nm[0] * nm[4] - nm[1] * nm[3];
+        const double scale = std::max(std::max(std::fabs(nm[0]), std::fabs(nm[4])), 1.0);
+        if (std::fabs(det) <= 2.220446049250313e-16 * scale * scale) return FLURSYS_ERR_BREAKDOWN;
+        out->inv[c] = {nm[4] / det, -nm[1] / det, 0.0, -nm[3] / det, nm[0] / det, 0.0, 0.0, 0.0, 0.0};
+    }
+    return FLURSYS_OK;
+}
+
+// least_squares_gradient_into (numerics.rs:650-682)
+std::vector<V3> ls_gradient(const LsStencil &s, const std::vector<double> &v) {
+    std::vector<V3> g(v.size());
+    for (size_t c = 0; c < v.size(); ++c) {
+        V3 r;
+        for (const LsEq &e : s.eqs[c]) {
+            const double adj = e.nb >= 0 ? v[e.nb] : e.value;
+            r = r + e.coef * (adj - v[c]);
+        }
+        const auto &I = s.inv[c];
+        g[c] = {I[0] * r.x + I[1] * r.y + I[2] * r.z, I[3] * r.x + I[4] * r.y + I[5] * r.z,
+                I[6] * r.x + I[7] * r.y + I[8] * r.z};
+    }
+    return g;
+}
+
+// CsrBuilder::add + finalize (csr.rs:131-192) into owned arrays.
+struct OwnedCsr {
+    int64_t n = 0;
+    std::vector<int64_t> ro, ci;
+    std::vector<double> v;
+    Csr view() const { return Csr{n, n, ro.data(), ci.data(), v.data()}; }
+    double diag(int64_t r) const {
+        for (int64_t e = ro[r]; e < ro[r + 1]; ++e)
+            if (ci[e] == r) return v[e];
+        return 0.0;
+    }
+};
+
+int32_t build_csr(int64_t n, const std::vector<std::tuple<int64_t, int64_t, double>> &entries, OwnedCsr *out) {
+    std::vector<int64_t> rows(entries.size()), cols(entries.size());
+    std::vector<double> vals(entries.size());
+    for (size_t k = 0; k < entries.size(); ++k) {
+        rows[k] = std::get<0>(entries[k]);
+        cols[k] = std::get<1>(entries[k]);
+        vals[k] = std::get<2>(entries[k]);
+    }
+    out->n = n;
+    out->ro.assign(n + 1, 0);
+    out->ci.assign(entries.size(), 0);
+    out->v.assign(entries.size(), 0.0);
+    int64_t nnz = 0;
+    int32_t st = orc_csr_build(n, n, (int64_t)entries.size(), rows.data(), cols.data(), vals.data(), out->ro.data(),
+                               out->ci.data(), out->v.data(), &nnz);
+    out->ci.resize(nnz);
+    out->v.resize(nnz);
+    return st;
+}
+
+// assemble_momentum_component (momentum.rs:180-341): upwind convection,
+// two-point diffusion, explicit source, equation under-relaxation.
+int32_t assemble_momentum(const FvMesh &m, double nu, const ScalarBc &bc, const std::vector<double> &flux,
+                          const std::vector<double> &source, const std::vector<double> &current, double alpha,
+                          OwnedCsr *A, std::vector<double> *rhs_out) {
+    const int64_t n = m.ncells();
+    std::vector<std::tuple<int64_t, int64_t, double>> e;
+    e.reserve(m.nfaces() * 4 + n);
+    std::vector<double> rhs(n, 0.0);
+    for (int64_t c = 0; c < n; ++c) rhs[c] += source[c] * m.vol[c];
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        const double phi = flux[f];
+        const int64_t o = m.owner[f];
+        if (m.neigh[f] >= 0) {
+            const int64_t nb = m.neigh[f];
+            const V3 d = m.cc[nb] - m.cc[o];
+            const double D = nu * dot(m.area[f], d) / dot(d, d);
+            e.emplace_back(o, o, D + std::max(phi, 0.0));
+            e.emplace_back(o, nb, -D + std::min(phi, 0.0));
+            e.emplace_back(nb, o, -D - std::max(phi, 0.0));
+            e.emplace_back(nb, nb, D - std::min(phi, 0.0));
+        } else {
+            const V3 d = m.fc[f] - m.cc[o];
+            const double D = nu * dot(m.area[f], d) / dot(d, d);
+            if (bc.fixed[f]) {
+                const double val = bc.value[f];
+                e.emplace_back(o, o, D + std::max(phi, 0.0));
+                rhs[o] += D * val - std::min(phi, 0.0) * val;
+            } else {
+                if (phi < 0.0) return FLURSYS_ERR_INVALID_CONFIG;  // BackflowOnZeroGradient
+                e.emplace_back(o, o, phi);
+            }
+        }
+    }
+    OwnedCsr un;
+    int32_t st = build_csr(n, e, &un);
+    if (st) return st;
+    if (alpha == 1.0) {
+        *A = std::move(un);
+        *rhs_out = std::move(rhs);
+        return FLURSYS_OK;
+    }
+    std::vector<std::tuple<int64_t, int64_t, double>> r;
+    r.reserve(un.v.size());
+    for (int64_t row = 0; row < n; ++row) {
+        const double dg = un.diag(row);
+        for (int64_t k = un.ro[row]; k < un.ro[row + 1]; ++k) {
+            double v = un.v[k];
+            if (un.ci[k] == row) v /= alpha;
+            r.emplace_back(row, un.ci[k], v);
+        }
+        rhs[row] += (1.0 - alpha) / alpha * dg * current[row];
+    }
+    st = build_csr(n, r, A);
+    *rhs_out = std::move(rhs);
+    return st;
+}
+
+struct SimpleOut {
+    std::vector<double> u, v, p, flux, history;
+    FlursysSimpleReport rep{};
+};
+
+// solve_incompressible + solve_simple for the channel case.
+int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
+    const int64_t nx = cfg.nx, ny = cfg.ny;
+    if (nx < 2 || ny < 2) return FLURSYS_ERR_INVALID_CONFIG;
+    if (cfg.max_outer_iterations < 1) return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(cfg.pressure_relaxation > 0.0 && cfg.pressure_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(cfg.velocity_relaxation > 0.0 && cfg.velocity_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
+    const FvMesh m = channel_mesh(nx, ny, cfg.length, cfg.height);
+    const int64_t n = m.ncells(), nf = m.nfaces();
+    const double H = cfg.height, U = cfg.inlet_peak_velocity;
+    // resolve_boundaries (unstructured_incompressible.rs:106-212)
+    ScalarBc vel[3], pbc, pcbc;
+    for (ScalarBc *b : {&vel[0], &vel[1], &vel[2], &pbc, &pcbc}) {
+        b->fixed.assign(nf, 0);
+        b->value.assign(nf, 0.0);
+    }
+    std::vector<double> bflux(nf, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+        if (m.patch[f] == kInternal) continue;
+        if (m.patch[f] == kOutlet) {
+            pbc.fixed[f] = 1;
+            pbc.value[f] = cfg.outlet_pressure;
+            pcbc.fixed[f] = 1;
+            pcbc.value[f] = 0.0;
+            continue;  // velocity zero gradient, no prescribed flux
+        }
+        V3 u{};
+        if (m.patch[f] == kInlet) {
+            const double y = m.fc[f].y;
+            u.x = U * 4.0 * y * (H - y) / (H * H);
+        }
+        vel[0].fixed[f] = vel[1].fixed[f] = vel[2].fixed[f] = 1;
+        vel[0].value[f] = u.x;
+        vel[1].value[f] = u.y;
+        vel[2].value[f] = u.z;
+        bflux[f] = dot(u, m.area[f]);
+    }
+    LsStencil stencil;
+    int32_t st = ls_stencil(m, pbc, &stencil);
+    if (st) return st;
+    std::vector<V3> U3(n);                // zero initial velocity
+    std::vector<double> p(n, 0.0);
+    // initial_face_flux (simple.rs:724-755): internal faces from the
+    // interpolated (zero) velocity, boundary faces prescribed.
+    std::vector<double> flux = bflux;
+    for (int64_t f = 0; f < nf; ++f)
+        if (m.neigh[f] >= 0) {
+            const double l = iweight(m, f);
+            flux[f] = dot(U3[m.owner[f]] * (1.0 - l) + U3[m.neigh[f]] * l, m.area[f]);
+        }
+    auto continuity = [&](const std::vector<double> &F) {
+        std::vector<double> div(n, 0.0);
+        for (int64_t f = 0; f < nf; ++f) {
+            div[m.owner[f]] += F[f];
+            if (m.neigh[f] >= 0) div[m.neigh[f]] -= F[f];
+        }
+        double s = 0.0;
+        for (double d : div) s += d * d;
+        return std::sqrt(s / double(n));
+    };
+    out->history.assign(1, continuity(flux));
+    FlursysSimpleReport &rep = out->rep;
+    rep = FlursysSimpleReport{};
+    rep.initial_continuity_rms = out->history[0];
+    for (int64_t it = 1; it <= cfg.max_outer_iterations; ++it) {
+        // pressure_gradient_source with unit density
+        const std::vector<V3> gp = ls_gradient(stencil, p);
+        OwnedCsr A[3];
+        std::vector<double> b[3];
+        for (int k = 0; k < 3; ++k) {
+            std::vector<double> src(n), cur(n);
+            for (int64_t c = 0; c < n; ++c) {
+                src[c] = -(k == 0 ? gp[c].x : k == 1 ? gp[c].y : gp[c].z);
+                cur[c] = k == 0 ? U3[c].x : k == 1 ? U3[c].y : U3[c].z;
+            }
+            st = assemble_momentum(m, cfg.kinematic_viscosity, vel[k], flux, src, cur, cfg.velocity_relaxation, &A[k],
+                                   &b[k]);
+            if (st) return st;
+        }
+        // solve_momentum_velocity: BiCGSTAB per component from the current velocity
+        std::vector<double> comp[3];
+        for (int k = 0; k < 3; ++k) {
+            comp[k].resize(n);
+            for (int64_t c = 0; c < n; ++c) comp[k][c] = k == 0 ? U3[c].x : k == 1 ? U3[c].y : U3[c].z;
+            st = solve_bicgstab(A[k].view(), b[k].data(), comp[k].data(), cfg.momentum_solver, &rep.momentum[k]);
+            if (st) return st;
+            if (rep.momentum[k].status != FLURSYS_LINEAR_CONVERGED) return FLURSYS_ERR_BREAKDOWN;
+        }
+        std::vector<V3> pred(n);
+        for (int64_t c = 0; c < n; ++c) pred[c] = {comp[0][c], comp[1][c], comp[2][c]};
+        // momentum_inverse_diagonal of the x system
+        std::vector<double> rau(n);
+        for (int64_t c = 0; c < n; ++c) {
+            const double d = A[0].diag(c);
+            if (!(std::isfinite(d) && d > 0.0)) return FLURSYS_ERR_BREAKDOWN;
+            rau[c] = 1.0 / d;
+        }
+        // rhie_chow_predicted_flux (simple.rs:757-805) + fixed correction faces
+        std::vector<double> coef(nf, 0.0);
+        for (int64_t f = 0; f < nf; ++f) {
+            const int64_t o = m.owner[f];
+            if (m.neigh[f] >= 0) {
+                const int64_t nb = m.neigh[f];
+                const double l = iweight(m, f);
+                const V3 d = m.cc[nb] - m.cc[o];
+                coef[f] = (rau[o] * (1.0 - l) + rau[nb] * l) * dot(m.area[f], d) / dot(d, d);
+            } else if (pcbc.fixed[f]) {
+                const V3 d = m.fc[f] - m.cc[o];
+                coef[f] = rau[o] * dot(m.area[f], d) / dot(d, d);
+            }
+        }
+        std::vector<double> pf = flux;
+        for (int64_t f = 0; f < nf; ++f) {
+            const int64_t o = m.owner[f];
+            if (m.neigh[f] >= 0) {
+                const int64_t nb = m.neigh[f];
+                const double l = iweight(m, f);
+                const V3 fu = pred[o] * (1.0 - l) + pred[nb] * l;
+                const V3 fr = gp[o] * rau[o] * (1.0 - l) + gp[nb] * rau[nb] * l;
+                pf[f] = dot(fu, m.area[f]) + dot(fr, m.area[f]) - coef[f] * (p[nb] - p[o]);
+            } else if (pcbc.fixed[f]) {
+                pf[f] = dot(pred[o], m.area[f]);
+            }
+        }
+        // assemble_pressure_correction_with_boundary (simple.rs:583-643)
+        std::vector<std::tuple<int64_t, int64_t, double>> pe;
+        std::vector<double> prhs(n, 0.0);
+        bool anchored = false;
+        for (int64_t f = 0; f < nf; ++f) {
+            const int64_t o = m.owner[f];
+            prhs[o] -= pf[f];
+            if (m.neigh[f] >= 0) {
+                const int64_t nb = m.neigh[f];
+                prhs[nb] += pf[f];
+                pe.emplace_back(o, o, coef[f]);
+                pe.emplace_back(o, nb, -coef[f]);
+                pe.emplace_back(nb, o, -coef[f]);
+                pe.emplace_back(nb, nb, coef[f]);
+            } else if (pcbc.fixed[f]) {
+                pe.emplace_back(o, o, coef[f]);
+                prhs[o] += coef[f] * pcbc.value[f];
+                anchored = true;
+            }
+        }
+        if (!anchored) return FLURSYS_ERR_INVALID_CONFIG;
+        OwnedCsr P;
+        if ((st = build_csr(n, pe, &P))) return st;
+        std::vector<double> pc(n, 0.0), inv;
+        int64_t bad = -1;
+        if ((st = jacobi(P.view(), inv, &bad))) return st;
+        st = solve_cg(P.view(), prhs.data(), pc.data(), cfg.pressure_solver, &inv, &rep.pressure);
+        if (st) return st;
+        if (rep.pressure.status != FLURSYS_LINEAR_CONVERGED) return FLURSYS_ERR_BREAKDOWN;
+        for (int64_t c = 0; c < n; ++c) p[c] += cfg.pressure_relaxation * pc[c];
+        const std::vector<V3> gpc = ls_gradient(stencil, pc);
+        for (int64_t c = 0; c < n; ++c) U3[c] = pred[c] - gpc[c] * rau[c];
+        // correct_face_flux_with_boundary (simple.rs:448-496)
+        flux = pf;
+        for (int64_t f = 0; f < nf; ++f) {
+            const int64_t o = m.owner[f];
+            if (m.neigh[f] >= 0) flux[f] -= coef[f] * (pc[m.neigh[f]] - pc[o]);
+            else if (pcbc.fixed[f]) flux[f] -= coef[f] * (pcbc.value[f] - pc[o]);
+        }
+        const double cont = continuity(flux);
+        out->history.push_back(cont);
+        rep.outer_iterations = it;
+        rep.final_continuity_rms = cont;
+        if (cont <= cfg.continuity_tolerance) {
+            rep.converged = 1;
+            break;
+        }
+    }
+    // backflow at the pressure outlet (unstructured_incompressible.rs:430-449)
+    for (int64_t f = 0; f < nf; ++f)
+        if (m.patch[f] == kOutlet && flux[f] < 0.0) return FLURSYS_ERR_INVALID_CONFIG;
+    for (int64_t f = 0; f < nf; ++f) {
+        if (m.neigh[f] >= 0) continue;
+        if (flux[f] < 0.0) rep.total_inflow += flux[f];
+        else rep.total_outflow += flux[f];
+    }
+    // outputs: cell fields and +x / +y face fluxes
+    out->u.resize(n);
+    out->v.resize(n);
+    out->p = p;
+    for (int64_t c = 0; c < n; ++c) {
+        out->u[c] = U3[c].x;
+        out->v[c] = U3[c].y;
+    }
+    out->flux.assign((nx + 1) * ny + nx * (ny + 1), 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+        const int64_t o = m.owner[f];
+        const int64_t i = o % nx, j = o / nx;
+        if (m.area[f].x != 0.0) {  // x-face: east face of the owner unless it is the inlet
+            const bool west = m.area[f].x < 0.0;
+            out->flux[(west ? i : i + 1) + (nx + 1) * j] = west ? -flux[f] : flux[f];
+        } else {
+            const bool south = m.area[f].y < 0.0;
+            out->flux[(nx + 1) * ny + i + nx * (south ? j : j + 1)] = south ? -flux[f] : flux[f];
+        }
+    }
+    return FLURSYS_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t orc_simple_channel(const FlursysSimpleConfig *cfg, double *velocity_x, double *velocity_y,
+                                      double *pressure, double *face_flux, double *continuity_history,
+                                      FlursysSimpleReport *report) {
+    if (!cfg) return FLURSYS_ERR_INVALID_ARGUMENT;
+    SimpleOut out;
+    const int32_t st = simple_channel(*cfg, &out);
+    if (st) return st;
+    const size_t n = out.p.size();
+    if (velocity_x) std::memcpy(velocity_x, out.u.data(), n * sizeof(double));
+    if (velocity_y) std::memcpy(velocity_y, out.v.data(), n * sizeof(double));
+    if (pressure) std::memcpy(pressure, out.p.data(), n * sizeof(double));
+    if (face_flux) std::memcpy(face_flux, out.flux.data(), out.flux.size() * sizeof(double));
+    if (continuity_history) std::memcpy(continuity_history, out.history.data(), out.history.size() * sizeof(double));
+    if (report) *report = out.rep;
+    return FLURSYS_OK;
+}

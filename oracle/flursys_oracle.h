@@ -84,6 +84,13 @@ int32_t orc_stencil_pcg(int64_t nx, int64_t ny, int64_t nz, double dx, double dy
                         const FlursysLinearSolverOptions *options,
                         FlursysLinearSolveReport *report);
 
+/* Steady collocated SIMPLE channel (src/simple.rs:148-314 with the case
+ * resolution of src/unstructured_incompressible.rs:106-212,368-482), FP64,
+ * same outputs as flursys_cuda_simple_channel. */
+int32_t orc_simple_channel(const FlursysSimpleConfig *cfg, double *velocity_x, double *velocity_y,
+                           double *pressure, double *face_flux, double *continuity_history,
+                           FlursysSimpleReport *report);
+
 #ifdef __cplusplus
 }
 #endif
