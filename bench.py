@@ -17,7 +17,8 @@ Arms:
                      host threads, bounded sample of the same workload.
 Extra lines on the same JSON object (rank 0): the 256^3 plain-PCG solve and
 the learned-FCG solve at the same stop rule (pcg_big, fcg_big), the batched
-2D cavities (batch2d) and the 2D 128^2 cavity (cavity2d_128).
+2D cavities (batch2d), the 2D 128^2 cavity (cavity2d_128) and the steady
+SIMPLE channel (simple_channel).
 Multi-GPU (torchrun): replicas only — every rank advances its own cavity; no
 collective is on the data path.
 """
@@ -291,6 +292,7 @@ def run_ours(args):
         if not args.no_extra:
             line["batch2d"] = batch2d_run(local)
             line["cavity2d_128"] = cavity2d_run(local)
+            line["simple_channel"] = simple_run()
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             steps, elapsed, cits = cpu_reference_run(n, 3, args.cpu_budget, threads)
@@ -392,6 +394,39 @@ def batch2d_run(device, instances=64, steps=5, warmup=2, seed=2024):
     return {"instances": instances, "cells": cells, "sides": [int(sides.min()), int(sides.max())],
             "steps": steps, "ms_per_step": ms, "cell_steps_per_s": cells / (ms / 1000.0),
             "pressure_iterations_min_max": [min(its), max(its)], "status": status, "tuning": tuning}
+
+
+def simple_run(outer=3):
+    """Steady SIMPLE plane channel, 2048 x 512 cells, L 8, H 1, parabolic
+    inlet (peak 1), Re 200 on the mean velocity: device ms per outer
+    iteration (momentum CSR + 2 BiCGSTAB, Rhie-Chow, pressure-correction
+    CSR + Jacobi-PCG, corrections), the continuity RMS after each, and the
+    FP64 oracle's time for one outer iteration of the 512 x 128 channel
+    beside the device's. The reference's continuity stop rule (RMS of the
+    integrated cell imbalance) is met after the first pressure correction,
+    so a fixed number of outer iterations is timed."""
+    from flursys_b200.solver import ChannelSimpleConfig, solve_simple_channel
+    opts = dict(continuity_tolerance=0.0, momentum_solver=(1e-10, 1e-8, 20000), pressure_solver=(1e-10, 1e-8, 50000))
+    big = solve_simple_channel(ChannelSimpleConfig(nx=2048, ny=512, max_outer_iterations=outer, **opts))
+    r = big["report"]
+    out = {"cells": 2048 * 512, "outer_iterations": int(r.outer_iterations),
+           "ms_per_outer": r.solve_ms / max(1, r.outer_iterations),
+           "pressure_pcg_iterations": int(r.pressure.iterations),
+           "momentum_bicgstab_iterations": [int(r.momentum[0].iterations), int(r.momentum[1].iterations)],
+           "continuity_rms": [float(x) for x in big["history"]]}
+    small = ChannelSimpleConfig(nx=512, ny=128, max_outer_iterations=1, **opts)
+    dev = solve_simple_channel(small)["report"]
+    out["small_512x128_device_ms_per_outer"] = dev.solve_ms
+    try:
+        from oracle import binding as ob
+        ob.load()
+        ob.set_threads(1)
+        t0 = time.perf_counter()
+        st = ob.simple_channel(small.to_c())[0]
+        out["small_512x128_oracle_ms_per_outer"] = (time.perf_counter() - t0) * 1e3 if st == 0 else None
+    except Exception as exc:  # the oracle library is a test artefact; report its absence
+        out["small_512x128_oracle_ms_per_outer"] = f"unavailable: {exc}"
+    return out
 
 
 def cavity2d_run(device, n=128, steps=1000):
