@@ -17,9 +17,9 @@ enum DeviceError : unsigned {
     kDevErrNonFinite = 2u,       // a NaN/Inf reached a checked value
 };
 
-// Upper bound on polls of one grid-barrier wait (each poll sleeps ~100 ns):
-// about one second, far above any legitimate wait of a co-resident grid.
-constexpr long long kBarrierSpinLimit = 10'000'000LL;
+// Upper bound on polls of one grid-barrier wait (each poll sleeps ~32 ns or
+// more): about one second, far above any legitimate wait of a co-resident grid.
+constexpr long long kBarrierSpinLimit = 30'000'000LL;
 
 struct GridBarrier {
     unsigned count;
@@ -56,7 +56,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
+                __nanosleep(32);
             }
         }
         __threadfence();
@@ -90,6 +90,61 @@ __device__ __forceinline__ double block_sum(double v, double *smem /* >= BLOCK/3
     t = smem[0];
     __syncthreads();
     return t;
+}
+
+// Block sums of N values per thread, and optionally (MAX) the block maximum
+// of one more, with one set of barriers; each value takes the same shuffle
+// tree and order as block_sum / block_max, so the results are bit-identical
+// to separate calls. smem holds at least (N + MAX) * BLOCK / 32 doubles.
+template <int BLOCK, int N, bool MAX>
+__device__ __forceinline__ void block_reduce_n(double (&v)[N], double &mx, double *smem) {
+    constexpr int NW = BLOCK / 32;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if (MAX)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) smem[k * NW + wid] = v[k];
+        if (MAX) smem[N * NW + wid] = mx;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            double t = lane < NW ? smem[k * NW + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            v[k] = t;
+        }
+        if (MAX) {
+            double t = lane < NW ? smem[N * NW + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+            mx = t;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) smem[k] = v[k];
+        if (MAX) smem[N] = mx;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = smem[k];
+    if (MAX) mx = smem[N];
+    __syncthreads();
+}
+template <int BLOCK, int N>
+__device__ __forceinline__ void block_sum_n(double (&v)[N], double *smem) {
+    double unused = 0.0;
+    block_reduce_n<BLOCK, N, false>(v, unused, smem);
 }
 
 template <int BLOCK>

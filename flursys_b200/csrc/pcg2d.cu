@@ -91,16 +91,46 @@ __device__ __forceinline__ T apply_row(const Ctx &k, int c, int i, int j, T vc, 
     return dg * vc - s;
 }
 
-__device__ __forceinline__ void write_parts(const Ctx &k, const double *v, int nv, double *red) {
-    for (int p = 0; p < nv; ++p) {
-        const double t = block_sum<kBlock>(v[p], red);
-        if (threadIdx.x == 0) k.in.partials[k.lb * kParts + p] = t;
+// Block partial sums of NV values into columns 0..NV-1 of this block's row.
+template <int NV>
+__device__ __forceinline__ void write_parts(const Ctx &k, double (&v)[NV], double *red) {
+    block_sum_n<kBlock, NV>(v, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int p = 0; p < NV; ++p) k.in.partials[k.lb * kParts + p] = v[p];
+}
+// Sums over the instance's blocks of columns 0..NV-1, in block order.
+template <int NV>
+__device__ __forceinline__ void read_sums(const Ctx &k, double (&out)[NV], double *red) {
+#pragma unroll
+    for (int p = 0; p < NV; ++p) out[p] = 0.0;
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock)
+#pragma unroll
+        for (int p = 0; p < NV; ++p) out[p] += k.in.partials[b * kParts + p];
+    block_sum_n<kBlock, NV>(out, red);
+}
+// write_parts plus the block maximum of mx into column NV.
+template <int NV>
+__device__ __forceinline__ void write_parts_max(const Ctx &k, double (&v)[NV], double mx, double *red) {
+    block_reduce_n<kBlock, NV, true>(v, mx, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int p = 0; p < NV; ++p) k.in.partials[k.lb * kParts + p] = v[p];
+        k.in.partials[k.lb * kParts + NV] = mx;
     }
 }
-__device__ __forceinline__ double read_sum(const Ctx &k, int p, double *red) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s += k.in.partials[b * kParts + p];
-    return block_sum<kBlock>(s, red);
+// read_sums plus the maximum over blocks of column NV.
+template <int NV>
+__device__ __forceinline__ void read_sums_max(const Ctx &k, double (&out)[NV], double &mx, double *red) {
+#pragma unroll
+    for (int p = 0; p < NV; ++p) out[p] = 0.0;
+    mx = 0.0;
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) {
+#pragma unroll
+        for (int p = 0; p < NV; ++p) out[p] += k.in.partials[b * kParts + p];
+        mx = fmax(mx, k.in.partials[b * kParts + NV]);
+    }
+    block_reduce_n<kBlock, NV, true>(out, mx, red);
 }
 __device__ __forceinline__ double read_max(const Ctx &k, int p, double *red) {
     double s = 0.0;
@@ -152,11 +182,13 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             }
         }
         double v[2] = {sx, sb};
-        write_parts(k, v, 2, red);
+        write_parts<2>(k, v, red);
     }
     if (!grid_sync(in.barrier, nb)) return;
-    double mx = proj ? read_sum(k, 0, red) / cnt : 0.0;
-    mb = proj ? read_sum(k, 1, red) / cnt : 0.0;
+    double m0[2];
+    read_sums<2>(k, m0, red);
+    double mx = proj ? m0[0] / cnt : 0.0;
+    mb = proj ? m0[1] / cnt : 0.0;
     if (proj) {
         for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
             if (!ident(f, c)) x[c] -= mx;
@@ -176,9 +208,11 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             r[c] = V(rv);
         }
         double v[1] = {sr};
-        write_parts(k, v, 1, red);
+        write_parts<1>(k, v, red);
         if (!grid_sync(in.barrier, nb)) return false;
-        const double mr = proj ? read_sum(k, 0, red) / cnt : 0.0;
+        double m1[1];
+        read_sums<1>(k, m1, red);
+        const double mr = proj ? m1[0] / cnt : 0.0;
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
         for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
             const int c = it.c, i = it.i, j = it.j;
@@ -200,16 +234,14 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             s_rz += rv * double(V(zv));
         }
         double v2[4] = {s_rr, s_z, s_rz, s_r};
-        write_parts(k, v2, 4, red);
-        write_max(k, 4, s_max, red);
+        write_parts_max<4>(k, v2, s_max, red);
         return grid_sync(in.barrier, nb);
     };
     auto read_residual_sums = [&](double &rr, double &rmax, double &rz) {
-        rr = read_sum(k, 0, red);
-        const double sz = read_sum(k, 1, red);
-        const double srz = read_sum(k, 2, red);
-        const double sr = read_sum(k, 3, red);
-        rmax = read_max(k, 4, red);
+        double s4[4];
+        read_sums_max<4>(k, s4, rmax, red);
+        rr = s4[0];
+        const double sz = s4[1], srz = s4[2], sr = s4[3];
         mz = proj ? sz / cnt : 0.0;
         rz = srz - mz * sr;  // r'.(z - mean z)
     };
@@ -251,12 +283,14 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         {
             double v[3] = {s_dq, s_q, s_d};
-            write_parts(k, v, 3, red);
+            write_parts<3>(k, v, red);
         }
         if (!grid_sync(in.barrier, nb)) return;
-        const double sdq = read_sum(k, 0, red);
-        const double md = proj ? read_sum(k, 2, red) / cnt : 0.0;
-        const double dq = proj ? sdq - md * read_sum(k, 1, red) : sdq;
+        double s3[3];
+        read_sums<3>(k, s3, red);
+        const double sdq = s3[0];
+        const double md = proj ? s3[2] / cnt : 0.0;
+        const double dq = proj ? sdq - md * s3[1] : sdq;
         if (fabs(dq) < 1.0e-30 || !isfinite(dq)) { error = FLURSYS_ERR_BREAKDOWN; break; }
         const double alpha = rz_old / dq;
         if (!isfinite(alpha)) { error = FLURSYS_ERR_BREAKDOWN; break; }
@@ -275,10 +309,12 @@ __device__ void pcg_instance(Ctx &k, double *red) {
                 s_r += double(rv);
             }
             double v[2] = {s_x, s_r};
-            write_parts(k, v, 2, red);
+            write_parts<2>(k, v, red);
             if (!grid_sync(in.barrier, nb)) return;
-            mx = read_sum(k, 0, red) / cnt;
-            mr = read_sum(k, 1, red) / cnt;
+            double s2[2];
+            read_sums<2>(k, s2, red);
+            mx = s2[0] / cnt;
+            mr = s2[1] / cnt;
         }
         // ---- pass 3: projection, residual, z, r.z ----
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
@@ -310,8 +346,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         {
             double v[4] = {s_rr, s_z, s_rz, s_r};
-            write_parts(k, v, 4, red);
-            write_max(k, 4, s_max, red);
+            write_parts_max<4>(k, v, s_max, red);
         }
         if (!grid_sync(in.barrier, nb)) return;
         double rz_new;
@@ -344,10 +379,12 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     }
     {
         double v[1] = {s_true};
-        write_parts(k, v, 1, red);
+        write_parts<1>(k, v, red);
     }
     if (!grid_sync(in.barrier, nb)) return;
-    const double true_rr = read_sum(k, 0, red);
+    double st1[1];
+    read_sums<1>(k, st1, red);
+    const double true_rr = st1[0];
     if (k.lb == 0 && threadIdx.x == 0) {
         PcgResultDev *res = in.result;
         res->error = error;
@@ -431,7 +468,7 @@ __device__ void sor_instance(Ctx &k, double *red) {
 
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock, 4) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kParts * (kBlock / 32)];
     int id = 0;
     for (int t = 0; t < ninst; ++t)
         if ((int)blockIdx.x >= insts[t].block0) id = t;
