@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "pcg3d.cuh"
 #include "pcg3d_seq.cuh"
+#include "tma.cuh"
 
 namespace flursys {
 
@@ -57,7 +58,7 @@ struct SeqArgs {
     const double *rhs;
     void *r, *d0, *d1, *q;
     float *dx;
-    double *partials;  // nblocks * 4
+    double *partials;  // nblocks * kSlots
     CgSeqState *st;
     const unsigned char *row_class;
     cudaGraphConditionalHandle h_loop, h_replace;
@@ -69,6 +70,12 @@ struct SeqArgs {
     int graph;   // 1: kernels run inside the solve graph and set its conditionals
     int sweep;   // stencil scheme of the operand pass (kSweep*)
     int nblocks_dir;  // grid of the operand pass
+    // single-reduction variant (MIXED): buffer sets 0/1 of r and p alternate
+    // per iteration; dx is updated in place
+    float *cr[2], *cp[2];
+    int cg1;          // 1: single-reduction variant
+    int cg1_tz;       // planes per tile of its step kernel (4 or 8)
+    int nblocks_cg1;  // grid of its step kernel
 };
 
 enum SweepKind : int { kSweepWarp = 0, kSweepTile = 1, kSweepDirect = 2, kSweepVec = 3 };
@@ -81,18 +88,20 @@ __device__ __forceinline__ void set_cond(const SeqArgs &a, cudaGraphConditionalH
 
 __device__ __forceinline__ int miss(int i, int n) { return (i == 0) + (i == n - 1); }
 
-// Writes this block's partials; returns true in the block that arrives last.
-template <int NV>
-__device__ __forceinline__ bool reduce_arrive(const double (&v)[NV], double *partials, unsigned *counter,
-                                              double *red) {
+constexpr int kSlots = 8;  // partial-sum slots per block
+
+// Writes this block's NS sums (slots 0..NS-1) and, with MAX, the block
+// maximum of mx (slot NS); returns true in the block that arrives last.
+template <int NS, bool MAX>
+__device__ __forceinline__ bool arrive_n(double (&v)[NS], double mx, double *partials, unsigned *counter,
+                                         double *red) {
     __shared__ bool s_last;
     const int nb = gridDim.x;
-    double t[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) t[k] = k == 2 ? block_max<kBlock>(v[k], red) : block_sum<kBlock>(v[k], red);
+    block_reduce_n<kBlock, NS, MAX>(v, mx, red);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) partials[blockIdx.x * 4 + k] = t[k];
+        for (int k = 0; k < NS; ++k) partials[blockIdx.x * kSlots + k] = v[k];
+        if (MAX) partials[blockIdx.x * kSlots + NS] = mx;
         __threadfence();
         const unsigned prev = atomicAdd(counter, 1u);
         s_last = prev == (unsigned)nb - 1u;
@@ -102,19 +111,49 @@ __device__ __forceinline__ bool reduce_arrive(const double (&v)[NV], double *par
     return s_last;
 }
 
-// Fixed-order sums over all blocks' partials (slot 2 is a max).
-template <int NV>
-__device__ __forceinline__ void reduce_finish(double (&out)[NV], const double *partials, double *red) {
+// Fixed-order sums (and maximum) over all blocks' partials.
+template <int NS, bool MAX>
+__device__ __forceinline__ void finish_n(double (&out)[NS], double &mx, const double *partials, double *red) {
     const int nb = gridDim.x;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double s = 0.0;
-        for (int b = threadIdx.x; b < nb; b += kBlock) {
-            const double p = __ldcg(partials + b * 4 + k);
-            s = k == 2 ? fmax(s, p) : s + p;
-        }
-        out[k] = k == 2 ? block_max<kBlock>(s, red) : block_sum<kBlock>(s, red);
+    for (int k = 0; k < NS; ++k) out[k] = 0.0;
+    mx = 0.0;
+    for (int b = threadIdx.x; b < nb; b += kBlock) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) out[k] += __ldcg(partials + b * kSlots + k);
+        if (MAX) mx = fmax(mx, __ldcg(partials + b * kSlots + NS));
     }
+    block_reduce_n<kBlock, NS, MAX>(out, mx, red);
+}
+
+// NV = 1: one sum. NV = 3: sums in slots 0 and 1, a maximum in slot 2.
+template <int NV>
+__device__ __forceinline__ bool reduce_arrive(const double (&v)[NV], double *partials, unsigned *counter,
+                                              double *red) {
+    static_assert(NV == 1 || NV == 3, "one sum, or two sums and a maximum");
+    if (NV == 1) {
+        double t[1] = {v[0]};
+        return arrive_n<1, false>(t, 0.0, partials, counter, red);
+    }
+    double t[2] = {v[0], v[NV > 1 ? 1 : 0]};
+    return arrive_n<2, true>(t, v[NV > 2 ? 2 : 0], partials, counter, red);
+}
+
+template <int NV>
+__device__ __forceinline__ void reduce_finish(double (&out)[NV], const double *partials, double *red) {
+    static_assert(NV == 1 || NV == 3, "one sum, or two sums and a maximum");
+    double mx;
+    if (NV == 1) {
+        double t[1];
+        finish_n<1, false>(t, mx, partials, red);
+        out[0] = t[0];
+        return;
+    }
+    double t[2];
+    finish_n<2, true>(t, mx, partials, red);
+    out[0] = t[0];
+    out[NV > 1 ? 1 : 0] = t[1];
+    out[NV > 2 ? 2 : 0] = mx;
 }
 
 // One tile of the 2.5D sweep (see pcg3d.cu). Raw inputs are prefetched two
@@ -356,9 +395,8 @@ __device__ __forceinline__ bool stop_ok(const SeqArgs &a, double res, double thr
 
 // Residual r = b - A x (FP64) over one tile with its sums; shared by init and replace.
 template <typename V, bool MIXED>
-__device__ __forceinline__ void residual_tile(const SeqArgs &a, void *tile, double &srr, double &srz, double &smax,
-                                              bool zero_dx) {
-    V *r = static_cast<V *>(a.r);
+__device__ __forceinline__ void residual_tile(const SeqArgs &a, V *r, void *tile, double &srr, double &srz,
+                                              double &smax, bool zero_dx) {
     const SeqGeo &g = a.g;
     tile_sweep(
         g, blockIdx.x, tile, [&](int c) -> double { return a.x[c]; },
@@ -378,10 +416,10 @@ __device__ __forceinline__ void residual_tile(const SeqArgs &a, void *tile, doub
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_init(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     double srr = 0.0, srz = 0.0, smax = 0.0;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.x[0] = 0.0;
-    residual_tile<V, MIXED>(a, tile, srr, srz, smax, true);
+    residual_tile<V, MIXED>(a, static_cast<V *>(a.r), tile, srr, srz, smax, true);
     const double v[3] = {srr, srz, smax};
     if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
     double o[3];
@@ -411,7 +449,7 @@ __global__ void __launch_bounds__(kBlock) seq_init(SeqArgs a) {
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_dir_spmv(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     const CgSeqState *s = a.st;
     if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
     const double beta = s->beta;
@@ -489,7 +527,7 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
     using VT = typename VecOf<V>::T;
     constexpr int W = VecOf<V>::W;
     constexpr int XW = 32 * W;
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     __shared__ V idg[27];
     const SeqGeo &g = a.g;
     if (threadIdx.x < 27) idg[threadIdx.x] = V(g.inv_diag[threadIdx.x]);
@@ -679,7 +717,7 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
 
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     const CgSeqState *s = a.st;
     if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
     const double alpha = s->alpha;
@@ -808,10 +846,10 @@ __global__ void __launch_bounds__(kBlock) seq_fold(SeqArgs a) {
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_replace(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     if (!a.graph && !a.st->replace) return;  // host-driven mode: no replacement due
     double srr = 0.0, srz = 0.0, smax = 0.0;
-    residual_tile<V, MIXED>(a, tile, srr, srz, smax, true);
+    residual_tile<V, MIXED>(a, static_cast<V *>(a.r), tile, srr, srz, smax, true);
     const double v[3] = {srr, srz, smax};
     if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
     double o[3];
@@ -844,7 +882,7 @@ __global__ void __launch_bounds__(kBlock) seq_replace(SeqArgs a) {
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_final(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[kSlots * (kBlock / 32)];
     double s_true = 0.0;
     tile_sweep(
         a.g, blockIdx.x, tile, [&](int c) -> double { return a.x[c]; },
@@ -876,13 +914,377 @@ __global__ void __launch_bounds__(kBlock) seq_fold_pending(SeqArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Single-reduction PCG (MIXED): one stencil launch per iteration.
+//
+// The vectors are those of the standard PCG (u = M r with M the Jacobi
+// inverse, p_i = u_i + beta_{i-1} p_{i-1}, s_i = A p_i, x += alpha_i p_i,
+// r_{i+1} = r_i - alpha_i s_i), computed in the same precisions; only the
+// scalars are rearranged so that an iteration needs one global reduction.
+// The launch of iteration i also forms u_{i+1} and w_{i+1} = A u_{i+1}, and
+// the denominator of the next step is expanded exactly (A symmetric on the
+// unpinned cells, where p and u live):
+//   (p_{i+1}, A p_{i+1}) = delta + 2 b e + b^2 f,
+//   delta = (u_{i+1}, w_{i+1}), e = (u_{i+1}, s_i), f = (p_i, s_i),
+// with b = beta_i rounded to FP32 as in the formation of p_{i+1}. So one
+// sweep yields gamma_{i+1} = r.M r, ||r||, max|r|, delta, e, f; its last
+// block sets beta_i = gamma_{i+1} / gamma_i and alpha_{i+1}.
+//
+// w needs u_{i+1} one cell around a cell, u_{i+1} needs s_i there, and s_i
+// needs p_i one cell further. Each block owns a 32 x 8 x TZ tile: one TMA box
+// load brings r_i and p_{i-1} on the tile plus two cells (R2; the box starts
+// four cells early in x for 16-byte alignment, and the hardware fills cells
+// outside the grid with zeros) and dx of the tile into shared memory; then,
+// separated by block barriers, p_i on R2 (in place), s_i, r_{i+1} and u_{i+1}
+// on the tile plus one cell (R1; u replaces r in place, the owned cells write
+// r, p and dx to the other buffer set), and w = A u on the tile. Halo values
+// repeat the owners' arithmetic with the same correctly rounded operations
+// (explicit fma / mul intrinsics), so they are bit-identical. r and p
+// alternate between two buffer sets (set iterations & 1 is read, the other
+// written). Per iteration a cell costs 24 B of compulsory traffic (read r, p,
+// dx; write r, p, dx) against 40 B for the two-launch form; the halo re-reads
+// are served by L2. Needs nx % 4 == 0 (TMA row stride); other grids take the
+// two-launch form.
+// The FP64 residual replacement (every `replace_every` iterations and before
+// accepting convergence) folds dx into x, recomputes r = b - A x, then delta,
+// e and f of the replaced state.
+// ---------------------------------------------------------------------------
+// 7-point operator row with a fixed operation order.
+__device__ __forceinline__ float cg1_row(float c, float xm, float xp, float ym, float yp, float zm, float zp, float wxm,
+                                         float wxp, float wym, float wyp, float wzm, float wzp) {
+    const float dg = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(wxm, wxp), wym), wyp), wzm), wzp);
+    float nb = __fmul_rn(wxm, xm);
+    nb = __fmaf_rn(wxp, xp, nb);
+    nb = __fmaf_rn(wym, ym, nb);
+    nb = __fmaf_rn(wyp, yp, nb);
+    nb = __fmaf_rn(wzm, zm, nb);
+    nb = __fmaf_rn(wzp, zp, nb);
+    return __fmaf_rn(dg, c, -nb);
+}
+
+// beta_i and alpha_{i+1} from the sums of an iteration (or of a replacement);
+// marks the solve done on the iteration cap or a breakdown.
+__device__ __forceinline__ void cg1_next(const SeqArgs &a, CgSeqState *w, double gam, double del, double e,
+                                         double f) {
+    if (fabs(w->rz_old) < 1.0e-30 || w->iterations >= a.max_iters) {
+        w->done = 1;
+        return;
+    }
+    const double beta = gam / w->rz_old;
+    const double bf = double(float(beta));  // p_{i+1} = u + float(beta) p_i
+    const double den = del + 2.0 * bf * e + bf * bf * f;
+    const double alpha = gam / den;
+    if (fabs(den) < 1.0e-30 || !isfinite(den) || !isfinite(alpha)) {
+        w->error = FLURSYS_ERR_BREAKDOWN;
+        w->done = 1;
+        w->alpha = 0.0;
+        return;
+    }
+    w->beta = beta;
+    w->alpha = alpha;
+    w->rz_old = gam;
+    w->first = 0;
+}
+
+// Last block of a step launch: o = {gamma, ||r||^2, e, f, delta}, mx = max|r|.
+__device__ __forceinline__ void cg1_step_finish(const SeqArgs &a, const double (&o)[5], double mx) {
+    CgSeqState *w = a.st;
+    w->counter = 0;
+    w->iterations += 1;
+    const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
+    const double res = l2 ? sqrt(o[1]) : mx;
+    w->residual = res;
+    if (!isfinite(res)) {
+        w->error = FLURSYS_ERR_NON_FINITE;
+        w->done = 1;
+        set_cond(a, a.h_replace, 0u);
+        set_cond(a, a.h_loop, 0u);
+        return;
+    }
+    const bool conv = stop_ok(a, res, w->threshold);
+    if (conv || (w->iterations % a.replace_every) == 0) {
+        w->replace = 1;
+        w->rz_new = o[0];
+        set_cond(a, a.h_replace, 1u);
+        return;  // the replacement launches take the decision
+    }
+    set_cond(a, a.h_replace, 0u);
+    cg1_next(a, w, o[0], o[4], o[2], o[3]);
+    set_cond(a, a.h_loop, w->done ? 0u : 1u);
+}
+
+// Tensor maps of the step kernel: r and p (both buffer sets) with the halo
+// box, dx with the tile box.
+struct Cg1Maps {
+    CUtensorMap r[2], p[2], dx;
+};
+
+template <int TZ>
+struct Cg1Tile {
+    static constexpr int BX = TX + 8, BY = TY + 4, BZ = TZ + 4;  // halo box (x from i0 - 4)
+    static constexpr int PL = BX * BY;                            // one box plane
+    static constexpr int BOX = PL * BZ;
+    static constexpr int TILE = TX * TY * TZ;
+    static constexpr size_t smem_bytes = sizeof(float) * (2 * BOX + TILE) + 128;  // + alignment slack
+};
+
+constexpr long long kTmaWaitLimit = 4'000'000LL;  // polls of ~64 ns: well above any legitimate wait
+
+// The step kernel (one launch per iteration).
+template <int TZ>
+__global__ void __launch_bounds__(kBlock, 4) cg1_tile(const __grid_constant__ SeqArgs a, const __grid_constant__ Cg1Maps m) {
+    using L = Cg1Tile<TZ>;
+    constexpr int BX = L::BX, PL = L::PL;
+    extern __shared__ unsigned char dyn[];
+    float *Rs = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~uintptr_t(127));
+    float *Ps = Rs + L::BOX;
+    float *Ds = Ps + L::BOX;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ float idg[27];
+    __shared__ double red[kSlots * (kBlock / 32)];
+    __shared__ int s_bad;
+    const SeqGeo &g = a.g;
+    const CgSeqState *st = a.st;
+    if (!a.graph && st->done) return;  // host-driven mode: the solve has finished
+    const double alpha = st->alpha;
+    const float vbeta = float(st->beta);
+    const bool first = st->first != 0;
+    const int par = (int)(st->iterations & 1);
+    float *rB = par ? a.cr[0] : a.cr[1];
+    float *pB = par ? a.cp[0] : a.cp[1];
+    float *dxv = a.dx;
+    const int bid = blockIdx.x;
+    const int i0 = (bid % g.tiles_x) * TX;
+    const int j0 = ((bid / g.tiles_x) % g.tiles_y) * TY;
+    const int k0 = (bid / (g.tiles_x * g.tiles_y)) * TZ;
+    const int tid = threadIdx.x;
+    if (tid < 27) idg[tid] = float(g.inv_diag[tid]);
+    if (tid == 0) {
+        s_bad = 0;
+        mbar_init(&bar, 1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&bar, sizeof(float) * ((first ? 1 : 2) * L::BOX + L::TILE));
+        tma_load_3d(Rs, &m.r[par], i0 - 4, j0 - 2, k0 - 2, &bar);
+        if (!first) tma_load_3d(Ps, &m.p[par], i0 - 4, j0 - 2, k0 - 2, &bar);
+        tma_load_3d(Ds, &m.dx, i0, j0, k0, &bar);
+    }
+    if (!mbar_wait_bounded(&bar, 0, kTmaWaitLimit)) {
+        s_bad = 1;
+        mbar_wait_bounded(&bar, 0, kTmaWaitLimit);  // let copies in flight land before the block moves on
+    }
+    __syncthreads();
+    const bool bad = s_bad != 0;
+    const float wx = float(g.ix2), wy = float(g.iy2), wz = float(g.iz2);
+    double sg = 0.0, srr = 0.0, smx = 0.0, se = 0.0, sf = 0.0, sd = 0.0;
+    if (!bad) {
+        // z class of each box plane (missing neighbours in z), shared by all columns
+        auto zmiss = [&](int gk) { return miss(gk, g.nz); };
+        // (1) p_i on R2: columns -2..33, rows -2..9, planes -2..TZ+1 of the
+        // tile. The pinned cell needs no case: r = 0 and p_{i-1} = 0 there.
+        for (int q = tid; q < (TX + 4) * (TY + 4); q += kBlock) {
+            const int x = q % (TX + 4), y = q / (TX + 4);
+            const int gi = i0 - 2 + x, gj = j0 - 2 + y;
+            const float *idc = idg + 9 * miss(gi, g.nx) + 3 * miss(gj, g.ny);
+            const int s0 = y * BX + x + 2;
+#pragma unroll
+            for (int z = 0; z < TZ + 4; ++z) {
+                const int sc = z * PL + s0;
+                const float u = __fmul_rn(Rs[sc], idc[zmiss(k0 - 2 + z)]);
+                Ps[sc] = first ? u : __fmaf_rn(vbeta, Ps[sc], u);
+            }
+        }
+        __syncthreads();
+        // (2) s_i = A p_i, r_{i+1}, u_{i+1} on R1: columns -1..32, rows -1..8,
+        // planes -1..TZ; owned cells write r_{i+1}, p_i, dx and their sums.
+        // The pinned cell's identity row gives s = p = 0 there, hence r and u
+        // stay 0.
+        for (int q = tid; q < (TX + 2) * (TY + 2); q += kBlock) {
+            const int x = q % (TX + 2), y = q / (TX + 2);
+            const int gi = i0 - 1 + x, gj = j0 - 1 + y;
+            const bool inxy = gi >= 0 && gi < g.nx && gj >= 0 && gj < g.ny;
+            const float wxm = inxy && gi > 0 ? wx : 0.f, wxp = inxy && gi + 1 < g.nx ? wx : 0.f;
+            const float wym = inxy && gj > 0 ? wy : 0.f, wyp = inxy && gj + 1 < g.ny ? wy : 0.f;
+            const float *idc = idg + 9 * miss(gi, g.nx) + 3 * miss(gj, g.ny);
+            const bool pcol = gi == 0 && gj == 0;
+            const bool own_xy = inxy && x >= 1 && x <= TX && y >= 1 && y <= TY;
+            const int s0 = (y + 1) * BX + x + 3;
+            const int cg0 = own_xy ? gj * g.nx + gi : 0;
+            const float *dsc = Ds + (y - 1) * TX + (x - 1);
+            float pb = Ps[s0], pc = Ps[PL + s0];
+#pragma unroll
+            for (int z = 0; z < TZ + 2; ++z) {
+                const int gk = k0 - 1 + z;
+                const int sc = (z + 1) * PL + s0;
+                const float pa = Ps[sc + PL];
+                const bool inz = gk >= 0 && gk < g.nz;
+                const float wzm = inz && gk > 0 ? wz : 0.f, wzp = inz && gk + 1 < g.nz ? wz : 0.f;
+                float s = cg1_row(pc, Ps[sc - 1], Ps[sc + 1], Ps[sc - BX], Ps[sc + BX], pb, pa, wxm, wxp, wym, wyp, wzm,
+                                  wzp);
+                if (pcol && gk == 0) s = 0.f;
+                const float rn = float(__fma_rn(-alpha, double(s), double(Rs[sc])));
+                const float id = idc[zmiss(gk)];
+                const float u = __fmul_rn(rn, id);
+                if (z >= 1 && z <= TZ && own_xy && inz) {
+                    const int c = cg0 + gk * g.nxy;
+                    rB[c] = rn;
+                    pB[c] = pc;
+                    dxv[c] = float(double(dsc[(z - 1) * TX * TY]) + alpha * double(pc));
+                    const double rd = rn;
+                    sg += rd * rd * double(id);
+                    srr += rd * rd;
+                    smx = fmax(smx, fabs(rd));
+                    se += double(u) * double(s);
+                    sf += double(pc) * double(s);
+                }
+                Rs[sc] = u;  // read at this cell only in this phase
+                pb = pc;
+                pc = pa;
+            }
+        }
+        __syncthreads();
+        // (3) w = A u_{i+1} on the tile: delta (the pinned row is the identity, w = u = 0)
+        {
+            const int x = tid % TX, y = tid / TX;
+            const int gi = i0 + x, gj = j0 + y;
+            if (gi < g.nx && gj < g.ny) {
+                const float wxm = gi > 0 ? wx : 0.f, wxp = gi + 1 < g.nx ? wx : 0.f;
+                const float wym = gj > 0 ? wy : 0.f, wyp = gj + 1 < g.ny ? wy : 0.f;
+                const bool pcol = gi == 0 && gj == 0;
+                const int s0 = (y + 2) * BX + x + 4;
+                float ub = Rs[PL + s0], uc = Rs[2 * PL + s0];
+#pragma unroll
+                for (int z = 0; z < TZ; ++z) {
+                    const int gk = k0 + z;
+                    const int sc = (z + 2) * PL + s0;
+                    const float ua = Rs[sc + PL];
+                    const float wzm = gk > 0 ? wz : 0.f, wzp = gk + 1 < g.nz ? wz : 0.f;
+                    float w = cg1_row(uc, Rs[sc - 1], Rs[sc + 1], Rs[sc - BX], Rs[sc + BX], ub, ua, wxm, wxp, wym, wyp,
+                                      wzm, wzp);
+                    if (pcol && gk == 0) w = 0.f;
+                    if (gk < g.nz) sd += double(uc) * double(w);
+                    ub = uc;
+                    uc = ua;
+                }
+            }
+        }
+    }
+    if (bad && tid == 0) atomicExch(&a.st->error, (int)FLURSYS_ERR_TIMEOUT);
+    double v[5] = {sg, srr, se, sf, sd};
+    if (!arrive_n<5, true>(v, smx, a.partials, &a.st->counter, red)) return;
+    double o[5], mx;
+    finish_n<5, true>(o, mx, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        if (w->error) {
+            w->counter = 0;
+            w->done = 1;
+            set_cond(a, a.h_replace, 0u);
+            set_cond(a, a.h_loop, 0u);
+            return;
+        }
+        cg1_step_finish(a, o, mx);
+    }
+}
+
+// FP64 residual replacement of the single-reduction variant: r = b - A x into
+// the set the next step reads (x already holds the folded increment).
+__global__ void __launch_bounds__(kBlock) cg1_replace_r(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kSlots * (kBlock / 32)];
+    if (!a.graph && a.st->replace != 1) return;  // host-driven mode: no replacement due
+    float *r = (a.st->iterations & 1) ? a.cr[1] : a.cr[0];
+    double srr = 0.0, srz = 0.0, smax = 0.0;
+    residual_tile<float, true>(a, r, tile, srr, srz, smax, true);
+    const double v[3] = {srr, srz, smax};
+    if (!reduce_arrive<3>(v, a.partials, &a.st->counter, red)) return;
+    double o[3];
+    reduce_finish<3>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
+        const double res = l2 ? sqrt(o[0]) : o[2];
+        w->residual = res;
+        if (!isfinite(res)) {
+            w->error = FLURSYS_ERR_NON_FINITE;
+            w->done = 1;
+        } else if (stop_ok(a, res, w->threshold)) {
+            w->status = FLURSYS_LINEAR_CONVERGED;
+            w->done = 1;
+        } else if (fabs(w->rz_old) < 1.0e-30 || w->iterations >= a.max_iters) {
+            w->done = 1;
+        } else {
+            w->rz_new = o[1];
+        }
+        w->replace = w->done ? 0 : 2;
+        set_cond(a, a.h_loop, w->done ? 0u : 1u);
+    }
+}
+
+// delta = (u, A u) with u = M r of the current set, and with MODE 1 also
+// e = (u, A p) and f = (p, A p) of the current p; then the step
+// coefficients. MODE 0 follows the initial residual (alpha_0 = gamma_0 /
+// delta_0, p_0 = u_0), MODE 1 a residual replacement.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) cg1_ws(SeqArgs a) {
+    __shared__ double tile[(TY + 2) * (TX + 2)];
+    __shared__ double red[kSlots * (kBlock / 32)];
+    const CgSeqState *st = a.st;
+    if (st->done) return;                                   // converged at the start or the replacement
+    if (MODE == 1 && !a.graph && st->replace != 2) return;  // host-driven mode: no replacement due
+    const bool par = (st->iterations & 1) != 0;
+    const float *r = par ? a.cr[1] : a.cr[0];
+    const float *p = par ? a.cp[1] : a.cp[0];
+    const SeqGeo &g = a.g;
+    double sd = 0.0, se = 0.0, sf = 0.0;
+    tile_sweep(
+        g, blockIdx.x, tile, [&](int c) -> float { return r[c]; },
+        [&](float v, int cls, bool pin) -> float { return pin ? 0.f : __fmul_rn(v, float(g.inv_diag[cls])); },
+        [&](int, int, bool, float u, float w) { sd += double(u) * double(w); });
+    if (MODE == 1) {
+        tile_sweep(
+            g, blockIdx.x, tile, [&](int c) -> float { return p[c]; },
+            [&](float v, int, bool pin) -> float { return pin ? 0.f : v; },
+            [&](int c, int cls, bool pin, float pc, float s) {
+                const float u = pin ? 0.f : __fmul_rn(r[c], float(g.inv_diag[cls]));
+                se += double(u) * double(s);
+                sf += double(pc) * double(s);
+            });
+    }
+    double v[3] = {sd, se, sf};
+    if (!arrive_n<3, false>(v, 0.0, a.partials, &a.st->counter, red)) return;
+    double o[3], mx;
+    finish_n<3, false>(o, mx, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        if (MODE == 0) {
+            const double alpha = w->rz_old / o[0];
+            if (fabs(o[0]) < 1.0e-30 || !isfinite(o[0]) || !isfinite(alpha)) {
+                w->error = FLURSYS_ERR_BREAKDOWN;
+                w->done = 1;
+                w->alpha = 0.0;
+                set_cond(a, a.h_loop, 0u);
+            } else {
+                w->alpha = alpha;
+            }
+        } else {
+            w->replace = 0;
+            cg1_next(a, w, w->rz_new, o[0], o[1], o[2]);
+            set_cond(a, a.h_loop, w->done ? 0u : 1u);
+        }
+    }
+}
+
 cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t ndeps,
-                       const void *fn, int grid, void **args) {
+                       const void *fn, int grid, void **args, unsigned smem = 0) {
     cudaKernelNodeParams p{};
     p.func = const_cast<void *>(fn);
     p.gridDim = dim3(grid);
     p.blockDim = dim3(kBlock);
-    p.sharedMemBytes = 0;
+    p.sharedMemBytes = smem;
     p.kernelParams = args;
     p.extra = nullptr;
     return cudaGraphAddKernelNode(node, g, deps, ndeps, &p);
@@ -953,6 +1355,62 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
     return cudaGraphInstantiate(&plan.exec, g, 0);
 }
 
+// Graph of the single-reduction variant (MIXED):
+//   init -> ws<0> -> WHILE(continue) { step -> IF(replace) { fold -> replace_r -> ws<1> } }
+//        -> fold_pending -> final
+cudaError_t build_cg1(Pcg3dSeqPlan &plan, SeqArgs &a, const Cg1Maps &maps) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    plan.graph = g;
+    cudaGraphConditionalHandle hl;
+    e = cudaGraphConditionalHandleCreate(&hl, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    a.h_loop = hl;
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hl;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t n_while;
+    e = cudaGraphAddNode(&n_while, g, nullptr, 0, &wp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle hr;
+    e = cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    a.h_replace = hr;
+    void *args[] = {&a};
+    cudaGraphNode_t n_init, n_prime, n_step, n_if, n_pend, n_final;
+    e = add_kernel(g, &n_init, nullptr, 0, (const void *)seq_init<float, true>, a.nblocks_stencil, args);
+    if (e == cudaSuccess) e = add_kernel(g, &n_prime, &n_init, 1, (const void *)cg1_ws<0>, a.nblocks_stencil, args);
+    if (e == cudaSuccess) e = cudaGraphAddDependencies(g, &n_prime, &n_while, 1);
+    {
+        void *step_args[] = {&a, const_cast<Cg1Maps *>(&maps)};
+        const void *fn = a.cg1_tz == 4 ? (const void *)cg1_tile<4> : (const void *)cg1_tile<8>;
+        const unsigned smem = (unsigned)(a.cg1_tz == 4 ? Cg1Tile<4>::smem_bytes : Cg1Tile<8>::smem_bytes);
+        if (e == cudaSuccess) e = add_kernel(body, &n_step, nullptr, 0, fn, a.nblocks_cg1, step_args, smem);
+    }
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams ip{};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hr;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    e = cudaGraphAddNode(&n_if, body, &n_step, 1, &ip);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    cudaGraphNode_t n_fold, n_rep, n_ws;
+    e = add_kernel(rb, &n_fold, nullptr, 0, (const void *)seq_fold, a.nblocks_point, args);
+    if (e == cudaSuccess) e = add_kernel(rb, &n_rep, &n_fold, 1, (const void *)cg1_replace_r, a.nblocks_stencil, args);
+    if (e == cudaSuccess) e = add_kernel(rb, &n_ws, &n_rep, 1, (const void *)cg1_ws<1>, a.nblocks_stencil, args);
+    if (e == cudaSuccess) e = add_kernel(g, &n_pend, &n_while, 1, (const void *)seq_fold_pending, a.nblocks_point, args);
+    if (e == cudaSuccess)
+        e = add_kernel(g, &n_final, &n_pend, 1, (const void *)seq_final<float, true>, a.nblocks_stencil, args);
+    if (e != cudaSuccess) return e;
+    return cudaGraphInstantiate(&plan.exec, g, 0);
+}
+
 }  // namespace
 
 cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precision, int device) {
@@ -975,7 +1433,6 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     g.tiles_x = (g.nx + TX - 1) / TX;
     g.tiles_y = (g.ny + TY - 1) / TY;
-    const long long cols = (long long)g.tiles_x * g.tiles_y;
     // Chunk length in z: about `waves` waves of four resident blocks per SM,
     // at least `kc_min` planes per chunk (FLURSYS_KC overrides both sweeps).
     const char *kc_env = std::getenv("FLURSYS_KC");
@@ -1014,8 +1471,8 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.max_iters = args.max_iters;
     a.replace_every = args.replace_every > 0 ? args.replace_every : 50;
     const int nb = std::max({a.nblocks_stencil, a.nblocks_point, g.tiles_x * g.tiles_yw * g.chunksw,
-                             g.tiles_xv * g.tiles_yv * g.chunksv});
-    cudaError_t e = cudaMalloc(&plan.partials, sizeof(double) * 4 * nb);
+                             g.tiles_xv * g.tiles_yv * g.chunksv, g.tiles_x * g.tiles_y * ((g.nz + 3) / 4)});
+    cudaError_t e = cudaMalloc(&plan.partials, sizeof(double) * kSlots * nb);
     if (e == cudaSuccess) e = cudaMalloc(&plan.state, sizeof(CgSeqState));
     if (e == cudaSuccess) e = cudaMemset(plan.state, 0, sizeof(CgSeqState));
     if (e != cudaSuccess) return e;
@@ -1032,7 +1489,39 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.nblocks_dir = a.sweep == kSweepWarp ? g.tiles_x * g.tiles_yw * g.chunksw
                   : a.sweep == kSweepVec  ? g.tiles_xv * g.tiles_yv * g.chunksv
                                           : a.nblocks_stencil;
-    e = precision == FLURSYS_PRECISION_MIXED ? build<float, true>(plan, a) : build<double, false>(plan, a);
+    // FLURSYS_PCG_CG1=1 selects the single-reduction variant for MIXED when
+    // the TMA maps can be made (nx % 4 == 0); FLURSYS_CG1_TZ=4 selects
+    // 4-plane tiles (8 by default). It is not the default: on B200 at 128^3
+    // it takes 39.5 us per iteration against 32.5 us for the two-launch form
+    // (instruction-bound by the halo recomputation, 238 instructions per cell).
+    const char *cg1_env = std::getenv("FLURSYS_PCG_CG1");
+    a.cg1 = precision == FLURSYS_PRECISION_MIXED && g.nx % 4 == 0 && cg1_env && std::strcmp(cg1_env, "1") == 0;
+    Cg1Maps maps{};
+    if (a.cg1) {
+        a.cr[0] = static_cast<float *>(args.r);
+        a.cr[1] = static_cast<float *>(args.q);
+        a.cp[0] = static_cast<float *>(args.d0);
+        a.cp[1] = static_cast<float *>(args.d1);
+        const char *tz_env = std::getenv("FLURSYS_CG1_TZ");
+        a.cg1_tz = tz_env && std::atoi(tz_env) == 4 ? 4 : 8;
+        const unsigned tz = (unsigned)a.cg1_tz;
+        bool ok = true;
+        for (int b = 0; b < 2; ++b) {
+            ok = ok && tma_map_f32_3d(&maps.r[b], a.cr[b], g.nx, g.ny, g.nz, TX + 8, TY + 4, tz + 4);
+            ok = ok && tma_map_f32_3d(&maps.p[b], a.cp[b], g.nx, g.ny, g.nz, TX + 8, TY + 4, tz + 4);
+        }
+        ok = ok && tma_map_f32_3d(&maps.dx, args.dx, g.nx, g.ny, g.nz, TX, TY, tz);
+        if (!ok) return cudaErrorNotSupported;
+        a.nblocks_cg1 = g.tiles_x * g.tiles_y * ((g.nz + a.cg1_tz - 1) / a.cg1_tz);
+        const void *fn = a.cg1_tz == 4 ? (const void *)cg1_tile<4> : (const void *)cg1_tile<8>;
+        const int smem = (int)(a.cg1_tz == 4 ? Cg1Tile<4>::smem_bytes : Cg1Tile<8>::smem_bytes);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        plan.cg1_maps = new Cg1Maps(maps);
+        e = build_cg1(plan, a, maps);
+    } else {
+        e = precision == FLURSYS_PRECISION_MIXED ? build<float, true>(plan, a) : build<double, false>(plan, a);
+    }
     plan.host_args = new SeqArgs(a);
     const char *v = std::getenv("FLURSYS_PCG_VARIANT");
     if (v && std::strcmp(v, "host") == 0) plan.host_iterations = 1;
@@ -1053,6 +1542,27 @@ cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t st) {
     SeqArgs a = *static_cast<const SeqArgs *>(plan.host_args);
     a.graph = 0;
     const bool mixed = plan.precision == FLURSYS_PRECISION_MIXED;
+    if (a.cg1) {
+        seq_init<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+        cg1_ws<0><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+        int done = 0;
+        for (long long it = 0; it < a.max_iters && !done; it += 16) {
+            for (int j = 0; j < 16; ++j) {
+                const Cg1Maps &maps = *static_cast<const Cg1Maps *>(plan.cg1_maps);
+                if (a.cg1_tz == 4) cg1_tile<4><<<a.nblocks_cg1, kBlock, Cg1Tile<4>::smem_bytes, st>>>(a, maps);
+                else cg1_tile<8><<<a.nblocks_cg1, kBlock, Cg1Tile<8>::smem_bytes, st>>>(a, maps);
+                seq_fold<<<a.nblocks_point, kBlock, 0, st>>>(a);
+                cg1_replace_r<<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+                cg1_ws<1><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+            }
+            cudaError_t e = cudaMemcpyAsync(&done, &plan.state->done, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return e;
+        }
+        seq_fold_pending<<<a.nblocks_point, kBlock, 0, st>>>(a);
+        seq_final<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
+        return cudaGetLastError();
+    }
     if (mixed) seq_init<float, true><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
     else seq_init<double, false><<<a.nblocks_stencil, kBlock, 0, st>>>(a);
     int done = 0;
@@ -1089,6 +1599,7 @@ void pcg3d_seq_destroy(Pcg3dSeqPlan &plan) {
     if (plan.graph) cudaGraphDestroy(plan.graph);
     cudaFree(plan.partials);
     cudaFree(plan.state);
+    delete static_cast<Cg1Maps *>(plan.cg1_maps);
     plan = Pcg3dSeqPlan{};
 }
 

@@ -25,6 +25,7 @@ struct Pcg3dSeqPlan {
     int precision = 0;
     int host_iterations = 0;    // > 0: host-driven mode (diagnostics; FLURSYS_PCG_VARIANT=host)
     void *host_args = nullptr;  // argument block of the kernels
+    void *cg1_maps = nullptr;   // tensor maps of the single-reduction step kernel
 };
 
 // Builds and instantiates the solve graph for fixed buffers (args as for
