@@ -37,6 +37,7 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kParts = 8;
+constexpr int kU = 4;  // cells per thread per step of the plain-operator passes
 
 __device__ __forceinline__ bool solid(const uint8_t *f, int c) { return (f[c] & kCellSolid) != 0; }
 __device__ __forceinline__ bool ident(const uint8_t *f, int c) { return (f[c] & 3) != 0; }
@@ -156,6 +157,10 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     const double cnt = in.count_fluid > 0 ? double(in.count_fluid) : 1.0;
     const unsigned nb = in.nblocks;
     const int nx = in.nx;
+    // no solid or outlet cell: every row is a fluid row of the plain
+    // 5-point operator, so the passes skip the flag bytes
+    const bool plain = in.count_fluid == (long long)in.nx * in.ny;
+    const int lane = threadIdx.x & 31;
     auto bval = [&](int c) -> double {  // b of the system (before projection)
         const uint8_t fc = f[c];
         if (fc & kCellOutlet) return in.outlet_pressure;
@@ -268,18 +273,68 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             return first ? V(zm) : V(zm + beta * (double(dold[m]) - md_old));
         };
         double s_dq = 0.0, s_q = 0.0, s_d = 0.0;
-        for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
-            const int c = it.c, i = it.i, j = it.j;
-            const V dc = dn(c);
-            V qc = dc;
-            if (!ident(f, c)) {
-                qc = apply_row<V>(k, c, i, j, dc, dn);
-                s_q += double(qc);
-                s_d += double(dc);
+        if (plain) {
+            // U cells per thread per step, every load issued before use; x
+            // neighbours by shuffle (lanes hold consecutive cells), lane 0 /
+            // lane 31 and the range tail load theirs
+            const V wxv = V(in.idx2), wyv = V(in.idy2);
+            auto dpl = [&](int m) -> V {
+                const double zm = double(z[m]) - mz;
+                return first ? V(zm) : V(zm + beta * (double(dold[m]) - md_old));
+            };
+            CellIter it = first_cell(k);
+            while (__any_sync(0xffffffffu, it.c < k.c_end)) {
+                CellIter cs[kU];
+                V dc[kU], dN[kU], dS[kU], dE[kU], dW[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    cs[u] = it;
+                    const bool ok = it.c < k.c_end;
+                    const int c = ok ? it.c : k.c_end - 1;
+                    const int i = ok ? it.i : 0, j = ok ? it.j : 0;
+                    dc[u] = dpl(c);
+                    dN[u] = ok && j + 1 < in.ny ? dpl(c + nx) : V(0);
+                    dS[u] = ok && j > 0 ? dpl(c - nx) : V(0);
+                    const bool own_e = lane < 31 && it.c + 1 < k.c_end;
+                    dE[u] = ok && !own_e && i + 1 < nx ? dpl(c + 1) : V(0);
+                    dW[u] = ok && lane == 0 && i > 0 ? dpl(c - 1) : V(0);
+                    next_cell(k, it);
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const V e_sh = __shfl_down_sync(0xffffffffu, dc[u], 1);
+                    const V w_sh = __shfl_up_sync(0xffffffffu, dc[u], 1);
+                    const int c = cs[u].c, i = cs[u].i, j = cs[u].j;
+                    if (c >= k.c_end) continue;
+                    const V east = (lane < 31 && c + 1 < k.c_end) ? e_sh : dE[u];
+                    const V west = lane > 0 ? w_sh : dW[u];
+                    V dg = V(0), sn = V(0);
+                    if (i + 1 < nx) { dg += wxv; sn += wxv * east; }
+                    if (i > 0) { dg += wxv; sn += wxv * west; }
+                    if (j + 1 < in.ny) { dg += wyv; sn += wyv * dN[u]; }
+                    if (j > 0) { dg += wyv; sn += wyv * dS[u]; }
+                    const V qc = dg * dc[u] - sn;
+                    dcur[c] = dc[u];
+                    q[c] = qc;
+                    s_q += double(qc);
+                    s_d += double(dc[u]);
+                    s_dq += double(dc[u]) * double(qc);
+                }
             }
-            dcur[c] = dc;
-            q[c] = qc;
-            s_dq += double(dc) * double(qc);
+        } else {
+            for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
+                const int c = it.c, i = it.i, j = it.j;
+                const V dc = dn(c);
+                V qc = dc;
+                if (!ident(f, c)) {
+                    qc = apply_row<V>(k, c, i, j, dc, dn);
+                    s_q += double(qc);
+                    s_d += double(dc);
+                }
+                dcur[c] = dc;
+                q[c] = qc;
+                s_dq += double(dc) * double(qc);
+            }
         }
         {
             double v[3] = {s_dq, s_q, s_d};
@@ -298,15 +353,42 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         double mr = 0.0;
         if (proj) {
             double s_x = 0.0, s_r = 0.0;
-            for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-                if (ident(f, c)) continue;
-                const double dc = double(dcur[c]) - md;
-                const double xv = x[c] + alpha * dc;
-                const V rv = V(double(r[c]) - alpha * double(q[c]));
-                x[c] = xv;
-                r[c] = rv;
-                s_x += xv;
-                s_r += double(rv);
+            if (plain) {
+                for (int c0 = k.c_begin + threadIdx.x; c0 < k.c_end; c0 += kU * kBlock) {
+                    double xv[kU], dv[kU];
+                    V rv[kU], qv[kU];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) {
+                        const int c = c0 + u * kBlock;
+                        const bool ok = c < k.c_end;
+                        xv[u] = ok ? x[c] : 0.0;
+                        dv[u] = ok ? double(dcur[c]) : 0.0;
+                        rv[u] = ok ? r[c] : V(0);
+                        qv[u] = ok ? q[c] : V(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) {
+                        const int c = c0 + u * kBlock;
+                        if (c >= k.c_end) continue;
+                        const double xn = xv[u] + alpha * (dv[u] - md);
+                        const V rn = V(double(rv[u]) - alpha * double(qv[u]));
+                        x[c] = xn;
+                        r[c] = rn;
+                        s_x += xn;
+                        s_r += double(rn);
+                    }
+                }
+            } else {
+                for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
+                    if (ident(f, c)) continue;
+                    const double dc = double(dcur[c]) - md;
+                    const double xv = x[c] + alpha * dc;
+                    const V rv = V(double(r[c]) - alpha * double(q[c]));
+                    x[c] = xv;
+                    r[c] = rv;
+                    s_x += xv;
+                    s_r += double(rv);
+                }
             }
             double v[2] = {s_x, s_r};
             write_parts<2>(k, v, red);
@@ -318,6 +400,50 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         // ---- pass 3: projection, residual, z, r.z ----
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
+        if (plain) {
+            for (CellIter it = first_cell(k); it.c < k.c_end;) {
+                CellIter cs[kU];
+                double xv[kU], pv[kU];
+                V rv0[kU], qv[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    cs[u] = it;
+                    const bool ok = it.c < k.c_end;
+                    const int c = ok ? it.c : k.c_begin;
+                    xv[u] = x[c];
+                    rv0[u] = r[c];
+                    pv[u] = proj ? 0.0 : double(dcur[c]);
+                    qv[u] = proj ? V(0) : q[c];
+                    next_cell(k, it);
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int c = cs[u].c, i = cs[u].i, j = cs[u].j;
+                    if (c >= k.c_end) continue;
+                    double rv;
+                    if (proj) {
+                        x[c] = xv[u] - mx;
+                        rv = double(V(double(rv0[u]) - mr));
+                    } else {
+                        x[c] = xv[u] + alpha * pv[u];
+                        rv = double(V(double(rv0[u]) - alpha * double(qv[u])));
+                    }
+                    r[c] = V(rv);
+                    double dg = 0.0;
+                    if (i + 1 < nx) dg += in.idx2;
+                    if (i > 0) dg += in.idx2;
+                    if (j + 1 < in.ny) dg += in.idy2;
+                    if (j > 0) dg += in.idy2;
+                    const double zv = dg > 0.0 ? rv / dg : rv;
+                    s_z += zv;
+                    s_r += rv;
+                    z[c] = V(zv);
+                    s_rr += rv * rv;
+                    s_max = fmax(s_max, fabs(rv));
+                    s_rz += rv * double(V(zv));
+                }
+            }
+        } else
         for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
             const int c = it.c, i = it.i, j = it.j;
             double rv;
@@ -407,8 +533,8 @@ __device__ void sor_instance(Ctx &k, double *red) {
     double residual = INFINITY;
     long long its = 0;
     int error = 0;
-    for (long long it = 0; it < in.max_iters; ++it) {
-        its = it + 1;
+    for (long long sweep = 0; sweep < in.max_iters; ++sweep) {
+        its = sweep + 1;
         for (int color = 0; color < 2; ++color) {
             for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
                 const int c = it.c, i = it.i, j = it.j;
@@ -447,9 +573,9 @@ __device__ void sor_instance(Ctx &k, double *red) {
             const double lap = (pe - 2.0 * p0 + pw) * in.idx2 + (pn - 2.0 * p0 + ps) * in.idy2;
             m = fmax(m, fabs(lap - __ldg(in.rhs + c)));
         }
-        write_max(k, (int)(it & 1), m, red);
+        write_max(k, (int)(sweep & 1), m, red);
         if (!grid_sync(in.barrier, nb)) return;
-        residual = read_max(k, (int)(it & 1), red);
+        residual = read_max(k, (int)(sweep & 1), red);
         if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
         if (residual < in.tol) break;
     }
@@ -467,7 +593,7 @@ __device__ void sor_instance(Ctx &k, double *red) {
 }
 
 template <typename V, bool MIXED>
-__global__ void __launch_bounds__(kBlock, 4) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
+__global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
     __shared__ double red[kParts * (kBlock / 32)];
     int id = 0;
     for (int t = 0; t < ninst; ++t)
