@@ -14,7 +14,7 @@
 //       pool / up_add kernels, so fused and unfused paths agree bit for bit.
 //   conv_first  1 -> 16 channels (FP32 input, CUDA cores; training)
 //   conv_last   16 -> 1 channel (FP32 output, CUDA cores, staged tile; training)
-//   net_in_fused / net_out_fused  the full-resolution layers of inference,
+//   net_in_fused / net_out_interior + net_out_boundary  the full-resolution layers of inference,
 //               collapsed by linearity into composite stencils (see below)
 //   wgrad       dW[co][tap][ci] += sum_v dY[v][co] X[v + tap][ci] (CUDA cores,
 //               FP32, atomics per voxel chunk)
@@ -579,93 +579,207 @@ __global__ void pack_fused(const float *master, long long off_first, long long o
     }
 }
 
-// x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz).
-__global__ void __launch_bounds__(256) net_in_fused(const float *__restrict__ r, const float *__restrict__ fz,
-                                                    const double *scale_ptr, uint16_t *x2, int cx, int cy, int cz) {
-    __shared__ float k2[64][16];
-    for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x) k2[i % 64][i / 64] = fz[kFusedK2 + i];
-    __syncthreads();
-    const float scale = float(scale_ptr[0]);
+// x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz): one thread per
+// coarse cell, its 4 x 4 x 4 window of r read from a shared tile of one
+// coarse layer (float2, conflict-free), the 1024 weights a by-value
+// parameter (constant-bank operands of the unrolled FMAs).
+constexpr int kInCX = 32, kInCY = 8;                                        // coarse cells per block
+constexpr int kInWX = 2 * kInCX + 2, kInWY = 2 * kInCY + 2, kInWZ = 4;      // fine window
+__global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__restrict__ r, const double *scale_ptr,
+                                                              uint16_t *x2, int cx, int cy, int cz,
+                                                              const __grid_constant__ NetInParams P) {
+    __shared__ __align__(16) float win[kInWZ][kInWY][kInWX];
     const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
-    const long long n = (long long)cx * cy * cz;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
-        const int X = int(v % cx);
-        const long long t = v / cx;
-        const int Y = int(t % cy), Z = int(t / cy);
-        float acc[16];
-        #pragma unroll
-        for (int c = 0; c < 16; ++c) acc[c] = 0.f;
-        #pragma unroll 4
-        for (int o = 0; o < 64; ++o) {
-            const int x = 2 * X + (o & 3) - 1, y = 2 * Y + ((o >> 2) & 3) - 1, z = 2 * Z + (o >> 4) - 1;
-            if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) continue;
-            const float rv = __ldg(r + ((long long)z * ny + y) * nx + x);
-            #pragma unroll
-            for (int c = 0; c < 16; ++c) acc[c] = fmaf(k2[o][c], rv, acc[c]);
-        }
-        uint4 q[2];
-        uint16_t *h = reinterpret_cast<uint16_t *>(q);
-        #pragma unroll
-        for (int c = 0; c < 16; ++c) h[c] = f2bf(acc[c] * scale);
-        uint4 *o4 = reinterpret_cast<uint4 *>(x2 + v * 16);
-        o4[0] = q[0];
-        o4[1] = q[1];
+    const int X0 = blockIdx.x * kInCX, Y0 = blockIdx.y * kInCY, Z = blockIdx.z;
+    const int x0 = 2 * X0 - 1, y0 = 2 * Y0 - 1, z0 = 2 * Z - 1;
+    for (int i = threadIdx.x; i < kInWZ * kInWY * kInWX; i += blockDim.x) {
+        const int wx = i % kInWX, wy = (i / kInWX) % kInWY, wz = i / (kInWX * kInWY);
+        const int x = x0 + wx, y = y0 + wy, z = z0 + wz;
+        win[wz][wy][wx] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
+                              ? __ldg(r + ((long long)z * ny + y) * nx + x) : 0.f;
     }
+    __syncthreads();
+    const int tx = threadIdx.x % kInCX, ty = threadIdx.x / kInCX;
+    const int X = X0 + tx, Y = Y0 + ty;
+    if (X >= cx || Y >= cy) return;
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+#pragma unroll
+    for (int oz = 0; oz < 4; ++oz)
+#pragma unroll
+        for (int oy = 0; oy < 4; ++oy) {
+            // window columns 2 tx .. 2 tx + 3 (two float2)
+            const float *row = &win[oz][2 * ty + oy][2 * tx];
+            const float2 a = reinterpret_cast<const float2 *>(row)[0], b = reinterpret_cast<const float2 *>(row)[1];
+            const float v[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+            for (int ox = 0; ox < 4; ++ox)
+#pragma unroll
+                for (int c = 0; c < 16; ++c) acc[c] = fmaf(P.k2[((oz * 4 + oy) * 4 + ox) * 16 + c], v[ox], acc[c]);
+        }
+    const float scale = float(scale_ptr[0]);
+    uint4 q[2];
+    uint16_t *h = reinterpret_cast<uint16_t *>(q);
+#pragma unroll
+    for (int c = 0; c < 16; ++c) h[c] = f2bf(acc[c] * scale);
+    uint4 *o4 = reinterpret_cast<uint4 *>(x2 + (((long long)Z * cy + Y) * cx + X) * 16);
+    o4[0] = q[0];
+    o4[1] = q[1];
 }
 
-// z = (sum over 8 coarse cells of Wp * b2 + scale * K125[class] * r) * h2 / scale.
-constexpr int kOutTX = 32, kOutTY = 8;
-__global__ void __launch_bounds__(kOutTX * kOutTY) net_out_fused(const float *__restrict__ r,
-                                                                 const uint16_t *__restrict__ b2,
-                                                                 const float *__restrict__ fz, const double *scale_ptr,
-                                                                 double h2, float *out, int nx, int ny, int nz) {
-    __shared__ float tile[5][kOutTY + 4][kOutTX + 4];
-    __shared__ float k125[27 * 125];
-    __shared__ float wp[8 * 8 * 16];
-    for (int i = threadIdx.x; i < 27 * 125; i += blockDim.x) k125[i] = fz[kFusedK125 + i];
-    for (int i = threadIdx.x; i < 8 * 8 * 16; i += blockDim.x) wp[i] = fz[kFusedWp + i];
-    const int x0 = blockIdx.x * kOutTX, y0 = blockIdx.y * kOutTY, z = blockIdx.z;
-    for (int i = threadIdx.x; i < 5 * (kOutTY + 4) * (kOutTX + 4); i += blockDim.x) {
-        const int tx = i % (kOutTX + 4), ty = (i / (kOutTX + 4)) % (kOutTY + 4), tz = i / ((kOutTX + 4) * (kOutTY + 4));
-        const int x = x0 + tx - 2, y = y0 + ty - 2, zz = z + tz - 2;
-        tile[tz][ty][tx] = (x >= 0 && y >= 0 && zz >= 0 && x < nx && y < ny && zz < nz)
-                               ? __ldg(r + ((long long)zz * ny + y) * nx + x) : 0.f;
+// z = (sum over 8 coarse cells of Wp * b2 + scale * K125[class] * r) * h2 / scale,
+// in two launches. net_out_interior applies the interior-class stencil to
+// every cell: one thread per coarse cell computes its 2 x 2 x 2 fine cells,
+// reading their 6 x 6 x 6 window of r once (float2, conflict-free) from a
+// shared tile of one coarse layer and the 27 coarse neighbours of b2 once;
+// all taps are unrolled, so the weights (a by-value parameter) are
+// constant-bank operands. net_out_boundary then adds, on the cells of the
+// six faces, h2 * (K125[class] - K125[interior]) * r, the taps of c7 that
+// leave the domain.
+constexpr int kOutCX = 32, kOutCY = 8;                       // coarse cells per block
+constexpr int kOutWX = 2 * kOutCX + 4, kOutWY = 2 * kOutCY + 4, kOutWZ = 6;  // fine window
+constexpr int kFusedInterior = 13;                            // class 1 + 3 * 1 + 9 * 1
+__global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float *__restrict__ r,
+                                                                    const uint16_t *__restrict__ b2,
+                                                                    const double *scale_ptr, double h2, float *out,
+                                                                    int nx, int ny, int nz,
+                                                                    const __grid_constant__ NetOutParams P) {
+    __shared__ __align__(16) float win[kOutWZ][kOutWY][kOutWX];
+    const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
+    const int X0 = blockIdx.x * kOutCX, Y0 = blockIdx.y * kOutCY, Z = blockIdx.z;
+    const int x0 = 2 * X0 - 2, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
+    for (int i = threadIdx.x; i < kOutWZ * kOutWY * kOutWX; i += blockDim.x) {
+        const int wx = i % kOutWX, wy = (i / kOutWX) % kOutWY, wz = i / (kOutWX * kOutWY);
+        const int x = x0 + wx, y = y0 + wy, z = z0 + wz;
+        win[wz][wy][wx] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
+                              ? __ldg(r + ((long long)z * ny + y) * nx + x) : 0.f;
     }
     __syncthreads();
-    const int tx = threadIdx.x % kOutTX, ty = threadIdx.x / kOutTX;
-    const int x = x0 + tx, y = y0 + ty;
-    if (x >= nx || y >= ny) return;
-    const int cls = (x == 0 ? 0 : x + 1 == nx ? 2 : 1) + 3 * (y == 0 ? 0 : y + 1 == ny ? 2 : 1) +
-                    9 * (z == 0 ? 0 : z + 1 == nz ? 2 : 1);
-    const float *k = k125 + cls * 125;
-    float skip = 0.f;
-    #pragma unroll
-    for (int dz = 0; dz < 5; ++dz)
-        #pragma unroll
-        for (int dy = 0; dy < 5; ++dy)
-            #pragma unroll
-            for (int dx = 0; dx < 5; ++dx) skip = fmaf(k[dz * 25 + dy * 5 + dx], tile[dz][ty + dy][tx + dx], skip);
-    const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
-    const int px = x & 1, py = y & 1, pz = z & 1, par = px | (py << 1) | (pz << 2);
-    const int bxs = (x >> 1) - (px == 0), bys = (y >> 1) - (py == 0), bzs = (z >> 1) - (pz == 0);
-    float up = 0.f;
-    #pragma unroll
-    for (int c8 = 0; c8 < 8; ++c8) {
-        const int X = bxs + (c8 & 1), Y = bys + ((c8 >> 1) & 1), Z = bzs + (c8 >> 2);
-        if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
-        const uint4 *src = reinterpret_cast<const uint4 *>(b2 + (((long long)Z * cy + Y) * cx + X) * 16);
-        const uint4 qa = __ldg(src), qb = __ldg(src + 1);
-        const uint16_t *ha = reinterpret_cast<const uint16_t *>(&qa);
-        const uint16_t *hb = reinterpret_cast<const uint16_t *>(&qb);
-        const float *w = wp + (par * 8 + c8) * 16;
-        #pragma unroll
-        for (int j = 0; j < 8; ++j) up = fmaf(w[j], bf2f(ha[j]), up);
-        #pragma unroll
-        for (int j = 0; j < 8; ++j) up = fmaf(w[8 + j], bf2f(hb[j]), up);
+    const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
+    const int X = X0 + tx, Y = Y0 + ty;
+    if (X >= cx || Y >= cy) return;
+    // skip path: acc[f], f = fx + 2 fy + 4 fz
+    float acc[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) acc[f] = 0.f;
+#pragma unroll
+    for (int pz = 0; pz < 6; ++pz) {
+#pragma unroll
+        for (int py = 0; py < 6; ++py) {
+            const float2 *row = reinterpret_cast<const float2 *>(&win[pz][2 * ty + py][2 * tx]);
+            const float2 a = row[0], b = row[1], c = row[2];
+            const float v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
+#pragma unroll
+            for (int fz = 0; fz < 2; ++fz) {
+                const int dz = pz - 2 - fz;
+                if (dz < -2 || dz > 2) continue;
+#pragma unroll
+                for (int fy = 0; fy < 2; ++fy) {
+                    const int dy = py - 2 - fy;
+                    if (dy < -2 || dy > 2) continue;
+#pragma unroll
+                    for (int fx = 0; fx < 2; ++fx)
+#pragma unroll
+                        for (int dx = -2; dx <= 2; ++dx)
+                            acc[fx + 2 * fy + 4 * fz] =
+                                fmaf(P.k[((dz + 2) * 5 + dy + 2) * 5 + dx + 2], v[fx + dx + 2], acc[fx + 2 * fy + 4 * fz]);
+                }
+            }
+        }
     }
+    // up path: coarse neighbour (X + ox, Y + oy, Z + oz) feeds child f when
+    // o - (f == 0 ? -1 : 0) is 0 or 1 on every axis (that bit picks c8)
+    float up[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) up[f] = 0.f;
+#pragma unroll
+    for (int oz = -1; oz <= 1; ++oz)
+#pragma unroll
+        for (int oy = -1; oy <= 1; ++oy)
+#pragma unroll
+            for (int ox = -1; ox <= 1; ++ox) {
+                const int Xn = X + ox, Yn = Y + oy, Zn = Z + oz;
+                if (Xn < 0 || Yn < 0 || Zn < 0 || Xn >= cx || Yn >= cy || Zn >= cz) continue;
+                const uint4 *src = reinterpret_cast<const uint4 *>(b2 + (((long long)Zn * cy + Yn) * cx + Xn) * 16);
+                const uint4 qa = __ldg(src), qb = __ldg(src + 1);
+                const uint16_t *ha = reinterpret_cast<const uint16_t *>(&qa);
+                const uint16_t *hb = reinterpret_cast<const uint16_t *>(&qb);
+                float bv[16];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    bv[j] = bf2f(ha[j]);
+                    bv[8 + j] = bf2f(hb[j]);
+                }
+#pragma unroll
+                for (int fz = 0; fz < 2; ++fz)
+#pragma unroll
+                    for (int fy = 0; fy < 2; ++fy)
+#pragma unroll
+                        for (int fx = 0; fx < 2; ++fx) {
+                            const int bx = ox + (fx == 0 ? 1 : 0), by = oy + (fy == 0 ? 1 : 0), bz = oz + (fz == 0 ? 1 : 0);
+                            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+                            const int par = fx | (fy << 1) | (fz << 2), c8 = bx | (by << 1) | (bz << 2);
+                            const float *w = P.wp + (par * 8 + c8) * 16;
+                            float t = up[par];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) t = fmaf(w[j], bv[j], t);
+                            up[par] = t;
+                        }
+            }
     const double s = scale_ptr[0];
-    const long long v = ((long long)z * ny + y) * nx + x;
-    out[v] = s > 0.0 ? float((double(up) + s * double(skip)) * (h2 / s)) : 0.f;
+    const double fac = s > 0.0 ? h2 / s : 0.0;
+#pragma unroll
+    for (int fz = 0; fz < 2; ++fz)
+#pragma unroll
+        for (int fy = 0; fy < 2; ++fy) {
+            const long long v = ((long long)(2 * Z + fz) * ny + 2 * Y + fy) * nx + 2 * X;
+            float2 o;
+            o.x = float((double(up[2 * fy + 4 * fz]) + s * double(acc[2 * fy + 4 * fz])) * fac);
+            o.y = float((double(up[1 + 2 * fy + 4 * fz]) + s * double(acc[1 + 2 * fy + 4 * fz])) * fac);
+            *reinterpret_cast<float2 *>(out + v) = o;
+        }
+}
+
+// Cells of the six faces: out += h2 * (K125[class] - K125[interior]) * r.
+__global__ void __launch_bounds__(256) net_out_boundary(const float *__restrict__ r, const float *__restrict__ fz,
+                                                        const double *scale_ptr, double h2, float *out, int nx, int ny,
+                                                        int nz) {
+    __shared__ float k125[27 * 125];
+    for (int i = threadIdx.x; i < 27 * 125; i += blockDim.x) k125[i] = fz[kFusedK125 + i];
+    __syncthreads();
+    if (!(scale_ptr[0] > 0.0)) return;
+    const long long nzf = 2LL * nx * ny, nyf = 2LL * nx * (nz - 2), nxf = 2LL * (ny - 2) * (nz - 2);
+    const long long total = nzf + nyf + nxf;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        if (t < nzf) {  // z = 0 and z = nz - 1
+            const long long u = t % ((long long)nx * ny);
+            x = int(u % nx); y = int(u / nx); z = t < (long long)nx * ny ? 0 : nz - 1;
+        } else if (t < nzf + nyf) {  // y = 0 and y = ny - 1, 0 < z < nz - 1
+            const long long w = t - nzf, half = (long long)nx * (nz - 2);
+            const long long u = w % half;
+            x = int(u % nx); z = 1 + int(u / nx); y = w < half ? 0 : ny - 1;
+        } else {  // x = 0 and x = nx - 1, 0 < y < ny - 1, 0 < z < nz - 1
+            const long long w = t - nzf - nyf, half = (long long)(ny - 2) * (nz - 2);
+            const long long u = w % half;
+            y = 1 + int(u % (ny - 2)); z = 1 + int(u / (ny - 2)); x = w < half ? 0 : nx - 1;
+        }
+        const int cls = (x == 0 ? 0 : x + 1 == nx ? 2 : 1) + 3 * (y == 0 ? 0 : y + 1 == ny ? 2 : 1) +
+                        9 * (z == 0 ? 0 : z + 1 == nz ? 2 : 1);
+        const float *kc = k125 + cls * 125, *ki = k125 + kFusedInterior * 125;
+        float corr = 0.f;
+        for (int o = 0; o < 125; ++o) {
+            const int dx = o % 5 - 2, dy = (o / 5) % 5 - 2, dz = o / 25 - 2;
+            const int xx = x + dx, yy = y + dy, zz = z + dz;
+            if (xx < 0 || yy < 0 || zz < 0 || xx >= nx || yy >= ny || zz >= nz) continue;
+            const float d = kc[o] - ki[o];
+            if (d != 0.f) corr = fmaf(d, __ldg(r + ((long long)zz * ny + yy) * nx + xx), corr);
+        }
+        const long long v = ((long long)z * ny + y) * nx + x;
+        out[v] = float(double(out[v]) + h2 * double(corr));
+    }
 }
 
 __global__ void adam_kernel(float *w, const float *g, float *m, float *v, long long n, float lr, float b1, float b2,
@@ -847,6 +961,7 @@ cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st
     const long long n = net_param_count();
     pack_kernel<<<grid_1d(n), 256, 0, st>>>(master, w.fwd, w.bwd, w.fwd_f32, n);
     pack_fused<<<1, 256, 0, st>>>(master, net_param_offset(0), net_param_offset(kNetLayers - 1), w.fused);
+    w.host_params_valid = false;
     return cudaGetLastError();
 }
 
@@ -861,7 +976,24 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     scale_kernel<<<1, 256, 0, st>>>(ws.partials, np, n, ws.scalars);
     const int n2x = nx / 2, n2y = ny / 2, n2z = nz / 2, n3x = nx / 4, n3y = ny / 4, n3z = nz / 4;
     const int n4x = nx / 8, n4y = ny / 8, n4z = nz / 8;
-    net_in_fused<<<grid_1d((long long)n2x * n2y * n2z), 256, 0, st>>>(r, w.fused, ws.scalars, ws.x2, n2x, n2y, n2z);
+    if (!w.host_params_valid) {
+        // first application after a repack: bring the full-resolution layers' weights to the host
+        NetOutParams &P = w.out_params;
+        float k2[16 * 64];  // [channel][tap] as packed
+        e = cudaMemcpyAsync(k2, w.fused + kFusedK2, sizeof k2, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(P.k, w.fused + kFusedK125 + kFusedInterior * 125, sizeof P.k, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(P.wp, w.fused + kFusedWp, sizeof P.wp, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        for (int c = 0; c < 16; ++c)
+            for (int o = 0; o < 64; ++o) w.in_params.k2[o * 16 + c] = k2[c * 64 + o];
+        w.host_params_valid = true;
+    }
+    {
+        dim3 grid((n2x + kInCX - 1) / kInCX, (n2y + kInCY - 1) / kInCY, n2z);
+        net_in_fused<<<grid, kInCX * kInCY, 0, st>>>(r, ws.scalars, ws.x2, n2x, n2y, n2z, w.in_params);
+    }
     e = cudaGetLastError();
     const uint16_t *W = w.fwd;
     if (e == cudaSuccess) e = launch_conv<16, 32, kPlain>(Src{ws.x2, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
@@ -870,8 +1002,13 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     if (e == cudaSuccess) e = launch_conv<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
     if (e == cudaSuccess) e = launch_conv<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
     if (e == cudaSuccess) {
-        dim3 grid((nx + kOutTX - 1) / kOutTX, (ny + kOutTY - 1) / kOutTY, nz);
-        net_out_fused<<<grid, kOutTX * kOutTY, 0, st>>>(r, ws.b2, w.fused, ws.scalars, h2, z, nx, ny, nz);
+        dim3 grid((n2x + kOutCX - 1) / kOutCX, (n2y + kOutCY - 1) / kOutCY, n2z);
+        net_out_interior<<<grid, kOutCX * kOutCY, 0, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz, w.out_params);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        const long long faces = 2LL * nx * ny + 2LL * nx * (nz - 2) + 2LL * (ny - 2) * (nz - 2);
+        net_out_boundary<<<grid_1d(faces), 256, 0, st>>>(r, w.fused, ws.scalars, h2, z, nx, ny, nz);
         e = cudaGetLastError();
     }
     return e;

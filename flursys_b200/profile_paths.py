@@ -3,10 +3,11 @@ solver and the SIMPLE channel, for profilers (ncu launch lists, section
 captures) and quick timings.
 
     python -m flursys_b200.profile_paths fcgnet --size 256 --reps 2
+    python -m flursys_b200.profile_paths fcg --size 256 --steps 1
     python -m flursys_b200.profile_paths batch2d --instances 64 --steps 2
     python -m flursys_b200.profile_paths simple --nx 2048 --ny 512 --outer 1
 
-Launches per unit: fcgnet 9 kernels per application; batch2d 9 kernels per
+Launches per unit: fcgnet 10 kernels per application; batch2d 9 kernels per
 step (one graph launch); simple 1 kernel before the loop, then 12 kernels
 and 2 device copies per outer iteration.
 """
@@ -33,6 +34,24 @@ def run_fcgnet(size: int, reps: int) -> dict:
         net.apply(r, z, (n, n, n), 1.0 / (n * n))
     torch.cuda.synchronize()
     return {"size": n, "reps": reps, "ms_per_apply": (time.perf_counter() - t0) * 1e3 / reps}
+
+
+def run_fcg(size: int, steps: int) -> dict:
+    """`steps` 3D cavity steps (Re 400, central, mixed) with the learned FCG
+    pressure solve to 1e-8 relative, from the zero field."""
+    from .learned import DEFAULT_WEIGHTS
+    from .solver import BackendOptions, LidDrivenCavity3DConfig, _Handle
+    n = size
+    h = 1.0 / n
+    cfg = LidDrivenCavity3DConfig(nx=n, ny=n, nz=n, reynolds=400.0, dt=min(0.5 * h, 0.25 * h * h / (3 / 400.0)),
+                                  pressure_solver="fcg",
+                                  backend=BackendOptions(precision="mixed", stop_rule="rel-l2", pressure_rtol=1e-8,
+                                                         fcg_weights_path=DEFAULT_WEIGHTS))
+    hd = _Handle(cfg.to_c())
+    reps = [hd.step(1) for _ in range(steps)]
+    hd.close()
+    return {"size": n, "steps": steps, "iterations": [int(r.pressure_iterations) for r in reps],
+            "solve_ms": [r.pressure_solve_ms for r in reps]}
 
 
 def run_batch2d(instances: int, steps: int, seed: int = 2024) -> dict:
@@ -77,6 +96,9 @@ def main(argv=None) -> int:
     a = sub.add_parser("fcgnet")
     a.add_argument("--size", type=int, default=256)
     a.add_argument("--reps", type=int, default=2)
+    f = sub.add_parser("fcg")
+    f.add_argument("--size", type=int, default=256)
+    f.add_argument("--steps", type=int, default=1)
     b = sub.add_parser("batch2d")
     b.add_argument("--instances", type=int, default=64)
     b.add_argument("--steps", type=int, default=2)
@@ -87,6 +109,8 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.what == "fcgnet":
         out = run_fcgnet(args.size, args.reps)
+    elif args.what == "fcg":
+        out = run_fcg(args.size, args.steps)
     elif args.what == "batch2d":
         out = run_batch2d(args.instances, args.steps)
     else:
