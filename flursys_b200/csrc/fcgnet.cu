@@ -127,32 +127,55 @@ constexpr int conv_smem_bytes() {
     return (kHY * kHX * (CIN + kPad) + 9 * COUT * (CIN + kPad)) * 2;
 }
 
+__device__ __forceinline__ void ldsm_x4(uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3, const void *p) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+}
+
 // The 9 taps of one staged input plane (sIn: 18 x 10 halo tile, sW: the 9
 // taps' weights [t9][COUT][CIN + kPad]) accumulated into this warp's row of
-// 16 voxels x COUT channels.
+// 16 voxels x COUT channels. Fragments come from ldmatrix.x4: lane l
+// addresses row (l & 7) + 8 ((l >> 3) & 1) at k offset 8 (l >> 4) of A
+// (voxels x channels), and row (l & 7) + 8 (l >> 4) at k offset
+// 8 ((l >> 3) & 1) of two 8-channel blocks of B; rows are 16-byte aligned
+// (CIN + kPad is a multiple of 8) and, with the padding, conflict-free.
+// Taps alternate between two accumulator sets (acc for even t9, acc2 for
+// odd) so that each warp has twice as many independent MMA chains in flight.
 template <int CIN, int COUT>
-__device__ __forceinline__ void mma_plane(const uint16_t *sIn, const uint16_t *sW, float (&acc)[COUT / 8][4], int warp,
-                                          int g, int tig) {
-    #pragma unroll 1
-    for (int t9 = 0; t9 < 9; ++t9) {
-        const int dy = t9 / 3, dx = t9 % 3;  // halo-relative offsets 0..2
-        const uint16_t *rowA = sIn + ((warp + dy) * kHX + dx) * (CIN + kPad);
-        const uint16_t *wt = sW + t9 * COUT * (CIN + kPad);
+__device__ __forceinline__ void mma_tap(const uint16_t *sIn, const uint16_t *sW, float (&acc)[COUT / 8][4], int warp,
+                                        int t9, int a_row, int a_k, int b_row, int b_k) {
+    const int dy = t9 / 3, dx = t9 % 3;  // halo-relative offsets 0..2
+    const uint16_t *rowA = sIn + ((warp + dy) * kHX + dx) * (CIN + kPad);
+    const uint16_t *wt = sW + t9 * COUT * (CIN + kPad);
+    #pragma unroll
+    for (int kc = 0; kc < CIN; kc += 16) {
+        uint32_t a0, a1, a2, a3;
+        ldsm_x4(a0, a1, a2, a3, rowA + a_row * (CIN + kPad) + kc + a_k);
         #pragma unroll
-        for (int kc = 0; kc < CIN; kc += 16) {
-            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + tig * 2);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + tig * 2);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(rowA + g * (CIN + kPad) + kc + 8 + tig * 2);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(rowA + (g + 8) * (CIN + kPad) + kc + 8 + tig * 2);
-            #pragma unroll
-            for (int n = 0; n < COUT / 8; ++n) {
-                const uint16_t *wb = wt + (n * 8 + g) * (CIN + kPad) + kc + tig * 2;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wb);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wb + 8);
-                mma_bf16(acc[n], a0, a1, a2, a3, b0, b1);
-            }
+        for (int n = 0; n < COUT / 8; n += 2) {
+            uint32_t b0, b1, b2, b3;
+            ldsm_x4(b0, b1, b2, b3, wt + (n * 8 + b_row) * (CIN + kPad) + kc + b_k);
+            mma_bf16(acc[n], a0, a1, a2, a3, b0, b1);
+            mma_bf16(acc[n + 1], a0, a1, a2, a3, b2, b3);
         }
     }
+}
+
+template <int CIN, int COUT>
+__device__ __forceinline__ void mma_plane(const uint16_t *sIn, const uint16_t *sW, float (&acc)[COUT / 8][4],
+                                          float (&acc2)[COUT / 8][4], int warp, int g, int tig) {
+    static_assert(COUT % 16 == 0, "B fragments are loaded two 8-channel blocks at a time");
+    const int lane = threadIdx.x & 31;
+    const int a_row = (lane & 7) + 8 * ((lane >> 3) & 1), a_k = 8 * (lane >> 4);
+    const int b_row = (lane & 7) + 8 * (lane >> 4), b_k = 8 * ((lane >> 3) & 1);
+    #pragma unroll 1
+    for (int t9 = 0; t9 < 8; t9 += 2) {
+        mma_tap<CIN, COUT>(sIn, sW, acc, warp, t9, a_row, a_k, b_row, b_k);
+        mma_tap<CIN, COUT>(sIn, sW, acc2, warp, t9 + 1, a_row, a_k, b_row, b_k);
+    }
+    mma_tap<CIN, COUT>(sIn, sW, acc, warp, 8, a_row, a_k, b_row, b_k);
 }
 
 // Stores this warp's row of 16 voxels x COUT channels of plane z as BF16.
@@ -208,13 +231,19 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc_z(Src src, const uint16_
     for (int z = z0; z < z1; ++z) {
         stage_tile<CIN, MODE>(sIn + ((z - z0 + 2) % 3) * kPlane, src, x0, y0, z + 1, nx, ny, nz);
         __syncthreads();
-        float acc[COUT / 8][4];
+        float acc[COUT / 8][4], acc2[COUT / 8][4];
         #pragma unroll
-        for (int n = 0; n < COUT / 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+        for (int n = 0; n < COUT / 8; ++n)
+            #pragma unroll
+            for (int e = 0; e < 4; ++e) acc[n][e] = acc2[n][e] = 0.f;
         #pragma unroll 1
         for (int dz = 0; dz < 3; ++dz)
-            mma_plane<CIN, COUT>(sIn + ((z - z0 + dz) % 3) * kPlane, sW + dz * 9 * COUT * (CIN + kPad), acc, warp, g,
-                                 tig);
+            mma_plane<CIN, COUT>(sIn + ((z - z0 + dz) % 3) * kPlane, sW + dz * 9 * COUT * (CIN + kPad), acc, acc2,
+                                 warp, g, tig);
+        #pragma unroll
+        for (int n = 0; n < COUT / 8; ++n)
+            #pragma unroll
+            for (int e = 0; e < 4; ++e) acc[n][e] += acc2[n][e];
         store_row<COUT>(acc, out, x0, y0 + warp, z, nx, ny, g, tig);
         __syncthreads();  // the slot of plane z - 1 is staged next
     }
@@ -229,9 +258,11 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc(Src src, const uint16_t 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tig = lane & 3;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z = blockIdx.z;
-    float acc[COUT / 8][4];
+    float acc[COUT / 8][4], acc2[COUT / 8][4];
     #pragma unroll
-    for (int n = 0; n < COUT / 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+    for (int n = 0; n < COUT / 8; ++n)
+        #pragma unroll
+        for (int e = 0; e < 4; ++e) acc[n][e] = acc2[n][e] = 0.f;
 
     for (int dz = 0; dz < 3; ++dz) {
         __syncthreads();
@@ -244,8 +275,12 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc(Src src, const uint16_t 
             *reinterpret_cast<uint4 *>(sW + (t9 * COUT + co) * (CIN + kPad) + k8 * 8) = q;
         }
         __syncthreads();
-        mma_plane<CIN, COUT>(sIn, sW, acc, warp, g, tig);
+        mma_plane<CIN, COUT>(sIn, sW, acc, acc2, warp, g, tig);
     }
+    #pragma unroll
+    for (int n = 0; n < COUT / 8; ++n)
+        #pragma unroll
+        for (int e = 0; e < 4; ++e) acc[n][e] += acc2[n][e];
     store_row<COUT>(acc, out, x0, y0 + warp, z, nx, ny, g, tig);
 }
 
