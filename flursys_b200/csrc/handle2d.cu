@@ -137,6 +137,7 @@ struct Handle2D {
     uint8_t *flags = nullptr;
     Pcg2dInstance *inst_dev = nullptr;
     Pcg2dInstance inst{};
+    bool cluster = false;  // the pressure solve runs as one thread-block cluster
     Diag2Dev *h_diag = nullptr;
     int nblocks = 0;
 };
@@ -372,6 +373,21 @@ int32_t init2d(FlursysCudaHandle *h) {
     long long per_block = 512;
     if (const char *env = std::getenv("FLURSYS_2D_CELLS_PER_BLOCK")) per_block = std::max(1LL, std::atoll(env));
     in.nblocks = (int)std::max(1LL, std::min<long long>(h->pcg.grid, ((long long)nc + per_block - 1) / per_block));
+    // A small system without solid or outlet cells (at most 8 cells per
+    // thread) runs as one thread-block cluster instead: the hardware cluster
+    // barrier replaces the software grid barrier. FLURSYS_2D_CLUSTER=0 keeps
+    // the grid path.
+    {
+        const char *cl_env = std::getenv("FLURSYS_2D_CLUSTER");
+        const int maxc = pcg2d_max_cluster(c.precision);
+        const long long threads = (long long)maxc * pcg2d_block_size();
+        if (!(cl_env && std::strcmp(cl_env, "0") == 0) && fluid == (long long)nc && (long long)nc <= 8 * threads &&
+            maxc <= h->pcg.grid) {
+            h2->cluster = true;
+            in.nblocks = (int)std::max(1LL, std::min<long long>(maxc, ((long long)nc + pcg2d_block_size() - 1) /
+                                                                          pcg2d_block_size()));
+        }
+    }
     in.partials = h->pcg.partials;
     in.barrier = h->pcg.barrier;
     in.result = h->pcg.result;
@@ -436,7 +452,9 @@ int32_t step2d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (e == cudaSuccess) e = cavity2d_rhs(s, s.rho / (relax * step_dt), st);
     if (e == cudaSuccess) e = cudaEventRecord(h->ev[1], st);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->pcg.barrier, 0, sizeof(GridBarrier), st);
-    if (e == cudaSuccess) e = pcg2d_launch(h2->inst_dev, 1, h2->inst.nblocks, c.precision, st);
+    if (e == cudaSuccess)
+        e = h2->cluster ? pcg2d_launch_cluster(h2->inst_dev, h2->inst.nblocks, c.precision, st)
+                        : pcg2d_launch(h2->inst_dev, 1, h2->inst.nblocks, c.precision, st);
     if (e == cudaSuccess) e = cudaEventRecord(h->ev[2], st);
     if (e == cudaSuccess) e = cavity2d_correct(s, relax * step_dt / s.rho, st);
     if (simple && e == cudaSuccess) e = cavity2d_simple_relax(s, c.pressure_relaxation, st);

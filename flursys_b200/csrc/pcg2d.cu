@@ -39,6 +39,23 @@ constexpr int kBlock = 256;
 constexpr int kParts = 8;
 constexpr int kU = 4;  // cells per thread per step of the plain-operator passes
 
+// Barriers between the passes of one instance: the bounded software grid
+// barrier over the instance's blocks, or, when the instance runs as one
+// thread-block cluster, the hardware cluster barrier (release / acquire at
+// cluster scope, so the partials and vectors written before it are visible
+// after it in every block of the cluster).
+struct GridSync {
+    GridBarrier *bar;
+    unsigned nb;
+    __device__ __forceinline__ bool operator()() const { return grid_sync(bar, nb); }
+};
+struct ClusterSync {
+    __device__ __forceinline__ bool operator()() const {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        return true;
+    }
+};
+
 __device__ __forceinline__ bool solid(const uint8_t *f, int c) { return (f[c] & kCellSolid) != 0; }
 __device__ __forceinline__ bool ident(const uint8_t *f, int c) { return (f[c] & 3) != 0; }
 
@@ -107,7 +124,7 @@ __device__ __forceinline__ void read_sums(const Ctx &k, double (&out)[NV], doubl
     for (int p = 0; p < NV; ++p) out[p] = 0.0;
     for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock)
 #pragma unroll
-        for (int p = 0; p < NV; ++p) out[p] += k.in.partials[b * kParts + p];
+        for (int p = 0; p < NV; ++p) out[p] += __ldcg(k.in.partials + b * kParts + p);
     block_sum_n<kBlock, NV>(out, red);
 }
 // write_parts plus the block maximum of mx into column NV.
@@ -128,14 +145,14 @@ __device__ __forceinline__ void read_sums_max(const Ctx &k, double (&out)[NV], d
     mx = 0.0;
     for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) {
 #pragma unroll
-        for (int p = 0; p < NV; ++p) out[p] += k.in.partials[b * kParts + p];
-        mx = fmax(mx, k.in.partials[b * kParts + NV]);
+        for (int p = 0; p < NV; ++p) out[p] += __ldcg(k.in.partials + b * kParts + p);
+        mx = fmax(mx, __ldcg(k.in.partials + b * kParts + NV));
     }
     block_reduce_n<kBlock, NV, true>(out, mx, red);
 }
 __device__ __forceinline__ double read_max(const Ctx &k, int p, double *red) {
     double s = 0.0;
-    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s = fmax(s, k.in.partials[b * kParts + p]);
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s = fmax(s, __ldcg(k.in.partials + b * kParts + p));
     return block_max<kBlock>(s, red);
 }
 __device__ __forceinline__ void write_max(const Ctx &k, int p, double v, double *red) {
@@ -143,8 +160,8 @@ __device__ __forceinline__ void write_max(const Ctx &k, int p, double v, double 
     if (threadIdx.x == 0) k.in.partials[k.lb * kParts + p] = t;
 }
 
-template <typename V, bool MIXED>
-__device__ void pcg_instance(Ctx &k, double *red) {
+template <typename V, bool MIXED, typename Sync>
+__device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
     const Pcg2dInstance &in = k.in;
     const uint8_t *f = in.flags;
     double *x = in.x;
@@ -155,7 +172,6 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     const bool proj = in.project != 0;
     const bool l2 = in.stop_rule == FLURSYS_STOP_REL_L2;
     const double cnt = in.count_fluid > 0 ? double(in.count_fluid) : 1.0;
-    const unsigned nb = in.nblocks;
     const int nx = in.nx;
     // no solid or outlet cell: every row is a fluid row of the plain
     // 5-point operator, so the passes skip the flag bytes
@@ -189,7 +205,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         double v[2] = {sx, sb};
         write_parts<2>(k, v, red);
     }
-    if (!grid_sync(in.barrier, nb)) return;
+    if (!sync()) return;
     double m0[2];
     read_sums<2>(k, m0, red);
     double mx = proj ? m0[0] / cnt : 0.0;
@@ -197,7 +213,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     if (proj) {
         for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
             if (!ident(f, c)) x[c] -= mx;
-        if (!grid_sync(in.barrier, nb)) return;
+        if (!sync()) return;
     }
 
     // ---- r = b' - A x (FP64), projected; residual; z; r.z ----
@@ -214,7 +230,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         double v[1] = {sr};
         write_parts<1>(k, v, red);
-        if (!grid_sync(in.barrier, nb)) return false;
+        if (!sync()) return false;
         double m1[1];
         read_sums<1>(k, m1, red);
         const double mr = proj ? m1[0] / cnt : 0.0;
@@ -240,7 +256,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         }
         double v2[4] = {s_rr, s_z, s_rz, s_r};
         write_parts_max<4>(k, v2, s_max, red);
-        return grid_sync(in.barrier, nb);
+        return sync();
     };
     auto read_residual_sums = [&](double &rr, double &rmax, double &rz) {
         double s4[4];
@@ -340,7 +356,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             double v[3] = {s_dq, s_q, s_d};
             write_parts<3>(k, v, red);
         }
-        if (!grid_sync(in.barrier, nb)) return;
+        if (!sync()) return;
         double s3[3];
         read_sums<3>(k, s3, red);
         const double sdq = s3[0];
@@ -392,7 +408,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             }
             double v[2] = {s_x, s_r};
             write_parts<2>(k, v, red);
-            if (!grid_sync(in.barrier, nb)) return;
+            if (!sync()) return;
             double s2[2];
             read_sums<2>(k, s2, red);
             mx = s2[0] / cnt;
@@ -474,7 +490,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
             double v[4] = {s_rr, s_z, s_rz, s_r};
             write_parts_max<4>(k, v, s_max, red);
         }
-        if (!grid_sync(in.barrier, nb)) return;
+        if (!sync()) return;
         double rz_new;
         read_residual_sums(rr, rmax, rz_new);
         residual = l2 ? sqrt(rr) : rmax;
@@ -495,7 +511,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         first = false;
     }
     // ---- final FP64 check ||b' - A x||_2 over fluid rows ----
-    if (!grid_sync(in.barrier, nb)) return;
+    if (!sync()) return;
     double s_true = 0.0;
     for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
         const int c = it.c, i = it.i, j = it.j;
@@ -507,7 +523,7 @@ __device__ void pcg_instance(Ctx &k, double *red) {
         double v[1] = {s_true};
         write_parts<1>(k, v, red);
     }
-    if (!grid_sync(in.barrier, nb)) return;
+    if (!sync()) return;
     double st1[1];
     read_sums<1>(k, st1, red);
     const double true_rr = st1[0];
@@ -524,11 +540,11 @@ __device__ void pcg_instance(Ctx &k, double *red) {
     }
 }
 
-__device__ void sor_instance(Ctx &k, double *red) {
+template <typename Sync>
+__device__ void sor_instance(Ctx &k, double *red, const Sync &sync) {
     const Pcg2dInstance &in = k.in;
     const uint8_t *f = in.flags;
     double *p = in.x;
-    const unsigned nb = in.nblocks;
     const int nx = in.nx;
     double residual = INFINITY;
     long long its = 0;
@@ -552,14 +568,14 @@ __device__ void sor_instance(Ctx &k, double *red) {
                     p[c] = old + in.omega * ((s - __ldg(in.rhs + c)) / ap - old);
                 }
             }
-            if (!grid_sync(in.barrier, nb)) return;
+            if (!sync()) return;
         }
         if (in.project && in.ref_cell >= 0) {
             const double pr = p[in.ref_cell];
-            if (!grid_sync(in.barrier, nb)) return;
+            if (!sync()) return;
             for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock)
                 if (!solid(f, c)) p[c] -= pr;
-            if (!grid_sync(in.barrier, nb)) return;
+            if (!sync()) return;
         }
         double m = 0.0;
         for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
@@ -574,7 +590,7 @@ __device__ void sor_instance(Ctx &k, double *red) {
             m = fmax(m, fabs(lap - __ldg(in.rhs + c)));
         }
         write_max(k, (int)(sweep & 1), m, red);
-        if (!grid_sync(in.barrier, nb)) return;
+        if (!sync()) return;
         residual = read_max(k, (int)(sweep & 1), red);
         if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
         if (residual < in.tol) break;
@@ -592,24 +608,42 @@ __device__ void sor_instance(Ctx &k, double *red) {
     }
 }
 
-template <typename V, bool MIXED>
-__global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
-    __shared__ double red[kParts * (kBlock / 32)];
-    int id = 0;
-    for (int t = 0; t < ninst; ++t)
-        if ((int)blockIdx.x >= insts[t].block0) id = t;
-    Ctx k;
-    k.in = insts[id];
-    k.lb = (int)blockIdx.x - k.in.block0;
-    if (k.lb >= k.in.nblocks) return;  // spare block of the launch
+__device__ __forceinline__ void make_ctx(Ctx &k, const Pcg2dInstance &in, int lb) {
+    k.in = in;
+    k.lb = lb;
     k.n = k.in.nx * k.in.ny;
     const int chunk = (k.n + k.in.nblocks - 1) / k.in.nblocks;
     k.c_begin = k.lb * chunk;
     k.c_end = k.c_begin + chunk < k.n ? k.c_begin + chunk : k.n;
     k.step_j = kBlock / k.in.nx;
     k.step_i = kBlock - k.step_j * k.in.nx;
-    if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red);
-    else pcg_instance<V, MIXED>(k, red);
+}
+
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
+    __shared__ double red[kParts * (kBlock / 32)];
+    int id = 0;
+    for (int t = 0; t < ninst; ++t)
+        if ((int)blockIdx.x >= insts[t].block0) id = t;
+    const int lb = (int)blockIdx.x - insts[id].block0;
+    if (lb >= insts[id].nblocks) return;  // spare block of the launch
+    Ctx k;
+    make_ctx(k, insts[id], lb);
+    const GridSync sync{k.in.barrier, (unsigned)k.in.nblocks};
+    if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red, sync);
+    else pcg_instance<V, MIXED>(k, red, sync);
+}
+
+// One instance as one thread-block cluster (grid = cluster = nblocks): the
+// passes are separated by the hardware cluster barrier.
+template <typename V, bool MIXED>
+__global__ void __launch_bounds__(kBlock, 3) pcg2d_cluster_kernel(const Pcg2dInstance *__restrict__ inst) {
+    __shared__ double red[kParts * (kBlock / 32)];
+    Ctx k;
+    make_ctx(k, inst[0], (int)blockIdx.x);
+    const ClusterSync sync{};
+    if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red, sync);
+    else pcg_instance<V, MIXED>(k, red, sync);
 }
 
 }  // namespace
@@ -625,6 +659,48 @@ cudaError_t pcg2d_max_grid(int precision, int device, int *grid) {
     if (e != cudaSuccess) return e;
     *grid = sms * per_sm;
     return cudaSuccess;
+}
+
+int pcg2d_max_cluster(int precision) {
+    const void *fn = precision == FLURSYS_PRECISION_MIXED ? (const void *)pcg2d_cluster_kernel<float, true>
+                                                          : (const void *)pcg2d_cluster_kernel<double, false>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 8;  // the portable cluster size
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kBlock);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int size = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&size, fn, &cfg) != cudaSuccess || size < 1) {
+        cudaGetLastError();
+        return 8;
+    }
+    return size;
+}
+
+cudaError_t pcg2d_launch_cluster(const Pcg2dInstance *inst_dev, int nblocks, int precision, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = nblocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (precision == FLURSYS_PRECISION_MIXED) return cudaLaunchKernelEx(&cfg, pcg2d_cluster_kernel<float, true>, inst_dev);
+    return cudaLaunchKernelEx(&cfg, pcg2d_cluster_kernel<double, false>, inst_dev);
 }
 
 int pcg2d_block_size() { return kBlock; }

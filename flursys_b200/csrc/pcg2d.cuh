@@ -47,5 +47,11 @@ int pcg2d_num_partials();
 // Launches one cooperative grid over all instances (device array `inst`).
 cudaError_t pcg2d_launch(const Pcg2dInstance *inst_dev, int ninst, int total_blocks, int precision,
                          cudaStream_t stream);
+// Largest thread-block cluster the 2D solver kernel can run as (16 where the
+// device allows non-portable sizes, else 8).
+int pcg2d_max_cluster(int precision);
+// Launches one instance (device pointer) as a single cluster of `nblocks`
+// blocks, its passes separated by the hardware cluster barrier.
+cudaError_t pcg2d_launch_cluster(const Pcg2dInstance *inst_dev, int nblocks, int precision, cudaStream_t stream);
 
 }  // namespace flursys

@@ -164,3 +164,25 @@ def test_stencil_pcg_2d_entry_matches_oracle(oracle, cudalib, precision):
                                           C.byref(opts), C.byref(rep))
     assert st == 0 and rep.status == _abi.LINEAR_CONVERGED
     assert rel_l2(x, xref) < (1e-9 if precision == _abi.PRECISION_F64 else 1e-7)
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_F64, _abi.PRECISION_MIXED])
+def test_cluster_and_grid_barrier_paths_agree(oracle, monkeypatch, precision):
+    # A 128^2 cavity without solids runs its pressure solve as one thread-block
+    # cluster (hardware cluster barrier); FLURSYS_2D_CLUSTER=0 forces the
+    # software grid barrier. Same system, same stop rule: same iteration
+    # counts and fields to rounding.
+    cfg = cfg2d(oracle, 128, 128, stop_rule=_abi.STOP_REL_L2, pressure_rtol=1e-8, precision=precision)
+    runs = []
+    for env in ("1", "0"):
+        monkeypatch.setenv("FLURSYS_2D_CLUSTER", env)
+        g = _Handle(cfg)
+        reps = [g.step(1) for _ in range(3)]
+        runs.append((reps, {fid: g.download(fid) for fid, _ in FIELDS[:3]}))
+    monkeypatch.delenv("FLURSYS_2D_CLUSTER")
+    (rc, fc), (rg, fg) = runs
+    for a, b in zip(rc, rg):
+        assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
+        assert abs(a.pressure_iterations - b.pressure_iterations) <= 1
+    for fid, name in FIELDS[:3]:
+        assert rel_l2(fc[fid], fg[fid]) <= (1e-10 if precision == _abi.PRECISION_F64 else 1e-6), name
