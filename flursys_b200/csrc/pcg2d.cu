@@ -36,24 +36,39 @@ namespace flursys {
 namespace {
 
 constexpr int kBlock = 256;
-constexpr int kParts = 8;
+// Partial-sum columns per block: two sets of kRoundCols that alternate by
+// reduction round, so that a block never overwrites a set that a slower
+// block may still be reading (the next write to the same set is one
+// barrier further on).
+constexpr int kRoundCols = 8;
+constexpr int kParts = 2 * kRoundCols;
 constexpr int kU = 4;  // cells per thread per step of the plain-operator passes
 
-// Barriers between the passes of one instance: the bounded software grid
-// barrier over the instance's blocks, or, when the instance runs as one
-// thread-block cluster, the hardware cluster barrier (release / acquire at
-// cluster scope, so the partials and vectors written before it are visible
-// after it in every block of the cluster).
+// Barriers between the passes of one instance. GridSync: the bounded
+// software grid barrier over the instance's blocks. ClusterSync: the
+// instance runs as one thread-block cluster and the passes are separated by
+// the hardware cluster barrier (release / acquire at cluster scope, so
+// everything written before it is visible after it in every block of the
+// cluster). Either way the blocks' partial sums meet in global memory, read
+// through L2. (Partials in distributed shared memory measured no faster on
+// the 128^2 cavity and need a closing barrier to keep every block's shared
+// memory alive until the last read.)
 struct GridSync {
     GridBarrier *bar;
     unsigned nb;
+    double *partials;
     __device__ __forceinline__ bool operator()() const { return grid_sync(bar, nb); }
+    __device__ __forceinline__ void put(int lb, int col, double v) const { partials[lb * kParts + col] = v; }
+    __device__ __forceinline__ double get(int b, int col) const { return __ldcg(partials + b * kParts + col); }
 };
 struct ClusterSync {
+    double *partials;
     __device__ __forceinline__ bool operator()() const {
         asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
         return true;
     }
+    __device__ __forceinline__ void put(int lb, int col, double v) const { partials[lb * kParts + col] = v; }
+    __device__ __forceinline__ double get(int b, int col) const { return __ldcg(partials + b * kParts + col); }
 };
 
 __device__ __forceinline__ bool solid(const uint8_t *f, int c) { return (f[c] & kCellSolid) != 0; }
@@ -64,6 +79,7 @@ struct Ctx {
     int lb;  // block index within the instance
     int n, c_begin, c_end;
     int step_i, step_j;  // kBlock cells = step_j rows + step_i columns
+    int round;           // reduction rounds completed (selects the column set)
 };
 
 // A thread's walk over the cells of its block: c advances by kBlock and
@@ -109,55 +125,66 @@ __device__ __forceinline__ T apply_row(const Ctx &k, int c, int i, int j, T vc, 
     return dg * vc - s;
 }
 
-// Block partial sums of NV values into columns 0..NV-1 of this block's row.
-template <int NV>
-__device__ __forceinline__ void write_parts(const Ctx &k, double (&v)[NV], double *red) {
+// Block partial sums of NV values into columns 0..NV-1 of this round's set.
+template <int NV, typename Sync>
+__device__ __forceinline__ void write_parts(const Ctx &k, const Sync &sync, double (&v)[NV], double *red) {
     block_sum_n<kBlock, NV>(v, red);
+    const int base = (k.round & 1) * kRoundCols;
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int p = 0; p < NV; ++p) k.in.partials[k.lb * kParts + p] = v[p];
+        for (int p = 0; p < NV; ++p) sync.put(k.lb, base + p, v[p]);
 }
 // Sums over the instance's blocks of columns 0..NV-1, in block order.
-template <int NV>
-__device__ __forceinline__ void read_sums(const Ctx &k, double (&out)[NV], double *red) {
+template <int NV, typename Sync>
+__device__ __forceinline__ void read_sums(Ctx &k, const Sync &sync, double (&out)[NV], double *red) {
+    const int base = (k.round & 1) * kRoundCols;
 #pragma unroll
     for (int p = 0; p < NV; ++p) out[p] = 0.0;
     for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock)
 #pragma unroll
-        for (int p = 0; p < NV; ++p) out[p] += __ldcg(k.in.partials + b * kParts + p);
+        for (int p = 0; p < NV; ++p) out[p] += sync.get(b, base + p);
     block_sum_n<kBlock, NV>(out, red);
+    ++k.round;
 }
 // write_parts plus the block maximum of mx into column NV.
-template <int NV>
-__device__ __forceinline__ void write_parts_max(const Ctx &k, double (&v)[NV], double mx, double *red) {
+template <int NV, typename Sync>
+__device__ __forceinline__ void write_parts_max(const Ctx &k, const Sync &sync, double (&v)[NV], double mx,
+                                                double *red) {
     block_reduce_n<kBlock, NV, true>(v, mx, red);
+    const int base = (k.round & 1) * kRoundCols;
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int p = 0; p < NV; ++p) k.in.partials[k.lb * kParts + p] = v[p];
-        k.in.partials[k.lb * kParts + NV] = mx;
+        for (int p = 0; p < NV; ++p) sync.put(k.lb, base + p, v[p]);
+        sync.put(k.lb, base + NV, mx);
     }
 }
 // read_sums plus the maximum over blocks of column NV.
-template <int NV>
-__device__ __forceinline__ void read_sums_max(const Ctx &k, double (&out)[NV], double &mx, double *red) {
+template <int NV, typename Sync>
+__device__ __forceinline__ void read_sums_max(Ctx &k, const Sync &sync, double (&out)[NV], double &mx, double *red) {
+    const int base = (k.round & 1) * kRoundCols;
 #pragma unroll
     for (int p = 0; p < NV; ++p) out[p] = 0.0;
     mx = 0.0;
     for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) {
 #pragma unroll
-        for (int p = 0; p < NV; ++p) out[p] += __ldcg(k.in.partials + b * kParts + p);
-        mx = fmax(mx, __ldcg(k.in.partials + b * kParts + NV));
+        for (int p = 0; p < NV; ++p) out[p] += sync.get(b, base + p);
+        mx = fmax(mx, sync.get(b, base + NV));
     }
     block_reduce_n<kBlock, NV, true>(out, mx, red);
+    ++k.round;
 }
-__device__ __forceinline__ double read_max(const Ctx &k, int p, double *red) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s = fmax(s, __ldcg(k.in.partials + b * kParts + p));
-    return block_max<kBlock>(s, red);
-}
-__device__ __forceinline__ void write_max(const Ctx &k, int p, double v, double *red) {
+template <typename Sync>
+__device__ __forceinline__ void write_max(const Ctx &k, const Sync &sync, double v, double *red) {
     const double t = block_max<kBlock>(v, red);
-    if (threadIdx.x == 0) k.in.partials[k.lb * kParts + p] = t;
+    if (threadIdx.x == 0) sync.put(k.lb, (k.round & 1) * kRoundCols, t);
+}
+template <typename Sync>
+__device__ __forceinline__ double read_max(Ctx &k, const Sync &sync, double *red) {
+    const int col = (k.round & 1) * kRoundCols;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < k.in.nblocks; b += kBlock) s = fmax(s, sync.get(b, col));
+    ++k.round;
+    return block_max<kBlock>(s, red);
 }
 
 template <typename V, bool MIXED, typename Sync>
@@ -203,11 +230,11 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
             }
         }
         double v[2] = {sx, sb};
-        write_parts<2>(k, v, red);
+        write_parts<2>(k, sync, v, red);
     }
     if (!sync()) return;
     double m0[2];
-    read_sums<2>(k, m0, red);
+    read_sums<2>(k, sync, m0, red);
     double mx = proj ? m0[0] / cnt : 0.0;
     mb = proj ? m0[1] / cnt : 0.0;
     if (proj) {
@@ -229,10 +256,10 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
             r[c] = V(rv);
         }
         double v[1] = {sr};
-        write_parts<1>(k, v, red);
+        write_parts<1>(k, sync, v, red);
         if (!sync()) return false;
         double m1[1];
-        read_sums<1>(k, m1, red);
+        read_sums<1>(k, sync, m1, red);
         const double mr = proj ? m1[0] / cnt : 0.0;
         double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
         for (CellIter it = first_cell(k); it.c < k.c_end; next_cell(k, it)) {
@@ -255,12 +282,12 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
             s_rz += rv * double(V(zv));
         }
         double v2[4] = {s_rr, s_z, s_rz, s_r};
-        write_parts_max<4>(k, v2, s_max, red);
+        write_parts_max<4>(k, sync, v2, s_max, red);
         return sync();
     };
     auto read_residual_sums = [&](double &rr, double &rmax, double &rz) {
         double s4[4];
-        read_sums_max<4>(k, s4, rmax, red);
+        read_sums_max<4>(k, sync, s4, rmax, red);
         rr = s4[0];
         const double sz = s4[1], srz = s4[2], sr = s4[3];
         mz = proj ? sz / cnt : 0.0;
@@ -354,11 +381,11 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
         }
         {
             double v[3] = {s_dq, s_q, s_d};
-            write_parts<3>(k, v, red);
+            write_parts<3>(k, sync, v, red);
         }
         if (!sync()) return;
         double s3[3];
-        read_sums<3>(k, s3, red);
+        read_sums<3>(k, sync, s3, red);
         const double sdq = s3[0];
         const double md = proj ? s3[2] / cnt : 0.0;
         const double dq = proj ? sdq - md * s3[1] : sdq;
@@ -407,10 +434,10 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
                 }
             }
             double v[2] = {s_x, s_r};
-            write_parts<2>(k, v, red);
+            write_parts<2>(k, sync, v, red);
             if (!sync()) return;
             double s2[2];
-            read_sums<2>(k, s2, red);
+            read_sums<2>(k, sync, s2, red);
             mx = s2[0] / cnt;
             mr = s2[1] / cnt;
         }
@@ -488,7 +515,7 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
         }
         {
             double v[4] = {s_rr, s_z, s_rz, s_r};
-            write_parts_max<4>(k, v, s_max, red);
+            write_parts_max<4>(k, sync, v, s_max, red);
         }
         if (!sync()) return;
         double rz_new;
@@ -521,11 +548,11 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
     }
     {
         double v[1] = {s_true};
-        write_parts<1>(k, v, red);
+        write_parts<1>(k, sync, v, red);
     }
     if (!sync()) return;
     double st1[1];
-    read_sums<1>(k, st1, red);
+    read_sums<1>(k, sync, st1, red);
     const double true_rr = st1[0];
     if (k.lb == 0 && threadIdx.x == 0) {
         PcgResultDev *res = in.result;
@@ -589,9 +616,9 @@ __device__ void sor_instance(Ctx &k, double *red, const Sync &sync) {
             const double lap = (pe - 2.0 * p0 + pw) * in.idx2 + (pn - 2.0 * p0 + ps) * in.idy2;
             m = fmax(m, fabs(lap - __ldg(in.rhs + c)));
         }
-        write_max(k, (int)(sweep & 1), m, red);
+        write_max(k, sync, m, red);
         if (!sync()) return;
-        residual = read_max(k, (int)(sweep & 1), red);
+        residual = read_max(k, sync, red);
         if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
         if (residual < in.tol) break;
     }
@@ -617,11 +644,12 @@ __device__ __forceinline__ void make_ctx(Ctx &k, const Pcg2dInstance &in, int lb
     k.c_end = k.c_begin + chunk < k.n ? k.c_begin + chunk : k.n;
     k.step_j = kBlock / k.in.nx;
     k.step_i = kBlock - k.step_j * k.in.nx;
+    k.round = 0;
 }
 
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *__restrict__ insts, int ninst) {
-    __shared__ double red[kParts * (kBlock / 32)];
+    __shared__ double red[kRoundCols * (kBlock / 32)];
     int id = 0;
     for (int t = 0; t < ninst; ++t)
         if ((int)blockIdx.x >= insts[t].block0) id = t;
@@ -629,7 +657,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *_
     if (lb >= insts[id].nblocks) return;  // spare block of the launch
     Ctx k;
     make_ctx(k, insts[id], lb);
-    const GridSync sync{k.in.barrier, (unsigned)k.in.nblocks};
+    const GridSync sync{k.in.barrier, (unsigned)k.in.nblocks, k.in.partials};
     if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red, sync);
     else pcg_instance<V, MIXED>(k, red, sync);
 }
@@ -638,10 +666,10 @@ __global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *_
 // passes are separated by the hardware cluster barrier.
 template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock, 3) pcg2d_cluster_kernel(const Pcg2dInstance *__restrict__ inst) {
-    __shared__ double red[kParts * (kBlock / 32)];
+    __shared__ double red[kRoundCols * (kBlock / 32)];
     Ctx k;
     make_ctx(k, inst[0], (int)blockIdx.x);
-    const ClusterSync sync{};
+    const ClusterSync sync{k.in.partials};
     if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red, sync);
     else pcg_instance<V, MIXED>(k, red, sync);
 }
