@@ -4,7 +4,7 @@
 // persistent kernel of pcg3d.cu (see there), but each phase is its own
 // high-occupancy launch and the loop runs on the device:
 //
-//   graph:  init -> WHILE(continue) { dir_spmv -> update -> IF(replace) { fold -> replace } } -> final
+//   graph:  init -> WHILE(continue) { (dir_spmv -> update -> IF(replace) { fold -> replace }) x unroll } -> final
 //
 //   init      r = b - A x (FP64), sums r.r, r.z, max|r|; sets `continue`
 //   dir_spmv  d = z + beta d_old formed on the fly (cells and halo), q = A d,
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(kBlock) seq_dir_spmv(SeqArgs a) {
     __shared__ double tile[(TY + 2) * (TX + 2)];
     __shared__ double red[kSlots * (kBlock / 32)];
     const CgSeqState *s = a.st;
-    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
+    if (s->done) return;  // the solve has finished (host-driven mode, or a later iteration of an unrolled body)
     const double beta = s->beta;
     const bool first = s->first != 0;
     const int parity = (int)(s->iterations & 1);  // d buffers alternate per iteration
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
     if (threadIdx.x < 27) idg[threadIdx.x] = V(g.inv_diag[threadIdx.x]);
     __syncthreads();
     const CgSeqState *s = a.st;
-    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
+    if (s->done) return;  // the solve has finished (host-driven mode, or a later iteration of an unrolled body)
     const bool first = s->first != 0;
     const V beta = V(s->beta);
     const int parity = (int)(s->iterations & 1);
@@ -719,7 +719,17 @@ template <typename V, bool MIXED>
 __global__ void __launch_bounds__(kBlock) seq_update(SeqArgs a) {
     __shared__ double red[kSlots * (kBlock / 32)];
     const CgSeqState *s = a.st;
-    if (!a.graph && s->done) return;  // host-driven mode: the solve has finished
+    if (s->done) {
+        // The solve has finished: host-driven mode, a later iteration of an
+        // unrolled body, or a breakdown found by this iteration's operand
+        // kernel (which sets `done` and leaves the conditions to this kernel).
+        // Either way no replacement and no further iteration.
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            set_cond(a, a.h_replace, 0u);
+            set_cond(a, a.h_loop, 0u);
+        }
+        return;
+    }
     const double alpha = s->alpha;
     const bool dead = s->error != 0;
     const int parity = (int)(s->iterations & 1);
@@ -1311,38 +1321,55 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
     e = cudaGraphAddNode(&n_while, g, nullptr, 0, &wp);
     if (e != cudaSuccess) return e;
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    cudaGraphConditionalHandle hr;
-    e = cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) return e;
-    a.h_replace = hr;
+    // The body holds `unroll` iterations (FLURSYS_PCG_UNROLL, default 4;
+    // measured on B200 at 128^3: 39.7 / 38.2 / 37.4 ms per step for 1 / 2 /
+    // 4), so the loop condition is evaluated once per `unroll` iterations;
+    // the kernels of an iteration that follows the end of the solve return at
+    // once (and clear the conditions). Each IF node has its own handle, set
+    // by the pointwise kernel before it.
+    int unroll = 4;
+    if (const char *env = std::getenv("FLURSYS_PCG_UNROLL")) unroll = std::max(1, std::min(8, std::atoi(env)));
+    cudaGraphNode_t n_init, n_final;
     void *args[] = {&a};
-    cudaGraphNode_t n_init, n_dir, n_upd, n_if, n_final;
     e = add_kernel(g, &n_init, nullptr, 0, (const void *)seq_init<V, MIXED>, a.nblocks_stencil, args);
     if (e == cudaSuccess) e = cudaGraphAddDependencies(g, &n_init, &n_while, 1);
+    if (e != cudaSuccess) return e;
     const void *dir_fn = a.sweep == kSweepVec ? (const void *)seq_dir_vec<V, MIXED, kRyVec>
                                               : (const void *)seq_dir_spmv<V, MIXED>;
-    if (e == cudaSuccess) e = add_kernel(body, &n_dir, nullptr, 0, dir_fn, a.nblocks_dir, args);
-    if (e == cudaSuccess)
-        e = add_kernel(body, &n_upd, &n_dir, 1, (const void *)seq_update<V, MIXED>, a.nblocks_point, args);
-    if (e != cudaSuccess) return e;
-    cudaGraphNodeParams ip{};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = hr;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    e = cudaGraphAddNode(&n_if, body, &n_upd, 1, &ip);
-    if (e != cudaSuccess) return e;
-    cudaGraph_t rb = ip.conditional.phGraph_out[0];
-    if (MIXED) {
-        cudaGraphNode_t n_fold, n_rep;
-        e = add_kernel(rb, &n_fold, nullptr, 0, (const void *)seq_fold, a.nblocks_point, args);
+    cudaGraphNode_t prev{};
+    for (int u = 0; u < unroll; ++u) {
+        cudaGraphConditionalHandle hr;
+        e = cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return e;
+        SeqArgs au = a;
+        au.h_replace = hr;
+        if (u == 0) a.h_replace = hr;  // the argument block of the nodes outside the body
+        void *uargs[] = {&au};
+        cudaGraphNode_t n_dir, n_upd, n_if;
+        e = add_kernel(body, &n_dir, u ? &prev : nullptr, u ? 1 : 0, dir_fn, a.nblocks_dir, uargs);
         if (e == cudaSuccess)
-            e = add_kernel(rb, &n_rep, &n_fold, 1, (const void *)seq_replace<V, MIXED>, a.nblocks_stencil, args);
-    } else {
-        cudaGraphNode_t n_empty;
-        e = cudaGraphAddEmptyNode(&n_empty, rb, nullptr, 0);
+            e = add_kernel(body, &n_upd, &n_dir, 1, (const void *)seq_update<V, MIXED>, a.nblocks_point, uargs);
+        if (e != cudaSuccess) return e;
+        cudaGraphNodeParams ip{};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = hr;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        e = cudaGraphAddNode(&n_if, body, &n_upd, 1, &ip);
+        if (e != cudaSuccess) return e;
+        cudaGraph_t rb = ip.conditional.phGraph_out[0];
+        if (MIXED) {
+            cudaGraphNode_t n_fold, n_rep;
+            e = add_kernel(rb, &n_fold, nullptr, 0, (const void *)seq_fold, a.nblocks_point, uargs);
+            if (e == cudaSuccess)
+                e = add_kernel(rb, &n_rep, &n_fold, 1, (const void *)seq_replace<V, MIXED>, a.nblocks_stencil, uargs);
+        } else {
+            cudaGraphNode_t n_empty;
+            e = cudaGraphAddEmptyNode(&n_empty, rb, nullptr, 0);
+        }
+        if (e != cudaSuccess) return e;
+        prev = n_if;
     }
-    if (e != cudaSuccess) return e;
     cudaGraphNode_t after = n_while;
     if (MIXED) {
         cudaGraphNode_t n_pend;
