@@ -780,8 +780,36 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
 __global__ void __launch_bounds__(256) net_out_boundary(const float *__restrict__ r, const float *__restrict__ fz,
                                                         const double *scale_ptr, double h2, float *out, int nx, int ny,
                                                         int nz) {
-    __shared__ float k125[27 * 125];
-    for (int i = threadIdx.x; i < 27 * 125; i += blockDim.x) k125[i] = fz[kFusedK125 + i];
+    // Per boundary class, the taps (in increasing order) whose correction
+    // weight is nonzero and that can land inside the grid (a low class on an
+    // axis has no reachable tap below it, a high class none above); each warp
+    // compacts some classes with ballots.
+    __shared__ short tap[27][125];
+    __shared__ float wt[27][125];
+    __shared__ int cnt[27];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int cls = warp; cls < 27; cls += blockDim.x >> 5) {
+        const int clx = cls % 3, cly = (cls / 3) % 3, clz = cls / 9;
+        int n = 0;
+        for (int o0 = 0; o0 < 125; o0 += 32) {
+            const int o = o0 + lane;
+            float d = 0.f;
+            if (o < 125) {
+                const int dx = o % 5 - 2, dy = (o / 5) % 5 - 2, dz = o / 25 - 2;
+                const bool reach = !((clx == 0 && dx < 0) || (clx == 2 && dx > 0) || (cly == 0 && dy < 0) ||
+                                     (cly == 2 && dy > 0) || (clz == 0 && dz < 0) || (clz == 2 && dz > 0));
+                if (reach) d = __ldg(fz + kFusedK125 + cls * 125 + o) - __ldg(fz + kFusedK125 + kFusedInterior * 125 + o);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, d != 0.f);
+            if (d != 0.f) {
+                const int at = n + __popc(m & ((1u << lane) - 1u));
+                tap[cls][at] = (short)o;
+                wt[cls][at] = d;
+            }
+            n += __popc(m);
+        }
+        if (lane == 0) cnt[cls] = n;
+    }
     __syncthreads();
     if (!(scale_ptr[0] > 0.0)) return;
     const long long nzf = 2LL * nx * ny, nyf = 2LL * nx * (nz - 2), nxf = 2LL * (ny - 2) * (nz - 2);
@@ -803,14 +831,14 @@ __global__ void __launch_bounds__(256) net_out_boundary(const float *__restrict_
         }
         const int cls = (x == 0 ? 0 : x + 1 == nx ? 2 : 1) + 3 * (y == 0 ? 0 : y + 1 == ny ? 2 : 1) +
                         9 * (z == 0 ? 0 : z + 1 == nz ? 2 : 1);
-        const float *kc = k125 + cls * 125, *ki = k125 + kFusedInterior * 125;
         float corr = 0.f;
-        for (int o = 0; o < 125; ++o) {
+        const int nt = cnt[cls];
+        for (int k = 0; k < nt; ++k) {
+            const int o = tap[cls][k];
             const int dx = o % 5 - 2, dy = (o / 5) % 5 - 2, dz = o / 25 - 2;
             const int xx = x + dx, yy = y + dy, zz = z + dz;
             if (xx < 0 || yy < 0 || zz < 0 || xx >= nx || yy >= ny || zz >= nz) continue;
-            const float d = kc[o] - ki[o];
-            if (d != 0.f) corr = fmaf(d, __ldg(r + ((long long)zz * ny + yy) * nx + xx), corr);
+            corr = fmaf(wt[cls][k], __ldg(r + ((long long)zz * ny + yy) * nx + xx), corr);
         }
         const long long v = ((long long)z * ny + y) * nx + x;
         out[v] = float(double(out[v]) + h2 * double(corr));
@@ -1043,7 +1071,7 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     }
     if (e == cudaSuccess) {
         const long long faces = 2LL * nx * ny + 2LL * nx * (nz - 2) + 2LL * (ny - 2) * (nz - 2);
-        net_out_boundary<<<grid_1d(faces), 256, 0, st>>>(r, w.fused, ws.scalars, h2, z, nx, ny, nz);
+        net_out_boundary<<<std::min(grid_1d(faces), 148 * 4), 256, 0, st>>>(r, w.fused, ws.scalars, h2, z, nx, ny, nz);
         e = cudaGetLastError();
     }
     return e;
