@@ -196,6 +196,40 @@ __device__ __forceinline__ void store_row(const float (&acc)[COUT / 8][4], uint1
     }
 }
 
+// Raw global data of one staged element (PLAIN: the voxel's 8 channels;
+// UPADD: the coarse and skip channels), loaded before it is needed.
+struct RawStage {
+    uint4 a, b;
+};
+template <int C, int MODE>
+__device__ __forceinline__ RawStage raw_load(const Src &s, int x, int y, int z, int nx, int ny, int nz, int k8) {
+    RawStage r;
+    r.a = r.b = make_uint4(0, 0, 0, 0);
+    if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return r;
+    const long long fv = ((long long)z * ny + y) * nx + x;
+    if (MODE == kPlain) {
+        r.a = *reinterpret_cast<const uint4 *>(s.in + fv * C + k8 * 8);
+    } else {
+        const int cx = nx >> 1, cy = ny >> 1;
+        const long long cv = ((long long)(z >> 1) * cy + (y >> 1)) * cx + (x >> 1);
+        r.a = *reinterpret_cast<const uint4 *>(s.coarse + cv * C + k8 * 8);
+        r.b = *reinterpret_cast<const uint4 *>(s.in + fv * C + k8 * 8);
+    }
+    return r;
+}
+// The staged value of a raw element: the same FP32 sum and BF16 rounding as load8.
+template <int MODE>
+__device__ __forceinline__ uint4 raw_finish(const RawStage &r) {
+    if (MODE == kPlain) return r.a;
+    const uint16_t *ha = reinterpret_cast<const uint16_t *>(&r.a);
+    const uint16_t *hb = reinterpret_cast<const uint16_t *>(&r.b);
+    uint4 q;
+    uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) h[c] = f2bf(bf2f(ha[c]) + bf2f(hb[c]));
+    return q;
+}
+
 // Shared memory of conv_tc_z: all 27 taps' weights and a ring of 3 planes.
 template <int CIN, int COUT>
 constexpr int conv_z_smem_bytes() {
@@ -228,9 +262,38 @@ __global__ void __launch_bounds__(kConvThreads) conv_tc_z(Src src, const uint16_
     // ring slot of plane z: (z - z0 + 1) mod 3
     stage_tile<CIN, MODE>(sIn, src, x0, y0, z0 - 1, nx, ny, nz);
     stage_tile<CIN, MODE>(sIn + kPlane, src, x0, y0, z0, nx, ny, nz);
+    // PLAIN / UPADD: the global loads of plane z + 2 are issued before the
+    // MMAs of plane z and staged after the next barrier (POOL stages directly)
+    constexpr bool kPrefetch = MODE != kPool;
+    constexpr int kElems = kHY * kHX * K8;
+    constexpr int kPer = (kElems + kConvThreads - 1) / kConvThreads;
+    RawStage pre[kPrefetch ? kPer : 1];
+    auto prefetch = [&](int zz) {
+        #pragma unroll
+        for (int i = 0; i < (kPrefetch ? kPer : 1); ++i) {
+            const int idx = threadIdx.x + i * kConvThreads;
+            if (idx < kElems) {
+                const int k8 = idx % K8, cell = idx / K8;
+                pre[i] = raw_load<CIN, MODE>(src, x0 - 1 + cell % kHX, y0 - 1 + cell / kHX, zz, nx, ny, nz, k8);
+            }
+        }
+    };
+    auto stage_pre = [&](uint16_t *dst) {
+        #pragma unroll
+        for (int i = 0; i < (kPrefetch ? kPer : 1); ++i) {
+            const int idx = threadIdx.x + i * kConvThreads;
+            if (idx < kElems) {
+                const int k8 = idx % K8, cell = idx / K8;
+                *reinterpret_cast<uint4 *>(dst + cell * (CIN + kPad) + k8 * 8) = raw_finish<MODE>(pre[i]);
+            }
+        }
+    };
+    if (kPrefetch) prefetch(z0 + 1);
     for (int z = z0; z < z1; ++z) {
-        stage_tile<CIN, MODE>(sIn + ((z - z0 + 2) % 3) * kPlane, src, x0, y0, z + 1, nx, ny, nz);
+        if (kPrefetch) stage_pre(sIn + ((z - z0 + 2) % 3) * kPlane);
+        else stage_tile<CIN, MODE>(sIn + ((z - z0 + 2) % 3) * kPlane, src, x0, y0, z + 1, nx, ny, nz);
         __syncthreads();
+        if (kPrefetch && z + 1 < z1) prefetch(z + 2);
         float acc[COUT / 8][4], acc2[COUT / 8][4];
         #pragma unroll
         for (int n = 0; n < COUT / 8; ++n)
