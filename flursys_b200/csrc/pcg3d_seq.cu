@@ -1321,13 +1321,14 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
     e = cudaGraphAddNode(&n_while, g, nullptr, 0, &wp);
     if (e != cudaSuccess) return e;
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    // The body holds `unroll` iterations (FLURSYS_PCG_UNROLL, default 4;
+    // The body holds `unroll` iterations (FLURSYS_PCG_UNROLL, default 8;
     // measured on B200 at 128^3: 39.7 / 38.2 / 37.4 ms per step for 1 / 2 /
-    // 4), so the loop condition is evaluated once per `unroll` iterations;
+    // 4 on one box, 37.07 / 36.75 ms for 4 / 8 on another), so the loop
+    // condition is evaluated once per `unroll` iterations;
     // the kernels of an iteration that follows the end of the solve return at
     // once (and clear the conditions). Each IF node has its own handle, set
     // by the pointwise kernel before it.
-    int unroll = 4;
+    int unroll = 8;
     if (const char *env = std::getenv("FLURSYS_PCG_UNROLL")) unroll = std::max(1, std::min(8, std::atoi(env)));
     cudaGraphNode_t n_init, n_final;
     void *args[] = {&a};
