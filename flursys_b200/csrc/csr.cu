@@ -56,16 +56,31 @@ struct KrylovArgs {
     int method;  // 0 cg, 1 pcg, 2 bicgstab
 };
 
-__device__ __forceinline__ void write_parts(double *part, const double *v, int nv, double *red) {
-    for (int k = 0; k < nv; ++k) {
-        const double t = block_sum<kBlock>(v[k], red);
-        if (threadIdx.x == 0) part[blockIdx.x * kParts + k] = t;
-    }
+// Partial sums: every write -> grid barrier -> read group uses one of two
+// column sets (kParts / 2 columns each) by the parity of `round`, so that a
+// block never overwrites a set that a slower block may still be reading (the
+// next write to the same set is one barrier further on). Each group's values
+// are block-reduced through one set of block barriers (block_sum_n: the same
+// shuffle tree per value as one reduction each).
+template <int NV>
+__device__ __forceinline__ void write_parts(double *part, int round, double (&v)[NV], double *red) {
+    static_assert(NV <= kParts / 2, "one column set holds kParts / 2 values");
+    block_sum_n<kBlock, NV>(v, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[blockIdx.x * kParts + (round & 1) * (kParts / 2) + k] = v[k];
 }
-__device__ __forceinline__ double read_sum(const double *part, int k, double *red) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) s += part[b * kParts + k];
-    return block_sum<kBlock>(s, red);
+// Fixed-order sums over all blocks of the group's NV columns; ends the round.
+template <int NV>
+__device__ __forceinline__ void read_sums(const double *part, int &round, double (&out)[NV], double *red) {
+    const int base = (round & 1) * (kParts / 2);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) out[k] += __ldcg(part + b * kParts + base + k);
+    block_sum_n<kBlock, NV>(out, red);
+    ++round;
 }
 
 // Flags a non-finite SpMV row (first row wins through atomicMin).
@@ -74,7 +89,8 @@ __device__ __forceinline__ void flag_row(CsrResultDev *res, int row) {
 }
 
 __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
-    __shared__ double red[kBlock / 32];
+    __shared__ double red[(kParts / 2) * (kBlock / 32)];
+    int round = 0;  // partial-sum groups completed
     const int n = k.a.n;
     const int tid0 = blockIdx.x * kBlock + threadIdx.x, stride = gridDim.x * kBlock;
     const int *ro = k.a.ro, *ci = k.a.ci;
@@ -101,12 +117,14 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
             srr += rv * rv;
         }
         double v[1] = {srr};
-        write_parts(k.partials, v, 1, red);
+        write_parts<1>(k.partials, round, v, red);
     }
     if (!grid_sync(k.bar)) return;
+    double g0[1];
+    read_sums<1>(k.partials, round, g0, red);
     if (bail()) { error = FLURSYS_ERR_NON_FINITE; goto done; }
     {
-        const double rr0 = read_sum(k.partials, 0, red);
+        const double rr0 = g0[0];
         initial = sqrt(rr0);
         fin = initial;
         if (!isfinite(initial)) { error = FLURSYS_ERR_NON_FINITE; goto done; }
@@ -125,11 +143,13 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
             }
             {
                 double v[1] = {srz};
-                write_parts(k.partials, v, 1, red);
+                write_parts<1>(k.partials, round, v, red);
             }
             if (!grid_sync(k.bar)) return;
+            double g1[1];
+            read_sums<1>(k.partials, round, g1, red);
             if (bail()) { error = FLURSYS_ERR_NON_FINITE; goto done; }
-            double rho = read_sum(k.partials, 0, red);
+            double rho = g1[0];
             if (!isfinite(rho)) { error = FLURSYS_ERR_NON_FINITE; goto done; }
             double beta = 0.0;
             bool first = true;
@@ -149,11 +169,13 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[1] = {sdq};
-                    write_parts(k.partials, v, 1, red);
+                    write_parts<1>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
+                double gd[1];
+                read_sums<1>(k.partials, round, gd, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
-                const double den = read_sum(k.partials, 0, red);
+                const double den = gd[0];
                 if (!isfinite(den)) { error = FLURSYS_ERR_NON_FINITE; break; }  // dot() rejects it first
                 if (fabs(den) <= 1.0e-30) { error = FLURSYS_ERR_BREAKDOWN; break; }
                 const double alpha = rho / den;
@@ -171,15 +193,17 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[2] = {srr, srz2};
-                    write_parts(k.partials, v, 2, red);
+                    write_parts<2>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
-                const double rn = sqrt(read_sum(k.partials, 0, red));
+                double gr[2];
+                read_sums<2>(k.partials, round, gr, red);
+                const double rn = sqrt(gr[0]);
                 fin = rn;
                 if (!isfinite(rn)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (rn <= threshold) { status = FLURSYS_LINEAR_CONVERGED; break; }
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
-                const double rho_new = read_sum(k.partials, 1, red);
+                const double rho_new = gr[1];
                 if (!isfinite(rho_new)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (fabs(rho) <= 1.0e-30) { error = FLURSYS_ERR_BREAKDOWN; break; }
                 beta = rho_new / rho;
@@ -191,7 +215,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
         } else {
             // ---- BiCGSTAB ----
             double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
-            double rho = read_sum(k.partials, 0, red);  // r_hat = r0, so r_hat.r = ||r0||^2
+            double rho = g0[0];  // r_hat = r0, so r_hat.r = ||r0||^2
             for (int row = tid0; row < n; row += stride) { k.p[row] = 0.0; k.v[row] = 0.0; }
             if (!grid_sync(k.bar)) return;
             for (long long it = 1; it <= k.max_iters; ++it) {
@@ -211,11 +235,13 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[1] = {shv};
-                    write_parts(k.partials, v, 1, red);
+                    write_parts<1>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
+                double gv[1];
+                read_sums<1>(k.partials, round, gv, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
-                const double den = read_sum(k.partials, 0, red);
+                const double den = gv[0];
                 if (!isfinite(den)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (fabs(den) <= 1.0e-30) { error = FLURSYS_ERR_BREAKDOWN; break; }
                 alpha = rho / den;
@@ -228,10 +254,12 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[1] = {sss};
-                    write_parts(k.partials, v, 1, red);
+                    write_parts<1>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
-                const double sn = sqrt(read_sum(k.partials, 0, red));
+                double gs[1];
+                read_sums<1>(k.partials, round, gs, red);
+                const double sn = sqrt(gs[0]);
                 if (!isfinite(sn)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (sn <= threshold) {
                     for (int row = tid0; row < n; row += stride) k.x[row] += alpha * k.p[row];
@@ -249,12 +277,14 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[2] = {stt, sts};
-                    write_parts(k.partials, v, 2, red);
+                    write_parts<2>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
+                double gt[2];
+                read_sums<2>(k.partials, round, gt, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
-                const double tt = read_sum(k.partials, 0, red);
-                const double ts_ = read_sum(k.partials, 1, red);
+                const double tt = gt[0];
+                const double ts_ = gt[1];
                 if (!isfinite(tt) || !isfinite(ts_)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (fabs(tt) <= 1.0e-30) { error = FLURSYS_ERR_BREAKDOWN; break; }
                 omega = ts_ / tt;
@@ -269,15 +299,17 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 }
                 {
                     double v[2] = {srr, shr};
-                    write_parts(k.partials, v, 2, red);
+                    write_parts<2>(k.partials, round, v, red);
                 }
                 if (!grid_sync(k.bar)) return;
-                const double rn = sqrt(read_sum(k.partials, 0, red));
+                double gq[2];
+                read_sums<2>(k.partials, round, gq, red);
+                const double rn = sqrt(gq[0]);
                 fin = rn;
                 if (!isfinite(rn)) { error = FLURSYS_ERR_NON_FINITE; break; }
                 if (rn <= threshold) { status = FLURSYS_LINEAR_CONVERGED; break; }
                 rho_prev = rho;
-                rho = read_sum(k.partials, 1, red);
+                rho = gq[1];
             }
             if (status != FLURSYS_LINEAR_CONVERGED) iterations = k.max_iters;
         }
