@@ -89,7 +89,7 @@ __device__ __forceinline__ unsigned long long gtimer() {
 }
 
 struct SmemBase {
-    double red[kBlock / 32];
+    double red[3 * (kBlock / 32)];  // up to two sums and a maximum per reduction
     double inv_diag[27];
     float inv_diag_f[27];
 };
@@ -259,26 +259,29 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     const long long tid0 = (long long)blockIdx.x * kBlock + threadIdx.x;
     const long long stride = (long long)nblk * kBlock;
 
+    // r.r, r.z and max|r| through one set of block barriers (the same
+    // shuffle tree per value as separate reductions)
     auto write_partials3 = [&](double srr, double srz, double smax) {
-        const double t0 = block_sum<kBlock>(srr, sb.red);
-        const double t1 = block_sum<kBlock>(srz, sb.red);
-        const double t2 = block_max<kBlock>(smax, sb.red);
+        double t[2] = {srr, srz};
+        block_reduce_n<kBlock, 2, true>(t, smax, sb.red);
         if (threadIdx.x == 0) {
-            part[blockIdx.x * kNumPartials + 0] = t0;
-            part[blockIdx.x * kNumPartials + 1] = t1;
-            part[blockIdx.x * kNumPartials + 2] = t2;
+            part[blockIdx.x * kNumPartials + 0] = t[0];
+            part[blockIdx.x * kNumPartials + 1] = t[1];
+            part[blockIdx.x * kNumPartials + 2] = smax;
         }
     };
     auto reduce3 = [&](double &rr, double &rz, double &rmax) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        double t[2] = {0.0, 0.0};
+        double s2 = 0.0;
         for (int b = threadIdx.x; b < nblk; b += kBlock) {
-            s0 += part[b * kNumPartials + 0];
-            s1 += part[b * kNumPartials + 1];
+            t[0] += part[b * kNumPartials + 0];
+            t[1] += part[b * kNumPartials + 1];
             s2 = fmax(s2, part[b * kNumPartials + 2]);
         }
-        rr = block_sum<kBlock>(s0, sb.red);
-        rz = block_sum<kBlock>(s1, sb.red);
-        rmax = block_max<kBlock>(s2, sb.red);
+        block_reduce_n<kBlock, 2, true>(t, s2, sb.red);
+        rr = t[0];
+        rz = t[1];
+        rmax = s2;
     };
     auto reduce_slot3 = [&]() -> double {
         double s = 0.0;
