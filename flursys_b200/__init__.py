@@ -7,15 +7,17 @@ reference's solver and linear-algebra interfaces; it has no CPU fallback.
 from . import _abi
 from .cases import (BackwardStepCase, Case, CavityCase, ChannelCase, CylinderCase, SolverBoundaryOverride,
                     SolverBoundaryOverrides)
-from .solver import (BackendOptions, BatchedIncompressibleSolver, FieldUpdate, IncompressibleSolver, LidDrivenCavity3DConfig,
-                     LidDrivenCavity3DSolver, RunSummary, RunSummary3D, SimulationConfig, SolverError, SolverStep,
+from .solver import (BackendOptions, BatchedIncompressibleSolver, BoussinesqBuoyancy, FieldUpdate, IncompressibleSolver,
+                     LidDrivenCavity3DConfig, LidDrivenCavity3DSolver, PhysicsSettings, RunSummary, RunSummary3D,
+                     SimulationConfig, SolverError, SolverStep, ThermalBoundaryCondition, ThermalSettings,
                      TimeStepSettings)
 
 __all__ = [
     "BackendOptions", "BatchedIncompressibleSolver", "BackwardStepCase", "Case", "CavityCase", "ChannelCase", "CylinderCase", "FieldUpdate",
     "IncompressibleSolver", "LidDrivenCavity3DConfig", "LidDrivenCavity3DSolver", "RunSummary", "RunSummary3D",
     "SimulationConfig", "SolverBoundaryOverride", "SolverBoundaryOverrides", "SolverError", "SolverStep",
-    "TimeStepSettings", "load_library",
+    "TimeStepSettings", "load_library", "BoussinesqBuoyancy", "PhysicsSettings", "ThermalBoundaryCondition",
+    "ThermalSettings",
 ]
 
 

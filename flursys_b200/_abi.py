@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # FlursysStatus
 OK = 0
@@ -50,6 +50,7 @@ STOP_ABS_INF, STOP_REL_L2, STOP_REFERENCE_RESIDUAL = 0, 1, 2
 FIELD_U, FIELD_V, FIELD_W, FIELD_PRESSURE, FIELD_RHS = 0, 1, 2, 3, 4
 FIELD_U_STAR, FIELD_V_STAR, FIELD_W_STAR = 5, 6, 7
 FIELD_SPEED, FIELD_VORTICITY, FIELD_U_CELL, FIELD_V_CELL = 8, 9, 10, 11
+FIELD_TEMPERATURE = 12
 
 
 class LinearSolverOptions(C.Structure):
@@ -102,6 +103,30 @@ class BoundaryOverride(C.Structure):
     ]
 
 
+ENERGY_OFF, ENERGY_CONSTANT_PROPERTIES = 0, 1
+THERMAL_ADIABATIC, THERMAL_FIXED_TEMPERATURE = 0, 1
+BUOYANCY_OFF, BUOYANCY_BOUSSINESQ = 0, 1
+
+
+class ThermalBoundary(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("temperature", C.c_double)]
+
+
+class PhysicsSettings(C.Structure):
+    _fields_ = [
+        ("energy_model", C.c_int32),
+        ("buoyancy", C.c_int32),
+        ("initial_temperature", C.c_double),
+        ("thermal_diffusivity", C.c_double),
+        ("source_temperature_rate", C.c_double),
+        ("thermal", ThermalBoundary * 4),
+        ("reference_temperature", C.c_double),
+        ("thermal_expansion", C.c_double),
+        ("gravity_x", C.c_double),
+        ("gravity_y", C.c_double),
+    ]
+
+
 class CudaConfig(C.Structure):
     _fields_ = [
         ("abi_version", C.c_uint32),
@@ -139,6 +164,7 @@ class CudaConfig(C.Structure):
         ("device", C.c_int32),
         ("reserved1", C.c_int32),
         ("fcg_weights_path", C.c_char_p),
+        ("physics", PhysicsSettings),
     ]
 
 
@@ -250,6 +276,7 @@ SIGNATURES = {
     "flursys_cuda_solver_profile": (C.c_int32, [_P, _D, C.c_size_t]),
     "flursys_cuda_destroy": (C.c_int32, [_P]),
     "flursys_cuda_global_error": (C.c_int32, [C.c_char_p, C.c_size_t]),
+    "flursys_cuda_debug_inject_barrier_fault": (C.c_int32, [C.c_int32]),
     "flursys_cuda_csr_cg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,
                                         C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport)]),
     "flursys_cuda_csr_pcg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,

@@ -533,6 +533,7 @@ extern "C" int32_t flursys_cuda_batch_create(const FlursysCudaConfig *configs, i
         if (c.dimension != 2) why = "the batched solver is 2D only";
         else if (c.coupling != FLURSYS_COUPLING_PROJECTION) why = "the batched solver supports projection coupling only";
         else if (c.pressure_solver != FLURSYS_PRESSURE_PCG && c.pressure_solver != FLURSYS_PRESSURE_SOR) why = "the batched solver supports the PCG and SOR pressure solvers";
+        else if (c.physics.energy_model != FLURSYS_ENERGY_OFF) why = "the batched solver runs constant-property flow only; thermal and buoyancy models are not available";
         else if (c.precision != configs[0].precision) why = "every instance must use the same precision";
         else if (c.device != configs[0].device) why = "every instance must use the same device";
         if (why) {

@@ -7,9 +7,12 @@
 // a FlursysStatus and keeps a message for flursys_cuda_last_error().
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -36,9 +39,9 @@ void copy_msg(const std::string &s, char *buf, size_t size) {
     buf[n] = '\0';
 }
 
-// SimulationConfig::validate (incompressible.rs:93-191, thermal checks do not
-// apply: the backend runs flow-only physics) and LidDrivenCavity3DConfig::
-// validate (incompressible_3d.rs:50-84).
+// SimulationConfig::validate (incompressible.rs:93-191, with
+// PhysicsSettings::validate, src/physics.rs:79-131) and
+// LidDrivenCavity3DConfig::validate (incompressible_3d.rs:50-84).
 int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
     auto fin_pos = [](double x) { return std::isfinite(x) && x > 0.0; };
     if (c.abi_version != FLURSYS_CUDA_ABI_VERSION) { *msg = "config abi_version does not match the library"; return FLURSYS_ERR_INVALID_ARGUMENT; }
@@ -53,6 +56,8 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
     if (c.precision == FLURSYS_PRECISION_MIXED && c.residual_replacement_every < 1) { *msg = "residual_replacement_every must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
     if (c.dimension == 3) {
         if (c.case_params.kind != FLURSYS_CASE_CAVITY) { *msg = "the current 3D backend supports only a lid-driven cavity case"; return FLURSYS_ERR_UNSUPPORTED; }
+        // src/project.rs:276-284: the 3D backend runs constant-property flow only
+        if (c.physics.energy_model != FLURSYS_ENERGY_OFF || c.physics.buoyancy != FLURSYS_BUOYANCY_OFF) { *msg = "the current 3D backend supports constant-property flow only; thermal and buoyancy models are not available"; return FLURSYS_ERR_UNSUPPORTED; }
         if (c.nx < 4 || c.ny < 4 || c.nz < 4) { *msg = "nx, ny, and nz must all be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0 && c.case_params.depth > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!fin_pos(c.case_params.density)) { *msg = "density must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
@@ -96,6 +101,26 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
         if (!std::isfinite(c.max_growth_factor) || c.max_growth_factor < 1.0) { *msg = "adaptive max_growth_factor must be finite and at least 1"; return FLURSYS_ERR_INVALID_CONFIG; }
     }
     if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    if (c.physics.energy_model != FLURSYS_ENERGY_OFF && c.physics.energy_model != FLURSYS_ENERGY_CONSTANT_PROPERTIES) { *msg = "unknown energy model"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (c.physics.buoyancy != FLURSYS_BUOYANCY_OFF && c.physics.buoyancy != FLURSYS_BUOYANCY_BOUSSINESQ) { *msg = "unknown buoyancy model"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    for (int s = 0; s < 4; ++s)
+        if (c.physics.thermal[s].kind != FLURSYS_THERMAL_ADIABATIC && c.physics.thermal[s].kind != FLURSYS_THERMAL_FIXED_TEMPERATURE) { *msg = "unknown thermal boundary kind"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    // PhysicsSettings::validate at min_dt when adaptive, else dt (:180-189)
+    const FlursysPhysicsSettings &ph = c.physics;
+    const bool thermal = ph.energy_model == FLURSYS_ENERGY_CONSTANT_PROPERTIES;
+    if (thermal) {
+        if (!std::isfinite(ph.initial_temperature) || !std::isfinite(ph.thermal_diffusivity) || ph.thermal_diffusivity <= 0.0 || !std::isfinite(ph.source_temperature_rate)) { *msg = "thermal initial temperature, diffusivity, and source must be finite; diffusivity must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        for (int s = 0; s < 4; ++s)
+            if (ph.thermal[s].kind == FLURSYS_THERMAL_FIXED_TEMPERATURE && !std::isfinite(ph.thermal[s].temperature)) { *msg = "fixed thermal boundary temperatures must be finite"; return FLURSYS_ERR_INVALID_CONFIG; }
+        const double vdt = c.adaptive ? c.min_dt : c.dt;
+        const double dx = c.case_params.length / c.nx, dy = c.case_params.height / c.ny;
+        const double fourier = ph.thermal_diffusivity * vdt * (std::pow(1.0 / dx, 2) + std::pow(1.0 / dy, 2));
+        if (fourier > 0.5) { *msg = "explicit thermal diffusion is unstable: alpha*dt*(1/dx^2 + 1/dy^2)=" + rust_sci(fourier, 3) + " exceeds 0.5"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
+    if (ph.buoyancy == FLURSYS_BUOYANCY_BOUSSINESQ) {
+        if (!thermal) { *msg = "Boussinesq buoyancy requires the constant-property energy equation"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(ph.reference_temperature) || !std::isfinite(ph.thermal_expansion) || ph.thermal_expansion < 0.0 || !std::isfinite(ph.gravity_x) || !std::isfinite(ph.gravity_y)) { *msg = "Boussinesq reference temperature, expansion coefficient, and gravity must be finite; expansion must be non-negative"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
     return FLURSYS_OK;
 }
 
@@ -106,6 +131,36 @@ namespace flursys {
 int32_t validate_config_checked(const FlursysCudaConfig &c, std::string *msg) { return validate_config(c, msg); }
 
 void set_global_error(const std::string &msg) { g_error = msg; }
+
+std::string rust_sci(double v, int prec) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.*e", prec, v);
+    const std::string s(buf);
+    const size_t e = s.find('e');
+    if (e == std::string::npos) return s;
+    return s.substr(0, e) + "e" + std::to_string(std::atoi(s.c_str() + e + 1));
+}
+
+std::string nonfinite_message(const char *name, unsigned long long index, const double *field, long long step,
+                              bool two_d) {
+    double v = NAN;
+    if (field) cudaMemcpy(&v, field + index, sizeof v, cudaMemcpyDeviceToHost);
+    const char *shown = std::isnan(v) ? "NaN" : (v > 0 ? "inf" : "-inf");
+    char buf[256];
+    if (two_d)
+        std::snprintf(buf, sizeof buf, "Non-finite %s value at flat index %llu: %s (step %lld)", name, index, shown, step);
+    else
+        std::snprintf(buf, sizeof buf, "Non-finite 3D %s value at flat index %llu: %s", name, index, shown);
+    return buf;
+}
+
+namespace {
+std::atomic<int> g_injected_barrier_fault{0};
+}
+
+int take_injected_barrier_fault() { return g_injected_barrier_fault.exchange(0); }
 
 int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what) {
     char buf[256];
@@ -194,6 +249,15 @@ int32_t flursys_cuda_global_error(char *buf, size_t size) {
     return FLURSYS_OK;
 }
 
+int32_t flursys_cuda_debug_inject_barrier_fault(int32_t extra_arrivals) {
+    if (extra_arrivals < 0) {
+        g_error = "extra_arrivals must be >= 0";
+        return FLURSYS_ERR_INVALID_ARGUMENT;
+    }
+    g_injected_barrier_fault.store(extra_arrivals);
+    return FLURSYS_OK;
+}
+
 // LidDrivenCavity3DConfig::default() (incompressible_3d.rs:27-47) for
 // dimension 3; the CLI cavity defaults (src/bin/flursys.rs:102-123,236-300)
 // with TimeStepSettings::default() (incompressible.rs:45-56) otherwise.
@@ -205,6 +269,9 @@ int32_t flursys_cuda_default_config(int32_t dimension, FlursysCudaConfig *c) {
     c->case_params.kind = FLURSYS_CASE_CAVITY;
     c->case_params.length = 1.0;
     c->case_params.height = 1.0;
+    // ThermalSettings::default (src/physics.rs:43-56); buoyancy off
+    c->physics.initial_temperature = 293.15;
+    c->physics.thermal_diffusivity = 2.2e-5;
     c->case_params.depth = 1.0;
     c->case_params.density = 1.0;
     c->case_params.reference_velocity = 1.0;

@@ -65,6 +65,15 @@ struct FlursysCudaHandle {
 namespace flursys {
 
 int32_t set_cuda_error(std::string *dst, cudaError_t e, const char *what);
+// Rust's `{:.Ne}` rendering of an f64 ("1.500e-5"), for messages that
+// callers compare with the reference's.
+std::string rust_sci(double v, int prec);
+// ensure_finite's message for the non-finite value at `index` of the device
+// array `field`: "Non-finite {name} value at flat index {i}: {v} (step {s})"
+// in 2D (incompressible.rs:1707-1742), "Non-finite 3D {name} value at flat
+// index {i}: {v}" in 3D (incompressible_3d.rs:534-554).
+std::string nonfinite_message(const char *name, unsigned long long index, const double *field, long long step,
+                              bool two_d);
 // SimulationConfig::validate / LidDrivenCavity3DConfig::validate of a config.
 int32_t validate_config_checked(const FlursysCudaConfig &c, std::string *msg);
 // Message returned by flursys_cuda_global_error() on this thread.

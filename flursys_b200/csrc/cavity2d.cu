@@ -15,7 +15,7 @@ namespace flursys {
 namespace {
 
 constexpr int kBlk = 256;
-constexpr int kPostParts = 8;
+constexpr int kPostParts = 10;
 
 __global__ void __launch_bounds__(kBlk) predict2d(Cavity2dState s, double dt, int with_p, double relax) {
     const int n = (s.nx + 1) * s.ny + s.nx * (s.ny + 1);
@@ -42,15 +42,18 @@ __global__ void simple_relax2d(Cavity2dState s, double relax) {
     for (int c = blockIdx.x * kBlk + threadIdx.x; c < n; c += gridDim.x * kBlk) s.p[c] = s.pold[c] + relax * s.p[c];
 }
 
+// Parts 6 and 7 (force sums) add up; every other part is a maximum.
+__device__ __forceinline__ bool is_max_part(int k) { return k != 6 && k != 7; }
+
 __global__ void __launch_bounds__(kBlk) post2d(Cavity2dState s) {
     __shared__ double red[kBlk / 32];
     const int nc = s.nx * s.ny, nu = (s.nx + 1) * s.ny, nv = s.nx * (s.ny + 1);
     const int nmax = max(nc, max(nu, nv));
     PostAcc a;
     for (int id = blockIdx.x * kBlk + threadIdx.x; id < nmax; id += gridDim.x * kBlk) post_elem(s, id, a);
-    const double vals[kPostParts] = {a.mdiv, a.mspeed, a.mu, a.mv, a.du, a.dv, a.fx, a.fy};
+    const double vals[kPostParts] = {a.mdiv, a.mspeed, a.mu, a.mv, a.du, a.dv, a.fx, a.fy, a.muc, a.mvc};
     for (int k = 0; k < kPostParts; ++k) {
-        const double t = k < 6 ? block_max<kBlk>(vals[k], red) : block_sum<kBlk>(vals[k], red);
+        const double t = is_max_part(k) ? block_max<kBlk>(vals[k], red) : block_sum<kBlk>(vals[k], red);
         if (threadIdx.x == 0) s.partials[blockIdx.x * kPostParts + k] = t;
     }
 }
@@ -63,9 +66,9 @@ __global__ void post2d_finalize(Cavity2dState s) {
         double a = 0.0;
         for (int b = threadIdx.x; b < s.post_blocks; b += kBlk) {
             const double v = s.partials[b * kPostParts + k];
-            a = k < 6 ? fmax(a, v) : a + v;
+            a = is_max_part(k) ? fmax(a, v) : a + v;
         }
-        out[k] = k < 6 ? block_max<kBlk>(a, red) : block_sum<kBlk>(a, red);
+        out[k] = is_max_part(k) ? block_max<kBlk>(a, red) : block_sum<kBlk>(a, red);
     }
     if (threadIdx.x == 0) {
         Diag2Dev *d = s.diag;
@@ -77,11 +80,18 @@ __global__ void post2d_finalize(Cavity2dState s) {
         d->dv = out[5];
         d->fx = out[6];
         d->fy = out[7];
+        d->max_abs_uc = out[8];
+        d->max_abs_vc = out[9];
     }
 }
 
 __global__ void diag2d_reset(Diag2Dev *d) {
-    for (int f = 0; f < 4; ++f) d->bad_index[f] = ~0ull;
+    for (int f = 0; f < 5; ++f) d->bad_index[f] = ~0ull;
+}
+
+__global__ void __launch_bounds__(kBlk) temperature2d(Cavity2dState s, double dt) {
+    const int n = s.nx * s.ny;
+    for (int c = blockIdx.x * kBlk + threadIdx.x; c < n; c += gridDim.x * kBlk) temperature_elem(s, c, dt);
 }
 
 int grid_for(long long n, int sms) {
@@ -92,6 +102,8 @@ int grid_for(long long n, int sms) {
 }
 
 }  // namespace
+
+int cavity2d_post_parts() { return kPostParts; }
 
 int cavity2d_post_blocks(int nx, int ny, int sms) {
     return grid_for((long long)(nx + 1) * (ny + 1), sms);
@@ -122,6 +134,11 @@ cudaError_t cavity2d_correct(const Cavity2dState &s, double dt_over_rho, cudaStr
 
 cudaError_t cavity2d_simple_relax(const Cavity2dState &s, double relax, cudaStream_t st) {
     simple_relax2d<<<grid_for((long long)s.nx * s.ny, s.sms), kBlk, 0, st>>>(s, relax);
+    return cudaGetLastError();
+}
+
+cudaError_t cavity2d_temperature(const Cavity2dState &s, double dt, cudaStream_t st) {
+    temperature2d<<<grid_for((long long)s.nx * s.ny, s.sms), kBlk, 0, st>>>(s, dt);
     return cudaGetLastError();
 }
 

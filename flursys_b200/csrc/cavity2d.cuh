@@ -16,7 +16,8 @@ struct Diag2Dev {
     double max_abs_u, max_abs_v;
     double du, dv;          // max_field_difference of u and v (:2287-2292)
     double fx, fy;          // cylinder force sums (:1634-1676)
-    unsigned long long bad_index[4];  // first non-finite index of p, u, v, speed
+    double max_abs_uc, max_abs_vc;    // u_cell / v_cell max_abs (thermal CFL, :1449-1451)
+    unsigned long long bad_index[5];  // first non-finite index of p, u, v, speed, temperature
 };
 
 // Device pointers and constants of one 2D grid. Layout (Field2D,
@@ -38,6 +39,15 @@ struct Cavity2dState {
     double *uc, *vc, *speed, *vort;
     int cylinder;                       // compute force sums
     double cylinder_mu;
+    // Energy equation and Boussinesq force (src/physics.rs); temp is null
+    // when the energy model is off.
+    double *temp;                       // cell temperature of the current state
+    double *temp_next;                  // advance_temperature output
+    int buoyancy;                       // add g * beta * (T_face - T_ref) in the predictor
+    double gbx, gby, tref;              // gravity_x * beta, gravity_y * beta, T_ref
+    double alpha, tsource;              // thermal diffusivity, source temperature rate
+    int tkind[4];                       // FlursysThermalBoundaryKind per side
+    double twall[4];                    // fixed wall temperatures per side
     double *partials;                   // post-pass partial reductions
     int post_blocks;
     Diag2Dev *diag;
@@ -53,6 +63,10 @@ cudaError_t cavity2d_simple_relax(const Cavity2dState &s, double relax, cudaStre
 // compute_cell_fields (:1381-1439) of (un, vn) plus every diagnostic of
 // advance_one_step (:716-731) against the old state (u, v).
 cudaError_t cavity2d_post(const Cavity2dState &s, cudaStream_t st);
+// advance_temperature (:1441-1493) from temp into temp_next on the corrected
+// velocities (un, vn); flags the first non-finite result in bad_index[4].
+cudaError_t cavity2d_temperature(const Cavity2dState &s, double dt, cudaStream_t st);
 int cavity2d_post_blocks(int nx, int ny, int sms);
+int cavity2d_post_parts();  // partial sums per post-pass block
 
 }  // namespace flursys

@@ -51,8 +51,9 @@ __device__ __forceinline__ double transported(int scheme, double fv, double left
     return 0.5 * (left + right);
 }
 
-// predict_momentum (:748-922) without buoyancy for face `id` of the
-// concatenated u (nu) and v (nv) face sets; every face is written.
+// predict_momentum (:748-922) for face `id` of the concatenated u (nu) and
+// v (nv) face sets; every face is written. The Boussinesq term
+// g * beta * (T_face - T_ref) (:831-846, :896-911) is 0.0 when buoyancy is off.
 __device__ __forceinline__ void predict_elem(const Cavity2dState &s, int id, double dt, int with_p, double relax) {
     const int nu = (s.nx + 1) * s.ny;
     const double *u = s.u, *v = s.v, *p = s.p;
@@ -70,7 +71,8 @@ __device__ __forceinline__ void predict_elem(const Cavity2dState &s, int id, dou
         const double conv = (ue * pe - uw * pw) / s.dx + (vn * pn - vs * ps) / s.dy;
         const double diff = (ue_nb - 2.0 * up + uw_nb) / (s.dx * s.dx) + (un_nb - 2.0 * up + us_nb) / (s.dy * s.dy);
         const double pg = with_p ? (p[i + s.nx * j] - p[i - 1 + s.nx * j]) / s.dx : 0.0;
-        s.us[id] = up + relax * dt * (-conv + s.nu * diff - pg / s.rho);
+        const double bx = s.buoyancy ? s.gbx * (0.5 * (s.temp[i - 1 + s.nx * j] + s.temp[i + s.nx * j]) - s.tref) : 0.0;
+        s.us[id] = up + relax * dt * (-conv + s.nu * diff - pg / s.rho + bx);
     } else {
         const int vid = id - nu;
         const int j = vid / s.nx, i = vid - j * s.nx;
@@ -86,7 +88,8 @@ __device__ __forceinline__ void predict_elem(const Cavity2dState &s, int id, dou
         const double conv = (ue * pe - uw * pw) / s.dx + (vn * pn - vs * ps) / s.dy;
         const double diff = (ve_nb - 2.0 * vp + vw_nb) / (s.dx * s.dx) + (vn_nb - 2.0 * vp + vs_nb) / (s.dy * s.dy);
         const double pg = with_p ? (p[i + s.nx * j] - p[i + s.nx * (j - 1)]) / s.dy : 0.0;
-        s.vs[vid] = vp + relax * dt * (-conv + s.nu * diff - pg / s.rho);
+        const double by = s.buoyancy ? s.gby * (0.5 * (s.temp[i + s.nx * (j - 1)] + s.temp[i + s.nx * j]) - s.tref) : 0.0;
+        s.vs[vid] = vp + relax * dt * (-conv + s.nu * diff - pg / s.rho + by);
     }
 }
 
@@ -158,6 +161,7 @@ __device__ __forceinline__ double ucell(const Cavity2dState &s, int i, int j) {
 // Running reductions of the post-step pass.
 struct PostAcc {
     double mdiv = 0.0, mspeed = 0.0, mu = 0.0, mv = 0.0, du = 0.0, dv = 0.0, fx = 0.0, fy = 0.0;
+    double muc = 0.0, mvc = 0.0;
 };
 
 // compute_cell_fields (:1381-1439), max_divergence (:1569-1582), the velocity
@@ -175,6 +179,8 @@ __device__ __forceinline__ void post_elem(const Cavity2dState &s, int id, PostAc
             const double sp = sqrt(uu * uu + vv * vv);
             s.uc[id] = uu; s.vc[id] = vv; s.speed[id] = sp;
             a.mspeed = fmax(a.mspeed, sp);
+            a.muc = fmax(a.muc, fabs(uu));
+            a.mvc = fmax(a.mvc, fabs(vv));
             if (!isfinite(sp)) atomicMin(&s.diag->bad_index[3], (unsigned long long)id);
             const bool e_ok = i + 1 < s.nx && !sol(s, i + 1, j), w_ok = i > 0 && !sol(s, i - 1, j);
             const bool n_ok = j + 1 < s.ny && !sol(s, i, j + 1), s_ok = j > 0 && !sol(s, i, j - 1);
@@ -211,6 +217,36 @@ __device__ __forceinline__ void post_elem(const Cavity2dState &s, int id, PostAc
         a.dv = fmax(a.dv, fabs(x - s.v[id]));
         if (!isfinite(x)) atomicMin(&s.diag->bad_index[2], (unsigned long long)id);
     }
+}
+
+// temperature_neighbor (:1495-1530): a solid neighbour or an adiabatic wall
+// mirrors the centre; a fixed-temperature wall gives 2 T_w - centre.
+__device__ __forceinline__ double temp_nb(const Cavity2dState &s, int i, int j, int di, int dj, double c) {
+    const int ni = i + di, nj = j + dj;
+    if (ni >= 0 && ni < s.nx && nj >= 0 && nj < s.ny) return sol(s, ni, nj) ? c : s.temp[ni + s.nx * nj];
+    const int side = ni < 0 ? 0 : (ni >= s.nx ? 1 : (nj < 0 ? 2 : 3));
+    return s.tkind[side] == FLURSYS_THERMAL_FIXED_TEMPERATURE ? 2.0 * s.twall[side] - c : c;
+}
+
+// advance_temperature (:1441-1493) for cell c: explicit conservative update
+// with first-order upwind face values on the corrected face velocities.
+__device__ __forceinline__ void temperature_elem(const Cavity2dState &s, int c, double dt) {
+    const int j = c / s.nx, i = c - j * s.nx;
+    const double ctr = s.temp[c];
+    double t = ctr;
+    if (!sol(s, i, j)) {
+        const double e = temp_nb(s, i, j, 1, 0, ctr), w = temp_nb(s, i, j, -1, 0, ctr);
+        const double n = temp_nb(s, i, j, 0, 1, ctr), so = temp_nb(s, i, j, 0, -1, ctr);
+        const double ue = s.un[i + 1 + (s.nx + 1) * j], uw = s.un[i + (s.nx + 1) * j];
+        const double vn = s.vn[i + s.nx * (j + 1)], vsf = s.vn[i + s.nx * j];
+        const double fe = ue * (ue >= 0.0 ? ctr : e), fw = uw * (uw >= 0.0 ? w : ctr);
+        const double fn = vn * (vn >= 0.0 ? ctr : n), fs = vsf * (vsf >= 0.0 ? so : ctr);
+        const double conv = (fe - fw) / s.dx + (fn - fs) / s.dy;
+        const double diff = (e - 2.0 * ctr + w) / (s.dx * s.dx) + (n - 2.0 * ctr + so) / (s.dy * s.dy);
+        t = ctr + dt * (-conv + s.alpha * diff + s.tsource);
+    }
+    s.temp_next[c] = t;
+    if (!isfinite(t)) atomicMin(&s.diag->bad_index[4], (unsigned long long)c);
 }
 
 }  // namespace flursys

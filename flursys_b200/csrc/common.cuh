@@ -31,7 +31,8 @@ struct GridBarrier {
 // Sense-free generation barrier for a cooperative (co-resident) launch.
 // Every wait is bounded: on timeout the error word is set and the caller is
 // told to leave its loop. Returns false when the barrier failed.
-__device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
+__device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks,
+                                          long long spin_limit = kBarrierSpinLimit) {
     if (nblocks == 1u) {  // one block: a block barrier orders its global accesses
         __syncthreads();
         return true;
@@ -51,7 +52,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
         } else {
             long long spins = 0;
             while (gen.load(cuda::memory_order_acquire) == my_gen) {
-                if (err.load(cuda::memory_order_relaxed) != 0u || ++spins > kBarrierSpinLimit) {
+                if (err.load(cuda::memory_order_relaxed) != 0u || ++spins > spin_limit) {
                     err.fetch_or(kDevErrBarrierTimeout, cuda::memory_order_relaxed);
                     ok = 0;
                     break;
@@ -68,6 +69,17 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned nblocks) {
 
 // Barrier over the whole (cooperative) grid.
 __device__ __forceinline__ bool grid_sync(GridBarrier *bar) { return grid_sync(bar, gridDim.x); }
+
+// A barrier whose failure is also recorded in a word of the kernel's result
+// record. Blocks leave the kernel at the first failed barrier, so the block
+// that would write the final record never gets there; the timeout bit set
+// here is what tells the host that the solve did not finish.
+__device__ __forceinline__ bool grid_sync_report(GridBarrier *bar, unsigned nblocks, unsigned *report_word,
+                                                 long long spin_limit = kBarrierSpinLimit) {
+    if (grid_sync(bar, nblocks, spin_limit)) return true;
+    if (threadIdx.x == 0) atomicOr(report_word, (unsigned)kDevErrBarrierTimeout);
+    return false;
+}
 
 // Deterministic block sum of one double per thread (fixed shuffle tree).
 template <int BLOCK>

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
         double v[1] = {srr};
         write_parts<1>(k.partials, round, v, red);
     }
-    if (!grid_sync(k.bar)) return;
+    if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
     double g0[1];
     read_sums<1>(k.partials, round, g0, red);
     if (bail()) { error = FLURSYS_ERR_NON_FINITE; goto done; }
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 double v[1] = {srz};
                 write_parts<1>(k.partials, round, v, red);
             }
-            if (!grid_sync(k.bar)) return;
+            if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
             double g1[1];
             read_sums<1>(k.partials, round, g1, red);
             if (bail()) { error = FLURSYS_ERR_NON_FINITE; goto done; }
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[1] = {sdq};
                     write_parts<1>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gd[1];
                 read_sums<1>(k.partials, round, gd, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[2] = {srr, srz2};
                     write_parts<2>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gr[2];
                 read_sums<2>(k.partials, round, gr, red);
                 const double rn = sqrt(gr[0]);
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
             double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
             double rho = g0[0];  // r_hat = r0, so r_hat.r = ||r0||^2
             for (int row = tid0; row < n; row += stride) { k.p[row] = 0.0; k.v[row] = 0.0; }
-            if (!grid_sync(k.bar)) return;
+            if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
             for (long long it = 1; it <= k.max_iters; ++it) {
                 iterations = it;
                 if (!isfinite(rho)) { error = FLURSYS_ERR_NON_FINITE; break; }
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                 const double beta = (rho / rho_prev) * (alpha / omega);
                 if (!isfinite(beta)) { error = FLURSYS_ERR_BREAKDOWN; break; }
                 for (int row = tid0; row < n; row += stride) k.p[row] = k.r[row] + beta * (k.p[row] - omega * k.v[row]);
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double shv = 0.0;
                 for (int row = tid0; row < n; row += stride) {
                     const double vv = spmv_row(row, [&](int c) { return k.p[c]; });
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[1] = {shv};
                     write_parts<1>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gv[1];
                 read_sums<1>(k.partials, round, gv, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[1] = {sss};
                     write_parts<1>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gs[1];
                 read_sums<1>(k.partials, round, gs, red);
                 const double sn = sqrt(gs[0]);
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[2] = {stt, sts};
                     write_parts<2>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gt[2];
                 read_sums<2>(k.partials, round, gt, red);
                 if (bail()) { error = FLURSYS_ERR_NON_FINITE; break; }
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
                     double v[2] = {srr, shr};
                     write_parts<2>(k.partials, round, v, red);
                 }
-                if (!grid_sync(k.bar)) return;
+                if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
                 double gq[2];
                 read_sums<2>(k.partials, round, gq, red);
                 const double rn = sqrt(gq[0]);
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kBlock) krylov_kernel(KrylovArgs k) {
         }
     }
 done:
-    if (!grid_sync(k.bar)) return;
+    if (!grid_sync_report(k.bar, gridDim.x, &k.res->device_error)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         k.res->error = error;
         k.res->status = status;

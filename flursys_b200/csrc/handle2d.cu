@@ -200,21 +200,21 @@ void host_boundaries(const HostCase &hc, int nx, int ny, double dx, double dy, c
             if (!vo(i, j)) v[i + nx * j] = 0.0;
 }
 
-// adaptive_time_step (incompressible.rs:2308-2336), flow-only.
+// adaptive_time_step (incompressible.rs:2308-2336): the diffusion limit uses
+// max(alpha, nu) when the energy equation is on.
 int32_t adaptive_dt(double current, double mu, double mv, double dx, double dy, double nu,
                     const FlursysCudaConfig &c, double *out, std::string *err) {
     const double rate = mu / dx + mv / dy;
     const double cfl_dt = rate > 2.220446049250313e-16 ? c.target_cfl / rate : c.max_dt;
     const double inv = 1.0 / (dx * dx) + 1.0 / (dy * dy);
-    const double diff_dt = c.target_diffusion_number / (nu * inv);
+    const double eff = c.physics.energy_model == FLURSYS_ENERGY_CONSTANT_PROPERTIES
+                           ? std::max(c.physics.thermal_diffusivity, nu) : nu;
+    const double diff_dt = c.target_diffusion_number / (eff * inv);
     const double stable = std::min(std::min(c.max_dt, cfl_dt), diff_dt);
     if (stable < c.min_dt) {
-        char buf[512];
-        std::snprintf(buf, sizeof buf,
-                      "required stable time step %.3e is below configured min_dt %.3e; CFL constraint=%.3e, "
-                      "diffusion constraint=%.3e",
-                      stable, c.min_dt, cfl_dt, diff_dt);
-        *err = buf;
+        *err = "required stable time step " + rust_sci(stable, 3) + " is below configured min_dt " +
+               rust_sci(c.min_dt, 3) + "; CFL constraint=" + rust_sci(cfl_dt, 3) + ", diffusion constraint=" +
+               rust_sci(diff_dt, 3);
         return FLURSYS_ERR_INVALID_CONFIG;
     }
     *out = std::clamp(std::min(stable, current * c.max_growth_factor), c.min_dt, c.max_dt);
@@ -346,7 +346,29 @@ int32_t init2d(FlursysCudaHandle *h) {
     s.cylinder = c.case_params.kind == FLURSYS_CASE_CYLINDER;
     s.cylinder_mu = c.case_params.cylinder_mu;
     s.post_blocks = cavity2d_post_blocks(nx, ny, h->sms);
-    s.partials = dalloc(h2, (size_t)s.post_blocks * 8, &e);
+    s.partials = dalloc(h2, (size_t)s.post_blocks * cavity2d_post_parts(), &e);
+    // Energy equation (src/physics.rs, incompressible.rs:349-350,1441-1530):
+    // temperature starts uniform at initial_temperature.
+    const FlursysPhysicsSettings &ph = c.physics;
+    if (ph.energy_model == FLURSYS_ENERGY_CONSTANT_PROPERTIES) {
+        double *t0 = dalloc(h2, nc, &e);
+        s.temp_next = dalloc(h2, nc, &e);
+        const std::vector<double> init(nc, ph.initial_temperature);
+        if (e == cudaSuccess) e = cudaMemcpy(t0, init.data(), nc * sizeof(double), cudaMemcpyHostToDevice);
+        s.temp = t0;
+        s.alpha = ph.thermal_diffusivity;
+        s.tsource = ph.source_temperature_rate;
+        for (int side = 0; side < 4; ++side) {
+            s.tkind[side] = ph.thermal[side].kind;
+            s.twall[side] = ph.thermal[side].temperature;
+        }
+        if (ph.buoyancy == FLURSYS_BUOYANCY_BOUSSINESQ) {
+            s.buoyancy = 1;
+            s.gbx = ph.gravity_x * ph.thermal_expansion;
+            s.gby = ph.gravity_y * ph.thermal_expansion;
+            s.tref = ph.reference_temperature;
+        }
+    }
     if (e == cudaSuccess) e = cudaMalloc(&s.diag, sizeof(Diag2Dev));
     if (e == cudaSuccess) e = cudaMallocHost(&h2->h_diag, sizeof(Diag2Dev));
     if (e == cudaSuccess) e = h->pcg.allocate((long long)nc, c.precision, h->device, 2);
@@ -460,6 +482,7 @@ int32_t step2d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (simple && e == cudaSuccess) e = cavity2d_simple_relax(s, c.pressure_relaxation, st);
     if (e == cudaSuccess) e = cavity2d_boundaries(s, s.un, s.vn, st);
     if (e == cudaSuccess) e = cavity2d_post(s, st);
+    if (s.temp && e == cudaSuccess) e = cavity2d_temperature(s, step_dt, st);
     if (e == cudaSuccess) e = cudaEventRecord(h->ev[3], st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h->pcg.h_result, h->pcg.result, sizeof(PcgResultDev), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h2->h_diag, s.diag, sizeof(Diag2Dev), cudaMemcpyDeviceToHost, st);
@@ -474,13 +497,22 @@ int32_t step2d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     if (c.coupling == FLURSYS_COUPLING_PROJECTION) h->time += step_dt;
     else h->time = h->step * c.dt;
     const Diag2Dev &d = *h2->h_diag;
-    const char *names[4] = {"pressure", "u", "v", "speed"};
-    for (int f = 0; f < 4; ++f)
+    if (s.temp) {  // advance_temperature's runtime CFL check (:1449-1457)
+        const double tcfl = step_dt * (d.max_abs_uc / s.dx + d.max_abs_vc / s.dy);
+        if (tcfl > 1.0) {
+            h->err = "explicit thermal advection is unstable at step " + std::to_string((long long)h->step) +
+                     ": CFL=" + rust_sci(tcfl, 3) + " exceeds 1";
+            return FLURSYS_ERR_INVALID_CONFIG;
+        }
+        std::swap(s.temp, s.temp_next);
+    }
+    // ensure_finite (:1707-1742): the first non-finite value of pressure, u,
+    // v, speed, then temperature, read back for the message
+    const char *names[5] = {"pressure", "u", "v", "speed", "temperature"};
+    const double *fields[5] = {s.p, s.u, s.v, s.speed, s.temp};
+    for (int f = 0; f < (s.temp ? 5 : 4); ++f)
         if (d.bad_index[f] != ~0ull) {
-            char buf[200];
-            std::snprintf(buf, sizeof buf, "Non-finite %s value at flat index %llu (step %lld)", names[f],
-                          (unsigned long long)d.bad_index[f], (long long)h->step);
-            h->err = buf;
+            h->err = nonfinite_message(names[f], d.bad_index[f], fields[f], h->step, true);
             return FLURSYS_ERR_NON_FINITE;
         }
     h2->last_max_u = d.max_abs_u;
@@ -535,8 +567,13 @@ bool field_ptr2d(FlursysCudaHandle *h, int32_t id, double **p, size_t *n) {
         case FLURSYS_FIELD_VORTICITY: *p = s.vort; *n = nc; return true;
         case FLURSYS_FIELD_U_CELL: *p = s.uc; *n = nc; return true;
         case FLURSYS_FIELD_V_CELL: *p = s.vc; *n = nc; return true;
-        default: *p = nullptr; *n = 0; return false;
+        case FLURSYS_FIELD_TEMPERATURE:
+            if (!s.temp) break;
+            *p = s.temp; *n = nc; return true;
+        default: break;
     }
+    *p = nullptr; *n = 0;
+    return false;
 }
 
 // An uploaded velocity field changes the inputs of the next adaptive dt.

@@ -194,12 +194,10 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
     h->time = h->step * dt;
     // ensure_finite (incompressible_3d.rs:534-554)
     const char *names[4] = {"pressure", "u", "v", "w"};
+    const double *fields[4] = {h->s3.p, h->s3.u, h->s3.v, h->s3.w};
     for (int f = 0; f < 4; ++f) {
         if (h->h_diag3->bad_index[f] != ~0ull) {
-            char buf[160];
-            std::snprintf(buf, sizeof buf, "Non-finite 3D %s value at flat index %llu", names[f],
-                          (unsigned long long)h->h_diag3->bad_index[f]);
-            h->err = buf;
+            h->err = nonfinite_message(names[f], h->h_diag3->bad_index[f], fields[f], h->step, false);
             return FLURSYS_ERR_NON_FINITE;
         }
     }

@@ -15,7 +15,9 @@
 //     library until the process exits;
 //   * all calls share it and it keeps the last call's contents, so calls
 //     that overlap on the GPU (two streams, two threads) race; the barrier
-//     and the result record are cleared on every call;
+//     and the result record are cleared on every call, and a barrier that
+//     gives up waiting marks the record, so a timed-out solve reports
+//     FLURSYS_ERR_TIMEOUT rather than the cleared record;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture.
@@ -115,7 +117,7 @@ extern "C" int32_t flursys_cuda_stencil_pcg_noalloc(int64_t nx, int64_t ny, int6
         set_err("the allocation-free PCG solves the 3D pinned system: need nx, ny >= 1 and nz >= 2");
         return FLURSYS_ERR_INVALID_ARGUMENT;
     }
-    if (nx * ny * nz > kMaxCells) {
+    if (nx > kMaxCells || ny > kMaxCells || nz > kMaxCells || nx * ny * nz > kMaxCells) {
         set_err("grid exceeds the allocation-free PCG limit of 262144 cells (64^3)");
         return FLURSYS_ERR_INVALID_ARGUMENT;
     }

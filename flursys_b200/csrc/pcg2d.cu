@@ -57,7 +57,8 @@ struct GridSync {
     GridBarrier *bar;
     unsigned nb;
     double *partials;
-    __device__ __forceinline__ bool operator()() const { return grid_sync(bar, nb); }
+    unsigned *report;  // the instance's PcgResultDev::device_error
+    __device__ __forceinline__ bool operator()() const { return grid_sync_report(bar, nb, report); }
     __device__ __forceinline__ void put(int lb, int col, double v) const { partials[lb * kParts + col] = v; }
     __device__ __forceinline__ double get(int b, int col) const { return __ldcg(partials + b * kParts + col); }
 };
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg2d_kernel(const Pcg2dInstance *_
     if (lb >= insts[id].nblocks) return;  // spare block of the launch
     Ctx k;
     make_ctx(k, insts[id], lb);
-    const GridSync sync{k.in.barrier, (unsigned)k.in.nblocks, k.in.partials};
+    const GridSync sync{k.in.barrier, (unsigned)k.in.nblocks, k.in.partials, &k.in.result->device_error};
     if (k.in.solver == FLURSYS_PRESSURE_SOR) sor_instance(k, red, sync);
     else pcg_instance<V, MIXED>(k, red, sync);
 }

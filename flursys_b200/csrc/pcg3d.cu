@@ -118,6 +118,12 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     float *dx = a.dx;  // MIXED only
     double *part = a.partials;
     GridBarrier *bar = a.barrier;
+    // Grid barrier over the launch (plus a.barrier_extra arrivals that never
+    // come when a test injects a barrier fault); a failure is recorded in the
+    // result record before the block leaves.
+    auto gsync = [&]() -> bool {
+        return grid_sync_report(bar, gridDim.x + (unsigned)a.barrier_extra, &a.result->device_error, a.spin_limit);
+    };
     const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
     const int nblk = gridDim.x;
 
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
 
     if (blockIdx.x == 0 && threadIdx.x == 0) x[0] = 0.0;
     residual_pass(true);
-    if (!grid_sync(bar)) return;
+    if (!gsync()) return;
     double rr, rz_old, rmax;
     reduce3(rr, rz_old, rmax);
     const double initial_l2 = sqrt(rr);
@@ -365,7 +371,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
             const double t = block_sum<kBlock>(sdq, sb.red);
             if (threadIdx.x == 0) part[blockIdx.x * kNumPartials + 3] = t;
         }
-        if (!grid_sync(bar)) return;
+        if (!gsync()) return;
         const double dq = reduce_slot3();
         lap(2);
         if (fabs(dq) < 1.0e-30 || !isfinite(dq)) { error = FLURSYS_ERR_BREAKDOWN; break; }
@@ -433,7 +439,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
         }
         lap(1);
         write_partials3(srr, srz, smax);
-        if (!grid_sync(bar)) return;
+        if (!gsync()) return;
         double rz_new;
         reduce3(rr, rz_new, rmax);
         lap(2);
@@ -442,9 +448,9 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
         bool conv = l2 ? (residual <= threshold) : (residual < threshold);
         if (MIXED && (conv || ((it + 1) % a.replace_every) == 0)) {
             fold();
-            if (!grid_sync(bar)) return;
+            if (!gsync()) return;
             residual_pass(true);
-            if (!grid_sync(bar)) return;
+            if (!gsync()) return;
             reduce3(rr, rz_new, rmax);
             residual = l2 ? sqrt(rr) : rmax;
             if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
@@ -459,7 +465,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
     }
 
     if (MIXED && error == 0 && status != FLURSYS_LINEAR_CONVERGED) fold();
-    if (!grid_sync(bar)) return;
+    if (!gsync()) return;
     // ---- final FP64 check: ||b - A x||_2 of the solution in HBM ----
     double s_true = 0.0;
     stencil_pass(RyX{}, load_x, make_x, [&](int c, int, bool pin, double, double ax) {
@@ -470,7 +476,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
         const double t = block_sum<kBlock>(s_true, sb.red);
         if (threadIdx.x == 0) part[blockIdx.x * kNumPartials + 3] = t;
     }
-    if (!grid_sync(bar)) return;
+    if (!gsync()) return;
     const double true_rr = reduce_slot3();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         PcgResultDev *res = a.result;
@@ -543,6 +549,8 @@ int pcg3d_num_partials() { return kNumPartials; }
 
 cudaError_t pcg3d_launch(const Pcg3dArgs &args, int grid, int precision, cudaStream_t stream) {
     Pcg3dArgs a = args;
+    a.barrier_extra = take_injected_barrier_fault();
+    a.spin_limit = a.barrier_extra ? kInjectedFaultSpinLimit : kBarrierSpinLimit;
     Geo g = make_geo(args, grid);
     void *params[] = {&a, &g};
     if (precision == FLURSYS_PRECISION_MIXED)

@@ -40,7 +40,21 @@ struct Pcg3dArgs {
     int replace_every;
     int precision_vec_width;  // cells per vector in the pointwise pass (4 FP32, 2 FP64)
     const unsigned char *row_class;  // ny*nz bytes: 3*missing(j) + missing(k)
+    // Set by pcg3d_launch: arrivals the grid barriers wait for beyond the
+    // launched blocks (0 except under an injected barrier fault), and the
+    // poll limit of each barrier wait.
+    int barrier_extra;
+    long long spin_limit;
 };
+
+// Poll limit of the barrier waits of a launch that runs under an injected
+// barrier fault: the waits give up after a few milliseconds instead of
+// about a second.
+constexpr long long kInjectedFaultSpinLimit = 100'000LL;
+
+// Arrivals to add to the grid barriers of the next persistent 3D PCG launch
+// (0 when no fault is pending); reading it clears it.
+int take_injected_barrier_fault();
 
 size_t pcg3d_vector_bytes(int precision);
 // Device table of 3*missing(j) + missing(k) for every row (j, k) of an

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kBlock) sor3d_kernel(int nx, int ny, int nz, d
                 const double cand = (nbsum(g, p, c, i, j, k, pc) - __ldcg(rhs + c)) / diag;
                 p[c] = pc + omega * (cand - pc);
             }
-            if (!grid_sync(bar)) return;
+            if (!grid_sync_report(bar, gridDim.x, &res->device_error)) return;
         }
         double m = 0.0;
         for (long long c = tid0; c < g.n; c += stride) {
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kBlock) sor3d_kernel(int nx, int ny, int nz, d
         }
         const double bm = block_max<kBlock>(m, s_red);
         if (threadIdx.x == 0) part[blockIdx.x * 4 + (it & 1)] = bm;
-        if (!grid_sync(bar)) return;
+        if (!grid_sync_report(bar, gridDim.x, &res->device_error)) return;
         double s = 0.0;
         for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) s = fmax(s, __ldcg(&part[b * 4 + (it & 1)]));
         residual = block_max<kBlock>(s, s_red);

@@ -239,8 +239,67 @@ class TimeStepSettings:
 
 
 @dataclass
+class ThermalBoundaryCondition:
+    """src/physics.rs:17-25: "adiabatic" or "fixed-temperature" with its value."""
+    kind: str = "adiabatic"
+    temperature: float = 0.0
+
+    @classmethod
+    def fixed(cls, temperature: float) -> "ThermalBoundaryCondition":
+        return cls("fixed-temperature", temperature)
+
+
+@dataclass
+class ThermalSettings:
+    """src/physics.rs:27-56 (same fields and defaults)."""
+    model: str = "off"  # "off" | "constant-properties"
+    initial_temperature: float = 293.15
+    thermal_diffusivity: float = 2.2e-5
+    source_temperature_rate: float = 0.0
+    left: ThermalBoundaryCondition = field(default_factory=ThermalBoundaryCondition)
+    right: ThermalBoundaryCondition = field(default_factory=ThermalBoundaryCondition)
+    bottom: ThermalBoundaryCondition = field(default_factory=ThermalBoundaryCondition)
+    top: ThermalBoundaryCondition = field(default_factory=ThermalBoundaryCondition)
+
+
+@dataclass
+class BoussinesqBuoyancy:
+    """BuoyancyModel::Boussinesq (src/physics.rs:59-70): g * beta * (T - T_ref)."""
+    reference_temperature: float = 293.15
+    thermal_expansion: float = 3.4e-3
+    gravity_x: float = 0.0
+    gravity_y: float = -9.81
+
+
+@dataclass
+class PhysicsSettings:
+    """src/physics.rs:72-77; `buoyancy` is None for BuoyancyModel::Off."""
+    thermal: ThermalSettings = field(default_factory=ThermalSettings)
+    buoyancy: Optional[BoussinesqBuoyancy] = None
+
+    def fill(self, ph: _abi.PhysicsSettings) -> None:
+        t = self.thermal
+        ph.energy_model = {"off": _abi.ENERGY_OFF, "constant-properties": _abi.ENERGY_CONSTANT_PROPERTIES}[t.model]
+        ph.initial_temperature = t.initial_temperature
+        ph.thermal_diffusivity = t.thermal_diffusivity
+        ph.source_temperature_rate = t.source_temperature_rate
+        for side, bc in enumerate([t.left, t.right, t.bottom, t.top]):
+            ph.thermal[side].kind = {"adiabatic": _abi.THERMAL_ADIABATIC,
+                                     "fixed-temperature": _abi.THERMAL_FIXED_TEMPERATURE}[bc.kind]
+            ph.thermal[side].temperature = bc.temperature
+        if self.buoyancy is None:
+            ph.buoyancy = _abi.BUOYANCY_OFF
+        else:
+            b = self.buoyancy
+            ph.buoyancy = _abi.BUOYANCY_BOUSSINESQ
+            ph.reference_temperature = b.reference_temperature
+            ph.thermal_expansion = b.thermal_expansion
+            ph.gravity_x, ph.gravity_y = b.gravity_x, b.gravity_y
+
+
+@dataclass
 class SimulationConfig:
-    """src/solver/incompressible.rs:58-90 (flow-only physics)."""
+    """src/solver/incompressible.rs:58-90."""
     case: Case = field(default_factory=lambda: Case.lid_driven_cavity(CavityCase()))
     nx: int = 64
     ny: int = 64
@@ -263,6 +322,7 @@ class SimulationConfig:
     minimum_steps: int = 2000
     threads: int = 0
     boundary_overrides: SolverBoundaryOverrides = field(default_factory=SolverBoundaryOverrides)
+    physics: PhysicsSettings = field(default_factory=PhysicsSettings)
     output_dir: str = "results/cavity"
     backend: BackendOptions = field(default_factory=BackendOptions)
 
@@ -294,6 +354,7 @@ class SimulationConfig:
         cfg.pressure_relaxation = self.pressure_relaxation
         cfg.steady_tolerance = self.steady_tolerance
         cfg.minimum_steps = self.minimum_steps
+        self.physics.fill(cfg.physics)
         self.backend.apply(cfg)
         return cfg
 
@@ -338,7 +399,7 @@ class RunSummary:
 
 @dataclass
 class FieldUpdate:
-    """src/solver/incompressible.rs:231-244 (no temperature)."""
+    """src/solver/incompressible.rs:231-244."""
     nx: int
     ny: int
     pressure: np.ndarray
@@ -347,6 +408,7 @@ class FieldUpdate:
     velocity_y: np.ndarray
     vorticity: np.ndarray
     solid: np.ndarray
+    temperature: Optional[np.ndarray] = None
 
 
 class IncompressibleSolver:
@@ -394,7 +456,7 @@ class IncompressibleSolver:
         fid = {"u": _abi.FIELD_U, "v": _abi.FIELD_V, "pressure": _abi.FIELD_PRESSURE, "rhs": _abi.FIELD_RHS,
                "u_star": _abi.FIELD_U_STAR, "v_star": _abi.FIELD_V_STAR, "speed": _abi.FIELD_SPEED,
                "vorticity": _abi.FIELD_VORTICITY, "u_cell": _abi.FIELD_U_CELL,
-               "v_cell": _abi.FIELD_V_CELL}[name]
+               "v_cell": _abi.FIELD_V_CELL, "temperature": _abi.FIELD_TEMPERATURE}[name]
         return self._h.download(fid)
 
     def field_update(self) -> FieldUpdate:
@@ -406,7 +468,9 @@ class IncompressibleSolver:
                            velocity_x=(0.5 * (u[:, :-1] + u[:, 1:])).ravel(),
                            velocity_y=(0.5 * (v[:-1, :] + v[1:, :])).ravel(),
                            vorticity=self.field("vorticity"),
-                           solid=self.cfg.case.solid_mask(nx, ny).ravel())
+                           solid=self.cfg.case.solid_mask(nx, ny).ravel(),
+                           temperature=self.field("temperature")
+                           if self.cfg.physics.thermal.model == "constant-properties" else None)
 
     def close(self) -> None:
         self._h.close()

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define FLURSYS_CUDA_ABI_VERSION 1u
+#define FLURSYS_CUDA_ABI_VERSION 2u
 
 /* ------------------------------------------------------------------------
  * Status codes. 1..7 mirror LinearAlgebraError (src/linear/mod.rs:17-26);
@@ -144,6 +144,42 @@ typedef struct FlursysBoundaryOverride {
     double pressure;  /* PressureOutlet override */
 } FlursysBoundaryOverride;
 
+typedef enum FlursysEnergyModel { /* EnergyModel, src/physics.rs:9-15 */
+    FLURSYS_ENERGY_OFF = 0,
+    FLURSYS_ENERGY_CONSTANT_PROPERTIES = 1
+} FlursysEnergyModel;
+
+typedef enum FlursysThermalBoundaryKind { /* ThermalBoundaryCondition, src/physics.rs:17-25 */
+    FLURSYS_THERMAL_ADIABATIC = 0,
+    FLURSYS_THERMAL_FIXED_TEMPERATURE = 1
+} FlursysThermalBoundaryKind;
+
+typedef enum FlursysBuoyancyModel { /* BuoyancyModel, src/physics.rs:59-70 */
+    FLURSYS_BUOYANCY_OFF = 0,
+    FLURSYS_BUOYANCY_BOUSSINESQ = 1  /* body force g * beta * (T - T_ref) */
+} FlursysBuoyancyModel;
+
+typedef struct FlursysThermalBoundary {
+    int32_t kind; /* FlursysThermalBoundaryKind */
+    int32_t reserved;
+    double temperature; /* FixedTemperature value */
+} FlursysThermalBoundary;
+
+/* PhysicsSettings (src/physics.rs:72-77): ThermalSettings (:27-56) and the
+ * Boussinesq buoyancy parameters. 2D only: 3D configs with either model on
+ * are rejected, as src/project.rs:276-284 rejects them. */
+typedef struct FlursysPhysicsSettings {
+    int32_t energy_model;           /* FlursysEnergyModel */
+    int32_t buoyancy;               /* FlursysBuoyancyModel */
+    double initial_temperature;     /* uniform initial temperature, K (default 293.15) */
+    double thermal_diffusivity;     /* alpha = k / (rho cp), m^2/s (default 2.2e-5) */
+    double source_temperature_rate; /* volumetric source as a temperature rate, K/s */
+    FlursysThermalBoundary thermal[4]; /* indexed by FlursysSide */
+    double reference_temperature;   /* Boussinesq T_ref */
+    double thermal_expansion;       /* Boussinesq beta */
+    double gravity_x, gravity_y;
+} FlursysPhysicsSettings;
+
 typedef struct FlursysCudaConfig {
     uint32_t abi_version; /* FLURSYS_CUDA_ABI_VERSION */
     int32_t dimension;    /* 2 or 3 */
@@ -175,6 +211,7 @@ typedef struct FlursysCudaConfig {
     int32_t device;                     /* CUDA ordinal */
     int32_t reserved1;
     const char *fcg_weights_path;       /* learned preconditioner weights (FCG only), may be NULL */
+    FlursysPhysicsSettings physics;     /* SimulationConfig::physics (incompressible.rs:89) */
 } FlursysCudaConfig;
 
 /* SolverStep (incompressible.rs:211-229) plus backend diagnostics. */
@@ -214,7 +251,8 @@ typedef enum FlursysFieldId {
     FLURSYS_FIELD_SPEED = 8,    /* 2D cell-centred speed (compute_cell_fields, :1381-1439) */
     FLURSYS_FIELD_VORTICITY = 9,
     FLURSYS_FIELD_U_CELL = 10,
-    FLURSYS_FIELD_V_CELL = 11
+    FLURSYS_FIELD_V_CELL = 11,
+    FLURSYS_FIELD_TEMPERATURE = 12 /* 2D cell temperature nx*ny, when the energy model is on */
 } FlursysFieldId;
 
 typedef struct FlursysCudaHandle FlursysCudaHandle;
@@ -270,6 +308,17 @@ int32_t flursys_cuda_destroy(FlursysCudaHandle *h);
 
 /* Message for the last failed call on this thread that had no handle. */
 int32_t flursys_cuda_global_error(char *buf, size_t size);
+
+/* Host-side fault injection for tests of the bounded device waits. No
+ * reference counterpart. The next persistent 3D PCG launch (the kernel of
+ * flursys_cuda_stencil_pcg with nz >= 2, of flursys_cuda_stencil_pcg_noalloc,
+ * and of 3D handles configured with the persistent solver) waits at its grid
+ * barriers for `extra_arrivals` blocks that were never launched, with a poll
+ * limit of a few milliseconds; every wait gives up, the kernel returns, and
+ * the call reports FLURSYS_ERR_TIMEOUT with the device context intact. The
+ * injection applies to one launch and is then cleared; 0 cancels a pending
+ * one. Returns FLURSYS_ERR_INVALID_ARGUMENT for a negative count. */
+int32_t flursys_cuda_debug_inject_barrier_fault(int32_t extra_arrivals);
 
 /* ------------------------------------------------------------------------
  * Linear solvers with the src/linear signatures (src/linear/solver.rs:43-60,

@@ -16,6 +16,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <tuple>
@@ -34,6 +35,21 @@ void copy_msg(const std::string &s, char *buf, size_t size) {
     size_t n = std::min(size - 1, s.size());
     std::memcpy(buf, s.data(), n);
     buf[n] = '\0';
+}
+
+// Rust's `{:.Ne}` formatting of an f64: mantissa with N decimals, then `e`
+// and the exponent without sign padding or leading zeros ("1.500e-5").
+std::string rust_sci(double v, int prec) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.*e", prec, v);
+    std::string s(buf);
+    const size_t e = s.find('e');
+    if (e == std::string::npos) return s;
+    const std::string mant = s.substr(0, e);
+    int exp10 = std::atoi(s.c_str() + e + 1);
+    return mant + "e" + std::to_string(exp10);
 }
 
 // ---------------------------------------------------------------------------
@@ -399,12 +415,10 @@ int32_t adaptive_dt(double current_dt, double mu, double mv, double dx, double d
     double diffusion_dt = target_diff / (eff * inv);
     double stable = std::min(std::min(max_dt, cfl_dt), diffusion_dt);
     if (stable < min_dt) {
-        char buf[512];
-        std::snprintf(buf, sizeof buf,
-                      "required stable time step %.3e is below configured min_dt %.3e; CFL "
-                      "constraint=%.3e, diffusion constraint=%.3e",
-                      stable, min_dt, cfl_dt, diffusion_dt);
-        if (err) *err = buf;
+        if (err)
+            *err = "required stable time step " + rust_sci(stable, 3) + " is below configured min_dt " +
+                   rust_sci(min_dt, 3) + "; CFL constraint=" + rust_sci(cfl_dt, 3) +
+                   ", diffusion constraint=" + rust_sci(diffusion_dt, 3);
         return FLURSYS_ERR_INVALID_CONFIG;
     }
     double limited = std::min(stable, current_dt * growth);
@@ -714,8 +728,9 @@ struct Solver3D final : OracleSolver {
             size_t bad = 0;
             if (!all_finite(*fs[f], &bad)) {
                 char buf[256];
-                std::snprintf(buf, sizeof buf, "Non-finite 3D %s value at flat index %zu: %g",
-                              names[f], bad, (*fs[f])[bad]);
+                const double bv = (*fs[f])[bad];
+                std::snprintf(buf, sizeof buf, "Non-finite 3D %s value at flat index %zu: %s",
+                              names[f], bad, std::isnan(bv) ? "NaN" : (bv > 0 ? "inf" : "-inf"));
                 err = buf;
                 return FLURSYS_ERR_NON_FINITE;
             }
@@ -771,6 +786,8 @@ struct Solver2D final : OracleSolver {
     CaseModel cm;
     std::vector<uint8_t> solid;
     std::vector<double> p, rhs, u, v, us, vs, uc, vc, speed, vort;
+    std::vector<double> temp;  // cell temperature (empty when the energy model is off)
+    bool thermal = false, boussinesq = false;
     double current_dt;
 
     size_t iu(int64_t i, int64_t j) const { return i + (nx + 1) * j; }
@@ -799,6 +816,9 @@ struct Solver2D final : OracleSolver {
         u.assign((nx + 1) * ny, 0.0);
         v.assign(nx * (ny + 1), 0.0);
         us = u; vs = v;
+        thermal = c.physics.energy_model == FLURSYS_ENERGY_CONSTANT_PROPERTIES;
+        boussinesq = c.physics.buoyancy == FLURSYS_BUOYANCY_BOUSSINESQ;
+        if (thermal) temp.assign(nx * ny, c.physics.initial_temperature);  // :349-350
         initialize_velocity();
         compute_cell_fields();
     }
@@ -919,12 +939,18 @@ struct Solver2D final : OracleSolver {
 
     bool simple() const { return cfg.coupling == FLURSYS_COUPLING_SIMPLE; }
 
-    // predict_momentum (:748-922), without buoyancy.
+    // predict_momentum (:748-922), with the Boussinesq body force
+    // g * beta * (face temperature - T_ref) (:831-846, :896-911) when the
+    // buoyancy model is on and a temperature field exists (0.0 otherwise).
     int32_t predict(double step_dt) override {
         std::fill(us.begin(), us.end(), 0.0);
         std::fill(vs.begin(), vs.end(), 0.0);
         const bool with_p = simple();
         const double relax = with_p ? cfg.velocity_relaxation : 1.0;
+        const bool buoy = boussinesq && thermal;
+        const double tref = boussinesq ? cfg.physics.reference_temperature : 0.0;
+        const double gbx = cfg.physics.gravity_x * cfg.physics.thermal_expansion;
+        const double gby = cfg.physics.gravity_y * cfg.physics.thermal_expansion;
 #pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
         for (int64_t j = 0; j < ny; ++j)
             for (int64_t i = 1; i < nx; ++i) {
@@ -940,7 +966,8 @@ struct Solver2D final : OracleSolver {
                 double conv = (ue * pe - uw * pw) / dx + (vn * pn - vsf * ps) / dy;
                 double diff = (ue_nb - 2.0 * up + uw_nb) / (dx * dx) + (un_nb - 2.0 * up + us_nb) / (dy * dy);
                 double pg = with_p ? (p[ic(i, j)] - p[ic(i - 1, j)]) / dx : 0.0;
-                us[iu(i, j)] = up + relax * step_dt * (-conv + nu * diff - pg / rho);
+                double bx = buoy ? gbx * (0.5 * (temp[ic(i - 1, j)] + temp[ic(i, j)]) - tref) : 0.0;
+                us[iu(i, j)] = up + relax * step_dt * (-conv + nu * diff - pg / rho + bx);
             }
 #pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
         for (int64_t j = 1; j < ny; ++j)
@@ -957,7 +984,8 @@ struct Solver2D final : OracleSolver {
                 double conv = (ue * pe - uw * pw) / dx + (vn * pn - vsf * ps) / dy;
                 double diff = (ve_nb - 2.0 * vp + vw_nb) / (dx * dx) + (vn_nb - 2.0 * vp + vs_nb) / (dy * dy);
                 double pg = with_p ? (p[ic(i, j)] - p[ic(i, j - 1)]) / dy : 0.0;
-                vs[iv(i, j)] = vp + relax * step_dt * (-conv + nu * diff - pg / rho);
+                double by = buoy ? gby * (0.5 * (temp[ic(i, j - 1)] + temp[ic(i, j)]) - tref) : 0.0;
+                vs[iv(i, j)] = vp + relax * step_dt * (-conv + nu * diff - pg / rho + by);
             }
         return FLURSYS_OK;
     }
@@ -1165,6 +1193,46 @@ struct Solver2D final : OracleSolver {
         if (q > 0.0) { *cd = fx / q; *cl = fy / q; }
     }
 
+    // temperature_neighbor (:1495-1530): solid neighbours and adiabatic
+    // walls mirror the centre, a fixed-temperature wall is 2 T_w - centre.
+    double temp_nb(const std::vector<double> &t, int64_t i, int64_t j, int di, int dj, double center) const {
+        const int64_t ni = i + di, nj = j + dj;
+        if (ni >= 0 && ni < nx && nj >= 0 && nj < ny) return sol(ni, nj) ? center : t[ic(ni, nj)];
+        const int side = ni < 0 ? FLURSYS_SIDE_LEFT
+                                : (ni >= nx ? FLURSYS_SIDE_RIGHT : (nj < 0 ? FLURSYS_SIDE_BOTTOM : FLURSYS_SIDE_TOP));
+        const FlursysThermalBoundary &b = cfg.physics.thermal[side];
+        return b.kind == FLURSYS_THERMAL_FIXED_TEMPERATURE ? 2.0 * b.temperature - center : center;
+    }
+    // advance_temperature (:1441-1493): explicit conservative upwind update
+    // on the new face velocities, after the runtime thermal CFL check.
+    int32_t advance_temperature(double step_dt) {
+        if (!thermal) return FLURSYS_OK;
+        const double cfl = step_dt * (field_max_abs(uc) / dx + field_max_abs(vc) / dy);
+        if (cfl > 1.0) {
+            err = "explicit thermal advection is unstable at step " + std::to_string((long long)step) +
+                  ": CFL=" + rust_sci(cfl, 3) + " exceeds 1";
+            return FLURSYS_ERR_INVALID_CONFIG;
+        }
+        const std::vector<double> old = temp;
+        const double alpha = cfg.physics.thermal_diffusivity, source = cfg.physics.source_temperature_rate;
+        auto upw = [](double fv, double pos, double neg) { return fv >= 0.0 ? pos : neg; };
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                const int64_t k = ic(i, j);
+                if (sol(i, j)) { temp[k] = old[k]; continue; }
+                const double c = old[k];
+                const double e = temp_nb(old, i, j, 1, 0, c), w = temp_nb(old, i, j, -1, 0, c);
+                const double n = temp_nb(old, i, j, 0, 1, c), so = temp_nb(old, i, j, 0, -1, c);
+                const double ue = u[iu(i + 1, j)], uw = u[iu(i, j)], vn = v[iv(i, j + 1)], vsf = v[iv(i, j)];
+                const double fe = ue * upw(ue, c, e), fw = uw * upw(uw, w, c);
+                const double fn = vn * upw(vn, c, n), fs = vsf * upw(vsf, so, c);
+                const double conv = (fe - fw) / dx + (fn - fs) / dy;
+                const double diff = (e - 2.0 * c + w) / (dx * dx) + (n - 2.0 * c + so) / (dy * dy);
+                temp[k] = c + step_dt * (-conv + alpha * diff + source);
+            }
+        return FLURSYS_OK;
+    }
+
     // reached_end_time (:557-561)
     bool reached_end_time() const {
         double tol = 2.220446049250313e-16 * std::max(std::fabs(cfg.t_end), 1.0) * 16.0;
@@ -1179,7 +1247,8 @@ struct Solver2D final : OracleSolver {
         }
         double step_dt = cfg.dt;
         if (cfg.adaptive) {
-            int32_t st = adaptive_dt(current_dt, field_max_abs(u), field_max_abs(v), dx, dy, nu, -1.0,
+            int32_t st = adaptive_dt(current_dt, field_max_abs(u), field_max_abs(v), dx, dy, nu,
+                                     thermal ? cfg.physics.thermal_diffusivity : -1.0,
                                      cfg.min_dt, cfg.max_dt, cfg.target_cfl, cfg.target_diffusion_number,
                                      cfg.max_growth_factor, &step_dt, &err);
             if (st) return st;
@@ -1215,15 +1284,17 @@ struct Solver2D final : OracleSolver {
         if (cfg.coupling == FLURSYS_COUPLING_PROJECTION) time += step_dt;
         else time = step * cfg.dt;
         compute_cell_fields();
+        if (int32_t tst = advance_temperature(step_dt)) return tst;
         // ensure_finite (:1707-1742)
-        const char *names[4] = {"pressure", "u", "v", "speed"};
-        std::vector<double> *fs[4] = {&p, &u, &v, &speed};
-        for (int f = 0; f < 4; ++f) {
+        const char *names[5] = {"pressure", "u", "v", "speed", "temperature"};
+        std::vector<double> *fs[5] = {&p, &u, &v, &speed, &temp};
+        for (int f = 0; f < 5; ++f) {
             size_t bad = 0;
             if (!all_finite(*fs[f], &bad)) {
                 char buf[256];
-                std::snprintf(buf, sizeof buf, "Non-finite %s value at flat index %zu: %g (step %lld)",
-                              names[f], bad, (*fs[f])[bad], (long long)step);
+                const double bv = (*fs[f])[bad];
+                std::snprintf(buf, sizeof buf, "Non-finite %s value at flat index %zu: %s (step %lld)",
+                              names[f], bad, std::isnan(bv) ? "NaN" : (bv > 0 ? "inf" : "-inf"), (long long)step);
                 err = buf;
                 return FLURSYS_ERR_NON_FINITE;
             }
@@ -1269,6 +1340,7 @@ struct Solver2D final : OracleSolver {
             case FLURSYS_FIELD_VORTICITY: return &vort;
             case FLURSYS_FIELD_U_CELL: return &uc;
             case FLURSYS_FIELD_V_CELL: return &vc;
+            case FLURSYS_FIELD_TEMPERATURE: return thermal ? &temp : nullptr;
             default: return nullptr;
         }
     }
@@ -1579,6 +1651,8 @@ int32_t solve_bicgstab(const Csr &a, const double *rhs, double *x, const Flursys
 int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
     auto fin_pos = [](double x) { return std::isfinite(x) && x > 0.0; };
     if (c.dimension == 3) {
+        // src/project.rs:276-284: the 3D backend runs constant-property flow only
+        if (c.physics.energy_model != FLURSYS_ENERGY_OFF || c.physics.buoyancy != FLURSYS_BUOYANCY_OFF) { *msg = "the current 3D backend supports constant-property flow only; thermal and buoyancy models are not available"; return FLURSYS_ERR_UNSUPPORTED; }
         if (c.nx < 4 || c.ny < 4 || c.nz < 4) { *msg = "nx, ny, and nz must all be at least 4"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0 && c.case_params.depth > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
         if (!fin_pos(c.case_params.density)) { *msg = "density must be finite and positive"; return FLURSYS_ERR_INVALID_CONFIG; }
@@ -1613,6 +1687,23 @@ int32_t validate_config(const FlursysCudaConfig &c, std::string *msg) {
         if (!std::isfinite(c.max_growth_factor) || c.max_growth_factor < 1.0) { *msg = "adaptive max_growth_factor must be finite and at least 1"; return FLURSYS_ERR_INVALID_CONFIG; }
     }
     if (!(c.case_params.length > 0.0 && c.case_params.height > 0.0)) { *msg = "Domain dimensions must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+    // PhysicsSettings::validate (src/physics.rs:79-131) at min_dt when
+    // adaptive, else dt (incompressible.rs:180-189)
+    const FlursysPhysicsSettings &ph = c.physics;
+    const bool thermal = ph.energy_model == FLURSYS_ENERGY_CONSTANT_PROPERTIES;
+    if (thermal) {
+        if (!std::isfinite(ph.initial_temperature) || !std::isfinite(ph.thermal_diffusivity) || ph.thermal_diffusivity <= 0.0 || !std::isfinite(ph.source_temperature_rate)) { *msg = "thermal initial temperature, diffusivity, and source must be finite; diffusivity must be positive"; return FLURSYS_ERR_INVALID_CONFIG; }
+        for (int s = 0; s < 4; ++s)
+            if (ph.thermal[s].kind == FLURSYS_THERMAL_FIXED_TEMPERATURE && !std::isfinite(ph.thermal[s].temperature)) { *msg = "fixed thermal boundary temperatures must be finite"; return FLURSYS_ERR_INVALID_CONFIG; }
+        const double vdt = c.adaptive ? c.min_dt : c.dt;
+        const double dx = c.case_params.length / c.nx, dy = c.case_params.height / c.ny;
+        const double fourier = ph.thermal_diffusivity * vdt * (std::pow(1.0 / dx, 2) + std::pow(1.0 / dy, 2));
+        if (fourier > 0.5) { *msg = "explicit thermal diffusion is unstable: alpha*dt*(1/dx^2 + 1/dy^2)=" + rust_sci(fourier, 3) + " exceeds 0.5"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
+    if (ph.buoyancy == FLURSYS_BUOYANCY_BOUSSINESQ) {
+        if (!thermal) { *msg = "Boussinesq buoyancy requires the constant-property energy equation"; return FLURSYS_ERR_INVALID_CONFIG; }
+        if (!std::isfinite(ph.reference_temperature) || !std::isfinite(ph.thermal_expansion) || ph.thermal_expansion < 0.0 || !std::isfinite(ph.gravity_x) || !std::isfinite(ph.gravity_y)) { *msg = "Boussinesq reference temperature, expansion coefficient, and gravity must be finite; expansion must be non-negative"; return FLURSYS_ERR_INVALID_CONFIG; }
+    }
     return FLURSYS_OK;
 }
 
@@ -1750,6 +1841,9 @@ int32_t orc_default_config(int32_t dimension, FlursysCudaConfig *c) {
     c->pressure_rtol = 1.0e-8;
     c->precision = FLURSYS_PRECISION_F64;
     c->residual_replacement_every = 50;
+    // ThermalSettings::default (src/physics.rs:43-56); buoyancy off
+    c->physics.initial_temperature = 293.15;
+    c->physics.thermal_diffusivity = 2.2e-5;
     if (c->dimension == 3) {
         c->nx = c->ny = c->nz = 32;
         c->dt = 5.0e-4;

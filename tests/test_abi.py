@@ -37,6 +37,8 @@ STRUCTS = {
     "FlursysBoundaryOverride": _abi.BoundaryOverride,
     "FlursysCudaConfig": _abi.CudaConfig,
     "FlursysStepReport": _abi.StepReport,
+    "FlursysThermalBoundary": _abi.ThermalBoundary,
+    "FlursysPhysicsSettings": _abi.PhysicsSettings,
 }
 
 
@@ -74,6 +76,12 @@ def test_default_config_mirrors_reference_defaults():
     assert cfg.case_params.reynolds == 100.0 and cfg.pressure_solver == _abi.PRESSURE_SOR
     assert lib.flursys_cuda_default_config(2, C.byref(cfg)) == 0
     assert (cfg.nx, cfg.ny) == (64, 64) and cfg.pressure_tolerance == 1e-5 and cfg.pressure_max_iters == 1200
+    # ThermalSettings::default / BuoyancyModel::default (src/physics.rs:43-56,59-70)
+    ph = cfg.physics
+    assert ph.energy_model == _abi.ENERGY_OFF and ph.buoyancy == _abi.BUOYANCY_OFF
+    assert ph.initial_temperature == 293.15 and ph.thermal_diffusivity == 2.2e-5
+    assert ph.source_temperature_rate == 0.0
+    assert all(ph.thermal[s].kind == _abi.THERMAL_ADIABATIC for s in range(4))
 
 
 def test_create_rejects_invalid_configs_before_touching_a_device():

@@ -148,3 +148,31 @@ def test_stencil_pcg_entry_matches_oracle(oracle, cudalib, precision):
     assert rel_l2(x, xref) < tol
     if precision == _abi.PRECISION_F64:
         assert abs(rep.iterations - rref.iterations) <= 1
+
+
+def test_mixed_128_cubed_velocity_within_bound_of_fp64_oracle(oracle):
+    """The benchmark's workload: 128^3, Re 400, mixed PCG to 1e-8 relative L2,
+    three steps from the zero field, against the FP64 oracle on the same
+    config: velocity within 1e-6 relative L2 (u, v, w together and each)."""
+    import os
+    n = 128
+    cfg64 = cfg3d(oracle, n, n, n, rtol=1e-8)
+    cfgm = cfg3d(oracle, n, n, n, rtol=1e-8, precision=_abi.PRECISION_MIXED)
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        ref = oracle.OracleSolver(cfg64)
+        gpu = _Handle(cfgm)
+        for _ in range(3):
+            ref.step(1)
+            rep = gpu.step(1)
+            assert rep.pressure_status == _abi.LINEAR_CONVERGED
+            assert rep.pressure_true_relative_residual <= 1.0e-8 * 1.0001
+    finally:
+        oracle.set_threads(1)
+    du = nu = 0.0
+    for fid, name in FIELDS[:3]:
+        a, b = gpu.download(fid), ref.get(fid)
+        assert rel_l2(a, b) <= MIXED_TOL, name
+        du += float(np.sum((a - b) ** 2))
+        nu += float(np.sum(b ** 2))
+    assert (du / nu) ** 0.5 <= MIXED_TOL
