@@ -242,3 +242,237 @@ def simple_channel(cfg):
     st = lib.orc_simple_channel(C.byref(cfg), _abi.dptr(u), _abi.dptr(v), _abi.dptr(p), _abi.dptr(flux),
                                 _abi.dptr(hist), C.byref(rep))
     return st, u, v, p, flux, hist[:rep.outer_iterations + 1], rep
+
+
+# ---------------------------------------------------------------------------
+# Face-based meshes for the SIMPLE building blocks (test infrastructure)
+# ---------------------------------------------------------------------------
+class FvMesh:
+    """UnstructuredMesh::from_cells (src/mesh.rs:317-423) for 2D polygons:
+    faces are the polygons' edges in cell order and edge order, shared edges
+    are merged (the first cell owns the face), the area vector is the edge
+    (dy, -dx) oriented away from the owner's vertex average, the face centre
+    is the edge midpoint, and cell centre and volume are the polygon's
+    centroid and area (unit depth)."""
+
+    def __init__(self, points, cells):
+        pts = np.asarray(points, dtype=np.float64)
+        self.nc = len(cells)
+        owner, neigh, area, fc, verts = [], [], [], [], []
+        lookup = {}
+        cc, vol = [], []
+        for c, poly in enumerate(cells):
+            ref = pts[poly].mean(axis=0)
+            for a, b in zip(poly, poly[1:] + poly[:1]):
+                key = tuple(sorted((a, b)))
+                if key in lookup:
+                    neigh[lookup[key]] = c
+                    continue
+                e = pts[b] - pts[a]
+                s = np.array([e[1], -e[0], 0.0])
+                mid = 0.5 * (pts[a] + pts[b])
+                if np.dot(s, mid - ref) < 0.0:
+                    s = -s
+                lookup[key] = len(owner)
+                owner.append(c)
+                neigh.append(-1)
+                area.append(s)
+                fc.append(mid)
+                verts.append(key)
+            # shoelace centroid and area
+            x, y = pts[poly, 0], pts[poly, 1]
+            x1, y1 = np.roll(x, -1), np.roll(y, -1)
+            cr = x * y1 - x1 * y
+            a2 = cr.sum()
+            vol.append(0.5 * abs(a2))
+            cc.append([((x + x1) * cr).sum() / (3.0 * a2), ((y + y1) * cr).sum() / (3.0 * a2), 0.0])
+        self.nf = len(owner)
+        self.owner = np.array(owner, dtype=np.int64)
+        self.neigh = np.array(neigh, dtype=np.int64)
+        self.area = np.ascontiguousarray(np.array(area), dtype=np.float64)
+        self.fc = np.ascontiguousarray(np.array(fc), dtype=np.float64)
+        self.cc = np.ascontiguousarray(np.array(cc), dtype=np.float64)
+        self.vol = np.array(vol, dtype=np.float64)
+
+    def args(self):
+        return (self.nc, self.nf, _abi.i64ptr(self.owner), _abi.i64ptr(self.neigh), _abi.dptr(self.area),
+                _abi.dptr(self.fc), _abi.dptr(self.cc), _abi.dptr(self.vol))
+
+    def boundary_faces(self):
+        return np.nonzero(self.neigh < 0)[0]
+
+    def internal_faces(self):
+        return np.nonzero(self.neigh >= 0)[0]
+
+
+def quad_grid(nx, ny, x0=0.0, y0=0.0, dx=1.0, dy=1.0):
+    """Cells (x fastest) of an nx x ny grid of axis-aligned quads, as the
+    reference's test helpers square_grid / cavity_grid / channel build them
+    (points x fastest, polygons counter-clockwise)."""
+    pts = [(x0 + i * dx, y0 + j * dy, 0.0) for j in range(ny + 1) for i in range(nx + 1)]
+    p = lambda i, j: i + (nx + 1) * j  # noqa: E731
+    cells = [[p(i, j), p(i + 1, j), p(i + 1, j + 1), p(i, j + 1)] for j in range(ny) for i in range(nx)]
+    return FvMesh(pts, cells)
+
+
+_FV = [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D, _D]
+_I32P = C.POINTER(C.c_int32)
+
+
+def _fv_sigs(lib):
+    sig = {
+        "orc_fv_pressure_face_coefficients": _FV + [_D, _I32P, _D, _D],
+        "orc_fv_correct_face_flux": _FV + [_D, _D, _D, _I32P, _D, _D],
+        "orc_fv_assemble_pressure_correction": _FV + [_D, _D, _I32P, _D, C.c_int64, _I64P, _I64P, _D, C.c_int64,
+                                                      _I64P, _D],
+        "orc_fv_continuity_rms": _FV + [_D, _D],
+        "orc_fv_correct_cell_velocity": [C.c_int64, _D, _D, _D, _D],
+        "orc_fv_initial_face_flux": _FV + [_D, _D, _D],
+        "orc_fv_assemble_momentum": _FV + [C.c_double, _I32P, _D, _D, _D, _D, C.c_double, _I64P, _I64P, _D,
+                                           C.c_int64, _I64P, _D],
+        "orc_fv_simple": _FV + [_I32P, _D, _I32P, _D, _I32P, _D, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                C.c_int64, C.c_double, C.POINTER(_abi.LinearSolverOptions),
+                                C.POINTER(_abi.LinearSolverOptions), _D, _D, _D, _D, C.POINTER(_abi.SimpleReport)],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = C.c_int32
+        fn.argtypes = args
+
+
+def _i32(a):
+    if a is None:
+        return None
+    arr = np.ascontiguousarray(a, dtype=np.int32)
+    return arr, arr.ctypes.data_as(_I32P)
+
+
+def _dp(a):
+    if a is None:
+        return None
+    return _abi.dptr(a)
+
+
+def _bc(mesh, bc):
+    """bc: None, or (fixed[nf] of 0/1, value[nf])."""
+    if bc is None:
+        return None, None, None
+    fixed, value = bc
+    f = np.ascontiguousarray(fixed, dtype=np.int32)
+    v = np.ascontiguousarray(value, dtype=np.float64)
+    return (f, v), f.ctypes.data_as(_I32P), _abi.dptr(v)
+
+
+def fv_pressure_face_coefficients(mesh, rau, pc_bc=None):
+    lib = load()
+    _fv_sigs(lib)
+    rau = np.ascontiguousarray(rau, dtype=np.float64)
+    out = np.zeros(mesh.nf)
+    keep, f, v = _bc(mesh, pc_bc)
+    st = lib.orc_fv_pressure_face_coefficients(*mesh.args(), _abi.dptr(rau), f, v, _abi.dptr(out))
+    return st, out
+
+
+def fv_correct_face_flux(mesh, predicted, coef, correction, pc_bc=None):
+    lib = load()
+    _fv_sigs(lib)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (predicted, coef, correction)]
+    out = np.zeros(mesh.nf)
+    keep, f, v = _bc(mesh, pc_bc)
+    st = lib.orc_fv_correct_face_flux(*mesh.args(), *[_abi.dptr(x) for x in a], f, v, _abi.dptr(out))
+    return st, out
+
+
+def fv_assemble_pressure_correction(mesh, predicted, coef, reference_cell=0, pc_bc=None):
+    """Returns (status, row_offsets, columns, values, rhs)."""
+    lib = load()
+    _fv_sigs(lib)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (predicted, coef)]
+    cap = 4 * mesh.nf + mesh.nc + 1
+    ro = np.zeros(mesh.nc + 1, dtype=np.int64)
+    ci = np.zeros(cap, dtype=np.int64)
+    va = np.zeros(cap)
+    rhs = np.zeros(mesh.nc)
+    nnz = C.c_int64()
+    keep, f, v = _bc(mesh, pc_bc)
+    st = lib.orc_fv_assemble_pressure_correction(*mesh.args(), *[_abi.dptr(x) for x in a], f, v, reference_cell,
+                                                 _abi.i64ptr(ro), _abi.i64ptr(ci), _abi.dptr(va), cap,
+                                                 C.byref(nnz), _abi.dptr(rhs))
+    return st, ro, ci[:nnz.value], va[:nnz.value], rhs
+
+
+def fv_continuity_rms(mesh, flux):
+    lib = load()
+    _fv_sigs(lib)
+    f = np.ascontiguousarray(flux, dtype=np.float64)
+    out = C.c_double()
+    st = lib.orc_fv_continuity_rms(*mesh.args(), _abi.dptr(f), C.byref(out))
+    return st, out.value
+
+
+def fv_correct_cell_velocity(predictor, rau, grad):
+    lib = load()
+    _fv_sigs(lib)
+    p = np.ascontiguousarray(predictor, dtype=np.float64)
+    r = np.ascontiguousarray(rau, dtype=np.float64)
+    g = np.ascontiguousarray(grad, dtype=np.float64)
+    out = np.zeros_like(p)
+    st = lib.orc_fv_correct_cell_velocity(r.size, _abi.dptr(p), _abi.dptr(r), _abi.dptr(g), _abi.dptr(out))
+    return st, out
+
+
+def fv_initial_face_flux(mesh, velocity, wall_flux):
+    lib = load()
+    _fv_sigs(lib)
+    u = np.ascontiguousarray(velocity, dtype=np.float64)
+    w = np.ascontiguousarray(wall_flux, dtype=np.float64)
+    out = np.zeros(mesh.nf)
+    st = lib.orc_fv_initial_face_flux(*mesh.args(), _abi.dptr(u), _abi.dptr(w), _abi.dptr(out))
+    return st, out
+
+
+def fv_assemble_momentum(mesh, nu, bc, flux, source=None, current=None, alpha=1.0):
+    """Returns (status, row_offsets, columns, values, rhs)."""
+    lib = load()
+    _fv_sigs(lib)
+    fl = np.ascontiguousarray(flux, dtype=np.float64)
+    src = None if source is None else np.ascontiguousarray(source, dtype=np.float64)
+    cur = None if current is None else np.ascontiguousarray(current, dtype=np.float64)
+    cap = 4 * mesh.nf + mesh.nc + 1
+    ro = np.zeros(mesh.nc + 1, dtype=np.int64)
+    ci = np.zeros(cap, dtype=np.int64)
+    va = np.zeros(cap)
+    rhs = np.zeros(mesh.nc)
+    nnz = C.c_int64()
+    keep, f, v = _bc(mesh, bc)
+    st = lib.orc_fv_assemble_momentum(*mesh.args(), nu, f, v, _abi.dptr(fl), _dp(src), _dp(cur), alpha,
+                                      _abi.i64ptr(ro), _abi.i64ptr(ci), _abi.dptr(va), cap, C.byref(nnz),
+                                      _abi.dptr(rhs))
+    return st, ro, ci[:nnz.value], va[:nnz.value], rhs
+
+
+def fv_simple(mesh, vel_bc, p_bc, pc_bc=None, reference_cell=0, nu=0.1, velocity_relaxation=0.7,
+              pressure_relaxation=0.3, max_outer=200, continuity_tolerance=1e-10,
+              momentum_solver=(1e-10, 1e-8, 1000), pressure_solver=(1e-10, 1e-8, 1000), velocity=None,
+              pressure=None, face_flux=None):
+    """solve_simple on `mesh`. vel_bc = (fixed[nf], value[nf, 3]); p_bc and
+    pc_bc = (fixed[nf], value[nf]) or None. Returns (status, velocity[nc, 3],
+    pressure, face_flux, history, report)."""
+    lib = load()
+    _fv_sigs(lib)
+    u = np.zeros((mesh.nc, 3)) if velocity is None else np.array(velocity, dtype=np.float64).reshape(mesh.nc, 3)
+    u = np.ascontiguousarray(u)
+    p = np.zeros(mesh.nc) if pressure is None else np.array(pressure, dtype=np.float64)
+    fl = np.zeros(mesh.nf) if face_flux is None else np.array(face_flux, dtype=np.float64)
+    hist = np.zeros(max_outer + 1)
+    rep = _abi.SimpleReport()
+    vf = np.ascontiguousarray(vel_bc[0], dtype=np.int32)
+    vv = np.ascontiguousarray(np.asarray(vel_bc[1], dtype=np.float64).reshape(mesh.nf, 3))
+    kp, pf, pv = _bc(mesh, p_bc if p_bc is not None else (np.zeros(mesh.nf), np.zeros(mesh.nf)))
+    kc, cf, cv = _bc(mesh, pc_bc)
+    st = lib.orc_fv_simple(*mesh.args(), vf.ctypes.data_as(_I32P), _abi.dptr(vv), pf, pv, cf, cv, reference_cell,
+                           nu, velocity_relaxation, pressure_relaxation, max_outer, continuity_tolerance,
+                           C.byref(_abi.LinearSolverOptions(*momentum_solver)),
+                           C.byref(_abi.LinearSolverOptions(*pressure_solver)), _abi.dptr(u), _abi.dptr(p),
+                           _abi.dptr(fl), _abi.dptr(hist), C.byref(rep))
+    return st, u, p, fl, hist[:rep.outer_iterations + 1], rep

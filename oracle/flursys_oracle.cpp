@@ -2194,71 +2194,174 @@ struct SimpleOut {
     FlursysSimpleReport rep{};
 };
 
-// solve_incompressible + solve_simple for the channel case.
-int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
-    const int64_t nx = cfg.nx, ny = cfg.ny;
-    if (nx < 2 || ny < 2) return FLURSYS_ERR_INVALID_CONFIG;
-    if (cfg.max_outer_iterations < 1) return FLURSYS_ERR_INVALID_CONFIG;
-    if (!(cfg.pressure_relaxation > 0.0 && cfg.pressure_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
-    if (!(cfg.velocity_relaxation > 0.0 && cfg.velocity_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
-    const FvMesh m = channel_mesh(nx, ny, cfg.length, cfg.height);
-    const int64_t n = m.ncells(), nf = m.nfaces();
-    const double H = cfg.height, U = cfg.inlet_peak_velocity;
-    // resolve_boundaries (unstructured_incompressible.rs:106-212)
-    ScalarBc vel[3], pbc, pcbc;
-    for (ScalarBc *b : {&vel[0], &vel[1], &vel[2], &pbc, &pcbc}) {
-        b->fixed.assign(nf, 0);
-        b->value.assign(nf, 0.0);
-    }
-    std::vector<double> bflux(nf, 0.0);
-    for (int64_t f = 0; f < nf; ++f) {
-        if (m.patch[f] == kInternal) continue;
-        if (m.patch[f] == kOutlet) {
-            pbc.fixed[f] = 1;
-            pbc.value[f] = cfg.outlet_pressure;
-            pcbc.fixed[f] = 1;
-            pcbc.value[f] = 0.0;
-            continue;  // velocity zero gradient, no prescribed flux
+// pressure_face_coefficients[_with_boundary] (simple.rs:342-410): rAU
+// interpolated to internal faces times (S.d)/(d.d); fixed correction faces
+// (pcbc != null) take rAU_P (S.d)/(d.d) with d from the owner to the face.
+int32_t pressure_face_coefficients(const FvMesh &m, const std::vector<double> &rau, const ScalarBc *pcbc,
+                                   std::vector<double> *coef) {
+    coef->assign(m.nfaces(), 0.0);
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        const int64_t o = m.owner[f];
+        double c;
+        if (m.neigh[f] >= 0) {
+            const int64_t nb = m.neigh[f];
+            const V3 d = m.cc[nb] - m.cc[o];
+            const double d2 = dot(d, d);
+            if (!std::isfinite(d2) || d2 <= 2.220446049250313e-16) return FLURSYS_ERR_INVALID_CONFIG;
+            const double l = iweight(m, f);
+            c = (rau[o] * (1.0 - l) + rau[nb] * l) * dot(m.area[f], d) / d2;
+        } else if (pcbc && pcbc->fixed[f]) {
+            const V3 d = m.fc[f] - m.cc[o];
+            const double d2 = dot(d, d);
+            if (!std::isfinite(d2) || d2 <= 2.220446049250313e-16) return FLURSYS_ERR_INVALID_CONFIG;
+            c = rau[o] * dot(m.area[f], d) / d2;
+        } else {
+            continue;
         }
-        V3 u{};
-        if (m.patch[f] == kInlet) {
-            const double y = m.fc[f].y;
-            u.x = U * 4.0 * y * (H - y) / (H * H);
-        }
-        vel[0].fixed[f] = vel[1].fixed[f] = vel[2].fixed[f] = 1;
-        vel[0].value[f] = u.x;
-        vel[1].value[f] = u.y;
-        vel[2].value[f] = u.z;
-        bflux[f] = dot(u, m.area[f]);
+        if (!std::isfinite(c) || c <= 0.0) return FLURSYS_ERR_INVALID_CONFIG;  // InvalidPressureFaceCoefficient
+        (*coef)[f] = c;
     }
-    LsStencil stencil;
-    int32_t st = ls_stencil(m, pbc, &stencil);
-    if (st) return st;
-    std::vector<V3> U3(n);                // zero initial velocity
-    std::vector<double> p(n, 0.0);
-    // initial_face_flux (simple.rs:724-755): internal faces from the
-    // interpolated (zero) velocity, boundary faces prescribed.
-    std::vector<double> flux = bflux;
-    for (int64_t f = 0; f < nf; ++f)
+    return FLURSYS_OK;
+}
+
+// correct_face_flux[_with_boundary] (simple.rs:412-496):
+// Phi = Phi* - d_f (p'_N - p'_P) on internal faces and, with pcbc, on fixed
+// correction faces with p'_b in place of p'_N.
+int32_t correct_face_flux(const FvMesh &m, const std::vector<double> &pf, const std::vector<double> &coef,
+                          const std::vector<double> &pc, const ScalarBc *pcbc, std::vector<double> *out) {
+    *out = pf;
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        double other;
+        if (m.neigh[f] >= 0) other = pc[m.neigh[f]];
+        else if (pcbc && pcbc->fixed[f]) other = pcbc->value[f];
+        else continue;
+        const double c = coef[f];
+        if (!std::isfinite(c) || c <= 0.0) return FLURSYS_ERR_INVALID_CONFIG;
+        (*out)[f] -= c * (other - pc[m.owner[f]]);
+        if (!std::isfinite((*out)[f])) return FLURSYS_ERR_INVALID_CONFIG;
+    }
+    return FLURSYS_OK;
+}
+
+// assemble_pressure_correction (simple.rs:518-581, reference cell: its row
+// and column are eliminated, rhs 0, diagonal 1) or, with pcbc,
+// assemble_pressure_correction_with_boundary (:583-643).
+int32_t assemble_pressure_correction(const FvMesh &m, const std::vector<double> &pf, const std::vector<double> &coef,
+                                     const ScalarBc *pcbc, int64_t reference_cell, OwnedCsr *P,
+                                     std::vector<double> *rhs_out) {
+    const int64_t n = m.ncells();
+    std::vector<double> rhs(n, 0.0);
+    std::vector<std::tuple<int64_t, int64_t, double>> pe;
+    pe.reserve(m.nfaces() * 4 + 1);
+    bool anchored = false;
+    if (!pcbc && (reference_cell < 0 || reference_cell >= n)) return FLURSYS_ERR_INVALID_CONFIG;
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        const double flux = pf[f];
+        if (!std::isfinite(flux)) return FLURSYS_ERR_INVALID_CONFIG;
+        const int64_t o = m.owner[f];
+        rhs[o] -= flux;
+        if (m.neigh[f] >= 0) {
+            const int64_t nb = m.neigh[f];
+            rhs[nb] += flux;
+            const double c = coef[f];
+            if (!std::isfinite(c) || c <= 0.0) return FLURSYS_ERR_INVALID_CONFIG;
+            pe.emplace_back(o, o, c);
+            pe.emplace_back(o, nb, -c);
+            pe.emplace_back(nb, o, -c);
+            pe.emplace_back(nb, nb, c);
+        } else if (pcbc && pcbc->fixed[f]) {
+            const double c = coef[f], val = pcbc->value[f];
+            if (!std::isfinite(c) || c <= 0.0 || !std::isfinite(val)) return FLURSYS_ERR_INVALID_CONFIG;
+            pe.emplace_back(o, o, c);
+            rhs[o] += c * val;
+            anchored = true;
+        }
+    }
+    if (pcbc) {
+        if (!anchored) return FLURSYS_ERR_INVALID_CONFIG;  // InvalidPressureReference
+    } else {
+        std::vector<std::tuple<int64_t, int64_t, double>> kept;
+        kept.reserve(pe.size() + 1);
+        for (const auto &t : pe)
+            if (std::get<0>(t) != reference_cell && std::get<1>(t) != reference_cell) kept.push_back(t);
+        rhs[reference_cell] = 0.0;
+        kept.emplace_back(reference_cell, reference_cell, 1.0);
+        pe.swap(kept);
+    }
+    int32_t st = build_csr(n, pe, P);
+    *rhs_out = std::move(rhs);
+    return st;
+}
+
+// continuity_rms (simple.rs:706-718): RMS of the integrated cell imbalance.
+double continuity_rms(const FvMesh &m, const std::vector<double> &flux) {
+    std::vector<double> div(m.ncells(), 0.0);
+    for (int64_t f = 0; f < m.nfaces(); ++f) {
+        div[m.owner[f]] += flux[f];
+        if (m.neigh[f] >= 0) div[m.neigh[f]] -= flux[f];
+    }
+    double s = 0.0;
+    for (double d : div) s += d * d;
+    return std::sqrt(s / double(m.ncells()));
+}
+
+// correct_cell_velocity_from_gradient (simple.rs:673-704): U = U* - rAU grad p'.
+int32_t correct_cell_velocity(const std::vector<V3> &pred, const std::vector<double> &rau,
+                              const std::vector<V3> &grad, std::vector<V3> *out) {
+    out->resize(pred.size());
+    for (size_t c = 0; c < pred.size(); ++c) {
+        if (!std::isfinite(rau[c]) || rau[c] <= 0.0) return FLURSYS_ERR_INVALID_CONFIG;  // InvalidMomentumDiagonal
+        const V3 v = pred[c] - grad[c] * rau[c];
+        if (!(std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z))) return FLURSYS_ERR_INVALID_CONFIG;
+        (*out)[c] = v;
+    }
+    return FLURSYS_OK;
+}
+
+// initial_face_flux (simple.rs:724-755): internal faces from the
+// geometrically interpolated cell velocity, boundary faces from wall_flux.
+std::vector<double> initial_face_flux(const FvMesh &m, const std::vector<V3> &U, const std::vector<double> &wall) {
+    std::vector<double> flux = wall;
+    for (int64_t f = 0; f < m.nfaces(); ++f)
         if (m.neigh[f] >= 0) {
             const double l = iweight(m, f);
-            flux[f] = dot(U3[m.owner[f]] * (1.0 - l) + U3[m.neigh[f]] * l, m.area[f]);
+            flux[f] = dot(U[m.owner[f]] * (1.0 - l) + U[m.neigh[f]] * l, m.area[f]);
         }
-    auto continuity = [&](const std::vector<double> &F) {
-        std::vector<double> div(n, 0.0);
-        for (int64_t f = 0; f < nf; ++f) {
-            div[m.owner[f]] += F[f];
-            if (m.neigh[f] >= 0) div[m.neigh[f]] -= F[f];
-        }
-        double s = 0.0;
-        for (double d : div) s += d * d;
-        return std::sqrt(s / double(n));
-    };
-    out->history.assign(1, continuity(flux));
+    return flux;
+}
+
+// Steady SIMPLE on a face-based mesh: boundary conditions per face for the
+// velocity components and the pressure (the least-squares stencil), and an
+// optional pressure-correction boundary (fixed faces anchor the system,
+// otherwise `reference_cell` does).
+struct SimpleSetup {
+    ScalarBc vel[3], pbc;
+    const ScalarBc *pcbc = nullptr;
+    int64_t reference_cell = 0;
+    double nu = 0.0, velocity_relaxation = 0.7, pressure_relaxation = 0.3;
+    int64_t max_outer = 1;
+    double continuity_tolerance = 0.0;
+    FlursysLinearSolverOptions momentum_solver{}, pressure_solver{};
+};
+
+// solve_simple (simple.rs:148-314). U, p, flux carry the initial state in
+// and the result out; `out` receives the history and the report.
+int32_t simple_solve(const FvMesh &m, const SimpleSetup &su, std::vector<V3> &U3, std::vector<double> &p,
+                     std::vector<double> &flux, SimpleOut *out) {
+    const int64_t n = m.ncells(), nf = m.nfaces();
+    if (su.max_outer < 1) return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(std::isfinite(su.pressure_relaxation) && su.pressure_relaxation > 0.0 && su.pressure_relaxation <= 1.0))
+        return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(std::isfinite(su.continuity_tolerance) && su.continuity_tolerance >= 0.0)) return FLURSYS_ERR_INVALID_CONFIG;
+    LsStencil stencil;
+    int32_t st = ls_stencil(m, su.pbc, &stencil);
+    if (st) return st;
+    out->history.assign(1, continuity_rms(m, flux));
     FlursysSimpleReport &rep = out->rep;
     rep = FlursysSimpleReport{};
     rep.initial_continuity_rms = out->history[0];
-    for (int64_t it = 1; it <= cfg.max_outer_iterations; ++it) {
+    rep.final_continuity_rms = out->history[0];
+    for (int64_t it = 1; it <= su.max_outer; ++it) {
         // pressure_gradient_source with unit density
         const std::vector<V3> gp = ls_gradient(stencil, p);
         OwnedCsr A[3];
@@ -2269,8 +2372,7 @@ int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
                 src[c] = -(k == 0 ? gp[c].x : k == 1 ? gp[c].y : gp[c].z);
                 cur[c] = k == 0 ? U3[c].x : k == 1 ? U3[c].y : U3[c].z;
             }
-            st = assemble_momentum(m, cfg.kinematic_viscosity, vel[k], flux, src, cur, cfg.velocity_relaxation, &A[k],
-                                   &b[k]);
+            st = assemble_momentum(m, su.nu, su.vel[k], flux, src, cur, su.velocity_relaxation, &A[k], &b[k]);
             if (st) return st;
         }
         // solve_momentum_velocity: BiCGSTAB per component from the current velocity
@@ -2278,33 +2380,24 @@ int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
         for (int k = 0; k < 3; ++k) {
             comp[k].resize(n);
             for (int64_t c = 0; c < n; ++c) comp[k][c] = k == 0 ? U3[c].x : k == 1 ? U3[c].y : U3[c].z;
-            st = solve_bicgstab(A[k].view(), b[k].data(), comp[k].data(), cfg.momentum_solver, &rep.momentum[k]);
+            st = solve_bicgstab(A[k].view(), b[k].data(), comp[k].data(), su.momentum_solver, &rep.momentum[k]);
             if (st) return st;
             if (rep.momentum[k].status != FLURSYS_LINEAR_CONVERGED) return FLURSYS_ERR_BREAKDOWN;
         }
         std::vector<V3> pred(n);
         for (int64_t c = 0; c < n; ++c) pred[c] = {comp[0][c], comp[1][c], comp[2][c]};
-        // momentum_inverse_diagonal of the x system
+        // momentum_inverse_diagonal of the x system (simple.rs:319-332)
         std::vector<double> rau(n);
         for (int64_t c = 0; c < n; ++c) {
             const double d = A[0].diag(c);
-            if (!(std::isfinite(d) && d > 0.0)) return FLURSYS_ERR_BREAKDOWN;
+            if (!(std::isfinite(d) && d > 0.0)) return FLURSYS_ERR_INVALID_CONFIG;
             rau[c] = 1.0 / d;
         }
-        // rhie_chow_predicted_flux (simple.rs:757-805) + fixed correction faces
-        std::vector<double> coef(nf, 0.0);
-        for (int64_t f = 0; f < nf; ++f) {
-            const int64_t o = m.owner[f];
-            if (m.neigh[f] >= 0) {
-                const int64_t nb = m.neigh[f];
-                const double l = iweight(m, f);
-                const V3 d = m.cc[nb] - m.cc[o];
-                coef[f] = (rau[o] * (1.0 - l) + rau[nb] * l) * dot(m.area[f], d) / dot(d, d);
-            } else if (pcbc.fixed[f]) {
-                const V3 d = m.fc[f] - m.cc[o];
-                coef[f] = rau[o] * dot(m.area[f], d) / dot(d, d);
-            }
-        }
+        // rhie_chow_predicted_flux (simple.rs:757-805), then the prescribed
+        // normal flux of fixed correction faces from the owner's predictor
+        std::vector<double> coef_int;
+        st = pressure_face_coefficients(m, rau, nullptr, &coef_int);
+        if (st) return st;
         std::vector<double> pf = flux;
         for (int64_t f = 0; f < nf; ++f) {
             const int64_t o = m.owner[f];
@@ -2313,59 +2406,98 @@ int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
                 const double l = iweight(m, f);
                 const V3 fu = pred[o] * (1.0 - l) + pred[nb] * l;
                 const V3 fr = gp[o] * rau[o] * (1.0 - l) + gp[nb] * rau[nb] * l;
-                pf[f] = dot(fu, m.area[f]) + dot(fr, m.area[f]) - coef[f] * (p[nb] - p[o]);
-            } else if (pcbc.fixed[f]) {
+                pf[f] = dot(fu, m.area[f]) + dot(fr, m.area[f]) - coef_int[f] * (p[nb] - p[o]);
+                if (!std::isfinite(pf[f])) return FLURSYS_ERR_INVALID_CONFIG;
+            } else if (su.pcbc && su.pcbc->fixed[f]) {
                 pf[f] = dot(pred[o], m.area[f]);
             }
         }
-        // assemble_pressure_correction_with_boundary (simple.rs:583-643)
-        std::vector<std::tuple<int64_t, int64_t, double>> pe;
-        std::vector<double> prhs(n, 0.0);
-        bool anchored = false;
-        for (int64_t f = 0; f < nf; ++f) {
-            const int64_t o = m.owner[f];
-            prhs[o] -= pf[f];
-            if (m.neigh[f] >= 0) {
-                const int64_t nb = m.neigh[f];
-                prhs[nb] += pf[f];
-                pe.emplace_back(o, o, coef[f]);
-                pe.emplace_back(o, nb, -coef[f]);
-                pe.emplace_back(nb, o, -coef[f]);
-                pe.emplace_back(nb, nb, coef[f]);
-            } else if (pcbc.fixed[f]) {
-                pe.emplace_back(o, o, coef[f]);
-                prhs[o] += coef[f] * pcbc.value[f];
-                anchored = true;
-            }
+        std::vector<double> coef;
+        if (su.pcbc) {
+            st = pressure_face_coefficients(m, rau, su.pcbc, &coef);
+            if (st) return st;
+        } else {
+            coef = coef_int;
         }
-        if (!anchored) return FLURSYS_ERR_INVALID_CONFIG;
         OwnedCsr P;
-        if ((st = build_csr(n, pe, &P))) return st;
+        std::vector<double> prhs;
+        if ((st = assemble_pressure_correction(m, pf, coef, su.pcbc, su.reference_cell, &P, &prhs))) return st;
+        // solve_pressure_correction (simple.rs:648-668): Jacobi-PCG from zero
         std::vector<double> pc(n, 0.0), inv;
         int64_t bad = -1;
         if ((st = jacobi(P.view(), inv, &bad))) return st;
-        st = solve_cg(P.view(), prhs.data(), pc.data(), cfg.pressure_solver, &inv, &rep.pressure);
+        st = solve_cg(P.view(), prhs.data(), pc.data(), su.pressure_solver, &inv, &rep.pressure);
         if (st) return st;
         if (rep.pressure.status != FLURSYS_LINEAR_CONVERGED) return FLURSYS_ERR_BREAKDOWN;
-        for (int64_t c = 0; c < n; ++c) p[c] += cfg.pressure_relaxation * pc[c];
+        for (int64_t c = 0; c < n; ++c) p[c] += su.pressure_relaxation * pc[c];
         const std::vector<V3> gpc = ls_gradient(stencil, pc);
-        for (int64_t c = 0; c < n; ++c) U3[c] = pred[c] - gpc[c] * rau[c];
-        // correct_face_flux_with_boundary (simple.rs:448-496)
-        flux = pf;
-        for (int64_t f = 0; f < nf; ++f) {
-            const int64_t o = m.owner[f];
-            if (m.neigh[f] >= 0) flux[f] -= coef[f] * (pc[m.neigh[f]] - pc[o]);
-            else if (pcbc.fixed[f]) flux[f] -= coef[f] * (pcbc.value[f] - pc[o]);
-        }
-        const double cont = continuity(flux);
+        if ((st = correct_cell_velocity(pred, rau, gpc, &U3))) return st;
+        if ((st = correct_face_flux(m, pf, coef, pc, su.pcbc, &flux))) return st;
+        const double cont = continuity_rms(m, flux);
         out->history.push_back(cont);
         rep.outer_iterations = it;
         rep.final_continuity_rms = cont;
-        if (cont <= cfg.continuity_tolerance) {
+        if (cont <= su.continuity_tolerance) {
             rep.converged = 1;
             break;
         }
     }
+    return FLURSYS_OK;
+}
+
+// solve_incompressible for the channel case (unstructured_incompressible.rs:
+// 106-212, 368-482): parabolic velocity inlet, fixed-pressure outlet, no-slip
+// walls, zero initial state.
+int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
+    const int64_t nx = cfg.nx, ny = cfg.ny;
+    if (nx < 2 || ny < 2) return FLURSYS_ERR_INVALID_CONFIG;
+    if (cfg.max_outer_iterations < 1) return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(cfg.pressure_relaxation > 0.0 && cfg.pressure_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
+    if (!(cfg.velocity_relaxation > 0.0 && cfg.velocity_relaxation <= 1.0)) return FLURSYS_ERR_INVALID_CONFIG;
+    const FvMesh m = channel_mesh(nx, ny, cfg.length, cfg.height);
+    const int64_t n = m.ncells(), nf = m.nfaces();
+    const double H = cfg.height, U = cfg.inlet_peak_velocity;
+    SimpleSetup su;
+    ScalarBc pcbc;
+    for (ScalarBc *b : {&su.vel[0], &su.vel[1], &su.vel[2], &su.pbc, &pcbc}) {
+        b->fixed.assign(nf, 0);
+        b->value.assign(nf, 0.0);
+    }
+    std::vector<double> bflux(nf, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+        if (m.patch[f] == kInternal) continue;
+        if (m.patch[f] == kOutlet) {
+            su.pbc.fixed[f] = 1;
+            su.pbc.value[f] = cfg.outlet_pressure;
+            pcbc.fixed[f] = 1;
+            pcbc.value[f] = 0.0;
+            continue;  // velocity zero gradient, no prescribed flux
+        }
+        V3 u{};
+        if (m.patch[f] == kInlet) {
+            const double y = m.fc[f].y;
+            u.x = U * 4.0 * y * (H - y) / (H * H);
+        }
+        su.vel[0].fixed[f] = su.vel[1].fixed[f] = su.vel[2].fixed[f] = 1;
+        su.vel[0].value[f] = u.x;
+        su.vel[1].value[f] = u.y;
+        su.vel[2].value[f] = u.z;
+        bflux[f] = dot(u, m.area[f]);
+    }
+    su.pcbc = &pcbc;
+    su.nu = cfg.kinematic_viscosity;
+    su.velocity_relaxation = cfg.velocity_relaxation;
+    su.pressure_relaxation = cfg.pressure_relaxation;
+    su.max_outer = cfg.max_outer_iterations;
+    su.continuity_tolerance = cfg.continuity_tolerance;
+    su.momentum_solver = cfg.momentum_solver;
+    su.pressure_solver = cfg.pressure_solver;
+    std::vector<V3> U3(n);  // zero initial velocity
+    std::vector<double> p(n, 0.0);
+    std::vector<double> flux = initial_face_flux(m, U3, bflux);
+    int32_t st = simple_solve(m, su, U3, p, flux, out);
+    if (st) return st;
+    FlursysSimpleReport &rep = out->rep;
     // backflow at the pressure outlet (unstructured_incompressible.rs:430-449)
     for (int64_t f = 0; f < nf; ++f)
         if (m.patch[f] == kOutlet && flux[f] < 0.0) return FLURSYS_ERR_INVALID_CONFIG;
@@ -2397,7 +2529,189 @@ int32_t simple_channel(const FlursysSimpleConfig &cfg, SimpleOut *out) {
     return FLURSYS_OK;
 }
 
+// A face-based mesh handed in by a caller (the test meshes of the reference's
+// own SIMPLE and momentum tests): cell centres and volumes, face owner,
+// neighbour (-1 on the boundary), area vector and centre.
+FvMesh mesh_from_arrays(int64_t nc, int64_t nf, const int64_t *owner, const int64_t *neigh, const double *area,
+                        const double *fc, const double *cc, const double *vol) {
+    FvMesh m;
+    m.cc.resize(nc);
+    m.vol.assign(vol, vol + nc);
+    m.cell_faces.resize(nc);
+    for (int64_t c = 0; c < nc; ++c) m.cc[c] = {cc[3 * c], cc[3 * c + 1], cc[3 * c + 2]};
+    for (int64_t f = 0; f < nf; ++f) {
+        m.owner.push_back(owner[f]);
+        m.neigh.push_back(neigh[f]);
+        m.area.push_back({area[3 * f], area[3 * f + 1], area[3 * f + 2]});
+        m.fc.push_back({fc[3 * f], fc[3 * f + 1], fc[3 * f + 2]});
+        m.patch.push_back(neigh[f] >= 0 ? kInternal : kBottom);
+        m.cell_faces[owner[f]].push_back(f);
+        if (neigh[f] >= 0) m.cell_faces[neigh[f]].push_back(f);
+    }
+    return m;
+}
+
+ScalarBc scalar_bc(int64_t nf, const int32_t *fixed, const double *value) {
+    ScalarBc b;
+    b.fixed.assign(nf, 0);
+    b.value.assign(nf, 0.0);
+    for (int64_t f = 0; f < nf; ++f) {
+        b.fixed[f] = fixed ? fixed[f] : 0;
+        b.value[f] = value ? value[f] : 0.0;
+    }
+    return b;
+}
+
+void export_csr(const OwnedCsr &P, int64_t *ro, int64_t *ci, double *v, int64_t cap, int64_t *nnz) {
+    *nnz = (int64_t)P.v.size();
+    if (ro) std::copy(P.ro.begin(), P.ro.end(), ro);
+    for (int64_t k = 0; k < std::min<int64_t>(cap, *nnz); ++k) {
+        if (ci) ci[k] = P.ci[k];
+        if (v) v[k] = P.v[k];
+    }
+}
+
 }  // namespace
+
+// Face-based entry points (see flursys_oracle.h). Meshes are passed as
+// (nc, nf, owner, neigh, area[3 nf], face centre[3 nf], cell centre[3 nc], volume[nc]).
+#define ORC_MESH_ARGS int64_t nc, int64_t nf, const int64_t *owner, const int64_t *neigh, const double *area, \
+                      const double *fc, const double *cc, const double *vol
+#define ORC_MESH mesh_from_arrays(nc, nf, owner, neigh, area, fc, cc, vol)
+
+extern "C" int32_t orc_fv_pressure_face_coefficients(ORC_MESH_ARGS, const double *rau, const int32_t *pc_fixed,
+                                                     const double *pc_value, double *coef_out) {
+    const FvMesh m = ORC_MESH;
+    std::vector<double> r(rau, rau + nc), coef;
+    const ScalarBc pcbc = scalar_bc(nf, pc_fixed, pc_value);
+    const int32_t st = pressure_face_coefficients(m, r, pc_fixed ? &pcbc : nullptr, &coef);
+    if (!st) std::copy(coef.begin(), coef.end(), coef_out);
+    return st;
+}
+
+extern "C" int32_t orc_fv_correct_face_flux(ORC_MESH_ARGS, const double *predicted, const double *coef,
+                                            const double *correction, const int32_t *pc_fixed,
+                                            const double *pc_value, double *out) {
+    const FvMesh m = ORC_MESH;
+    const ScalarBc pcbc = scalar_bc(nf, pc_fixed, pc_value);
+    std::vector<double> res;
+    const int32_t st = correct_face_flux(m, std::vector<double>(predicted, predicted + nf),
+                                         std::vector<double>(coef, coef + nf),
+                                         std::vector<double>(correction, correction + nc),
+                                         pc_fixed ? &pcbc : nullptr, &res);
+    if (!st) std::copy(res.begin(), res.end(), out);
+    return st;
+}
+
+extern "C" int32_t orc_fv_assemble_pressure_correction(ORC_MESH_ARGS, const double *predicted, const double *coef,
+                                                       const int32_t *pc_fixed, const double *pc_value,
+                                                       int64_t reference_cell, int64_t *ro, int64_t *ci, double *v,
+                                                       int64_t cap, int64_t *nnz, double *rhs) {
+    const FvMesh m = ORC_MESH;
+    const ScalarBc pcbc = scalar_bc(nf, pc_fixed, pc_value);
+    OwnedCsr P;
+    std::vector<double> b;
+    const int32_t st = assemble_pressure_correction(m, std::vector<double>(predicted, predicted + nf),
+                                                    std::vector<double>(coef, coef + nf),
+                                                    pc_fixed ? &pcbc : nullptr, reference_cell, &P, &b);
+    if (st) return st;
+    export_csr(P, ro, ci, v, cap, nnz);
+    std::copy(b.begin(), b.end(), rhs);
+    return FLURSYS_OK;
+}
+
+extern "C" int32_t orc_fv_continuity_rms(ORC_MESH_ARGS, const double *flux, double *out) {
+    const FvMesh m = ORC_MESH;
+    *out = continuity_rms(m, std::vector<double>(flux, flux + nf));
+    return std::isfinite(*out) ? FLURSYS_OK : FLURSYS_ERR_INVALID_CONFIG;
+}
+
+extern "C" int32_t orc_fv_correct_cell_velocity(int64_t nc, const double *predictor, const double *rau,
+                                                const double *grad, double *out) {
+    std::vector<V3> pr(nc), g(nc), res;
+    for (int64_t c = 0; c < nc; ++c) {
+        pr[c] = {predictor[3 * c], predictor[3 * c + 1], predictor[3 * c + 2]};
+        g[c] = {grad[3 * c], grad[3 * c + 1], grad[3 * c + 2]};
+    }
+    const int32_t st = correct_cell_velocity(pr, std::vector<double>(rau, rau + nc), g, &res);
+    if (st) return st;
+    for (int64_t c = 0; c < nc; ++c) {
+        out[3 * c] = res[c].x;
+        out[3 * c + 1] = res[c].y;
+        out[3 * c + 2] = res[c].z;
+    }
+    return FLURSYS_OK;
+}
+
+extern "C" int32_t orc_fv_initial_face_flux(ORC_MESH_ARGS, const double *velocity, const double *wall_flux,
+                                            double *out) {
+    const FvMesh m = ORC_MESH;
+    std::vector<V3> U(nc);
+    for (int64_t c = 0; c < nc; ++c) U[c] = {velocity[3 * c], velocity[3 * c + 1], velocity[3 * c + 2]};
+    const std::vector<double> f = initial_face_flux(m, U, std::vector<double>(wall_flux, wall_flux + nf));
+    std::copy(f.begin(), f.end(), out);
+    return FLURSYS_OK;
+}
+
+extern "C" int32_t orc_fv_assemble_momentum(ORC_MESH_ARGS, double nu, const int32_t *fixed, const double *value,
+                                            const double *flux, const double *source, const double *current,
+                                            double alpha, int64_t *ro, int64_t *ci, double *v, int64_t cap,
+                                            int64_t *nnz, double *rhs) {
+    const FvMesh m = ORC_MESH;
+    const ScalarBc bc = scalar_bc(nf, fixed, value);
+    OwnedCsr A;
+    std::vector<double> b;
+    const int32_t st = assemble_momentum(m, nu, bc, std::vector<double>(flux, flux + nf),
+                                         source ? std::vector<double>(source, source + nc) : std::vector<double>(nc, 0.0),
+                                         current ? std::vector<double>(current, current + nc) : std::vector<double>(nc, 0.0),
+                                         alpha, &A, &b);
+    if (st) return st;
+    export_csr(A, ro, ci, v, cap, nnz);
+    std::copy(b.begin(), b.end(), rhs);
+    return FLURSYS_OK;
+}
+
+extern "C" int32_t orc_fv_simple(ORC_MESH_ARGS, const int32_t *vel_fixed, const double *vel_value,
+                                 const int32_t *p_fixed, const double *p_value, const int32_t *pc_fixed,
+                                 const double *pc_value, int64_t reference_cell, double nu,
+                                 double velocity_relaxation, double pressure_relaxation, int64_t max_outer,
+                                 double continuity_tolerance, const FlursysLinearSolverOptions *momentum_solver,
+                                 const FlursysLinearSolverOptions *pressure_solver, double *velocity,
+                                 double *pressure, double *face_flux, double *history, FlursysSimpleReport *report) {
+    const FvMesh m = ORC_MESH;
+    SimpleSetup su;
+    for (int k = 0; k < 3; ++k) {
+        su.vel[k] = scalar_bc(nf, vel_fixed, nullptr);
+        for (int64_t f = 0; f < nf; ++f) su.vel[k].value[f] = vel_value[3 * f + k];
+    }
+    su.pbc = scalar_bc(nf, p_fixed, p_value);
+    const ScalarBc pcbc = scalar_bc(nf, pc_fixed, pc_value);
+    su.pcbc = pc_fixed ? &pcbc : nullptr;
+    su.reference_cell = reference_cell;
+    su.nu = nu;
+    su.velocity_relaxation = velocity_relaxation;
+    su.pressure_relaxation = pressure_relaxation;
+    su.max_outer = max_outer;
+    su.continuity_tolerance = continuity_tolerance;
+    su.momentum_solver = *momentum_solver;
+    su.pressure_solver = *pressure_solver;
+    std::vector<V3> U(nc);
+    for (int64_t c = 0; c < nc; ++c) U[c] = {velocity[3 * c], velocity[3 * c + 1], velocity[3 * c + 2]};
+    std::vector<double> p(pressure, pressure + nc), flux(face_flux, face_flux + nf);
+    SimpleOut out;
+    const int32_t st = simple_solve(m, su, U, p, flux, &out);
+    if (st) return st;
+    for (int64_t c = 0; c < nc; ++c) {
+        velocity[3 * c] = U[c].x;
+        velocity[3 * c + 1] = U[c].y;
+        velocity[3 * c + 2] = U[c].z;
+    }
+    std::copy(p.begin(), p.end(), pressure);
+    std::copy(flux.begin(), flux.end(), face_flux);
+    if (history) std::copy(out.history.begin(), out.history.end(), history);
+    if (report) *report = out.rep;
+    return FLURSYS_OK;
+}
 
 extern "C" int32_t orc_simple_channel(const FlursysSimpleConfig *cfg, double *velocity_x, double *velocity_y,
                                       double *pressure, double *face_flux, double *continuity_history,

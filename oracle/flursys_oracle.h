@@ -91,6 +91,50 @@ int32_t orc_simple_channel(const FlursysSimpleConfig *cfg, double *velocity_x, d
                            double *pressure, double *face_flux, double *continuity_history,
                            FlursysSimpleReport *report);
 
+/* ---- The SIMPLE building blocks on a caller-supplied face-based mesh ----
+ * (the reference's own unit-test meshes: two cells, closed cavities,
+ * channels). A mesh is (nc, nf, owner[nf], neigh[nf] (-1 on the boundary),
+ * area vector[3 nf], face centre[3 nf], cell centre[3 nc], volume[nc]).
+ * Boundary conditions are per face: fixed (1) or zero gradient (0) with a
+ * value; a NULL pc_fixed means no pressure-correction boundary (the
+ * reference-cell form). CSR outputs hold nc+1 offsets and up to `cap`
+ * entries, *nnz receives the count. */
+#define ORC_FV_MESH int64_t nc, int64_t nf, const int64_t *owner, const int64_t *neigh, const double *area, \
+                    const double *fc, const double *cc, const double *vol
+/* pressure_face_coefficients[_with_boundary] (simple.rs:342-410) */
+int32_t orc_fv_pressure_face_coefficients(ORC_FV_MESH, const double *rau, const int32_t *pc_fixed,
+                                          const double *pc_value, double *coef_out);
+/* correct_face_flux[_with_boundary] (simple.rs:412-496) */
+int32_t orc_fv_correct_face_flux(ORC_FV_MESH, const double *predicted, const double *coef,
+                                 const double *correction, const int32_t *pc_fixed, const double *pc_value,
+                                 double *out);
+/* assemble_pressure_correction[_with_boundary] (simple.rs:518-643) */
+int32_t orc_fv_assemble_pressure_correction(ORC_FV_MESH, const double *predicted, const double *coef,
+                                            const int32_t *pc_fixed, const double *pc_value,
+                                            int64_t reference_cell, int64_t *ro, int64_t *ci, double *v,
+                                            int64_t cap, int64_t *nnz, double *rhs);
+/* continuity_rms (simple.rs:706-718) */
+int32_t orc_fv_continuity_rms(ORC_FV_MESH, const double *flux, double *out);
+/* correct_cell_velocity_from_gradient (simple.rs:673-704); vectors as xyz triples */
+int32_t orc_fv_correct_cell_velocity(int64_t nc, const double *predictor, const double *rau, const double *grad,
+                                     double *out);
+/* initial_face_flux (simple.rs:724-755) */
+int32_t orc_fv_initial_face_flux(ORC_FV_MESH, const double *velocity, const double *wall_flux, double *out);
+/* assemble_momentum_component (momentum.rs:180-341), steady, upwind, two-point diffusion */
+int32_t orc_fv_assemble_momentum(ORC_FV_MESH, double nu, const int32_t *fixed, const double *value,
+                                 const double *flux, const double *source, const double *current, double alpha,
+                                 int64_t *ro, int64_t *ci, double *v, int64_t cap, int64_t *nnz, double *rhs);
+/* solve_simple (simple.rs:148-314); velocity (3 nc), pressure, face_flux
+ * carry the initial state in and the result out; history holds up to
+ * max_outer + 1 continuity values. */
+int32_t orc_fv_simple(ORC_FV_MESH, const int32_t *vel_fixed, const double *vel_value, const int32_t *p_fixed,
+                      const double *p_value, const int32_t *pc_fixed, const double *pc_value,
+                      int64_t reference_cell, double nu, double velocity_relaxation, double pressure_relaxation,
+                      int64_t max_outer, double continuity_tolerance,
+                      const FlursysLinearSolverOptions *momentum_solver,
+                      const FlursysLinearSolverOptions *pressure_solver, double *velocity, double *pressure,
+                      double *face_flux, double *history, FlursysSimpleReport *report);
+
 #ifdef __cplusplus
 }
 #endif
