@@ -277,6 +277,9 @@ SIGNATURES = {
     "flursys_cuda_destroy": (C.c_int32, [_P]),
     "flursys_cuda_global_error": (C.c_int32, [C.c_char_p, C.c_size_t]),
     "flursys_cuda_debug_inject_barrier_fault": (C.c_int32, [C.c_int32]),
+    "flursys_cuda_snapshot_begin": (C.c_int32, [_P, C.POINTER(C.c_int32), C.c_int32, C.POINTER(_D),
+                                                C.POINTER(C.c_size_t)]),
+    "flursys_cuda_snapshot_wait": (C.c_int32, [_P]),
     "flursys_cuda_csr_cg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,
                                         C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport)]),
     "flursys_cuda_csr_pcg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,

@@ -376,6 +376,51 @@ int32_t flursys_cuda_download(FlursysCudaHandle *h, int32_t id, double *host, si
     return FLURSYS_OK;
 }
 
+int32_t flursys_cuda_snapshot_begin(FlursysCudaHandle *h, const int32_t *ids, int32_t count, double *const *host,
+                                    const size_t *sizes) {
+    if (!h || (count > 0 && (!ids || !host || !sizes))) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (count < 0 || count > 16) { h->err = "a snapshot holds 1 to 16 fields"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (h->snap_pending) { h->err = "a snapshot is already pending on this handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess && !h->snap_stream) e = cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !h->snap_taken) e = cudaEventCreateWithFlags(&h->snap_taken, cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->snap_done) e = cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "snapshot set-up");
+    for (int32_t i = 0; i < count; ++i) {
+        double *p = nullptr;
+        size_t fn = 0;
+        if (!host[i] || !field_ptr(h, ids[i], &p, &fn)) { h->err = "unknown field id for this handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+        if (fn != sizes[i]) { h->err = "field size mismatch"; return FLURSYS_ERR_DIMENSION_MISMATCH; }
+        if (h->snap_n[i] < fn) {
+            cudaFree(h->snap_buf[i]);
+            h->snap_buf[i] = nullptr;
+            h->snap_n[i] = 0;
+            e = cudaMalloc(&h->snap_buf[i], fn * sizeof(double));
+            if (e != cudaSuccess) return set_cuda_error(&h->err, e, "snapshot buffer");
+            h->snap_n[i] = fn;
+        }
+        e = cudaMemcpyAsync(h->snap_buf[i], p, fn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) return set_cuda_error(&h->err, e, "snapshot copy");
+    }
+    e = cudaEventRecord(h->snap_taken, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->snap_stream, h->snap_taken, 0);
+    for (int32_t i = 0; i < count && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(host[i], h->snap_buf[i], sizes[i] * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(h->snap_done, h->snap_stream);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "snapshot drain");
+    h->snap_pending = true;
+    return FLURSYS_OK;
+}
+
+int32_t flursys_cuda_snapshot_wait(FlursysCudaHandle *h) {
+    if (!h) { g_error = "null handle"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (!h->snap_pending) return FLURSYS_OK;
+    h->snap_pending = false;
+    const cudaError_t e = cudaEventSynchronize(h->snap_done);
+    if (e != cudaSuccess) return set_cuda_error(&h->err, e, "snapshot wait");
+    return FLURSYS_OK;
+}
+
 int32_t flursys_cuda_upload(FlursysCudaHandle *h, int32_t id, const double *host, size_t n) {
     if (!h || !host) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
     double *p = nullptr;
@@ -418,6 +463,11 @@ int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t si
 int32_t flursys_cuda_destroy(FlursysCudaHandle *h) {
     if (!h) return FLURSYS_OK;
     cudaSetDevice(h->device);
+    if (h->snap_pending) cudaEventSynchronize(h->snap_done);
+    for (double *b : h->snap_buf) cudaFree(b);
+    if (h->snap_taken) cudaEventDestroy(h->snap_taken);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
+    if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
     handle_free(h);
     delete h;
     return FLURSYS_OK;

@@ -60,6 +60,13 @@ struct FlursysCudaHandle {
     // 3D learned-preconditioner FCG (pressure_solver == FLURSYS_PRESSURE_FCG)
     FlursysFcgNet *fcg_net = nullptr;
     FlursysFcgReport fcg_report{};
+    // asynchronous snapshots: device copies of the fields, drained to the
+    // caller's host buffers on a copy stream while later steps run
+    double *snap_buf[16] = {};
+    size_t snap_n[16] = {};
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
 };
 
 namespace flursys {

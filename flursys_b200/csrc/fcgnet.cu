@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "fcgnet.cuh"
@@ -922,6 +923,211 @@ __global__ void adam_kernel(float *w, const float *g, float *m, float *v, long l
 
 int grid_1d(long long n, int per = 256) { return (int)std::max<long long>(1, std::min<long long>((n + per - 1) / per, 148LL * 16)); }
 
+// ---------------------------------------------------------------------------
+// conv_umma<CIN, COUT, MODE>: the same 3x3x3 convolution on the 5th-generation
+// tensor cores. One CTA (4 warps) owns an 8 (x) x 16 (y) column of voxels
+// and marches it through kz planes. Per output plane one thread issues
+// 27 x CIN/16 tcgen05.mma (kind::f16, M = 128 voxels, N = COUT, K = 16,
+// BF16 operands from shared memory, FP32 accumulator in tensor memory),
+// commits them to an mbarrier, and the four warps read the accumulator back
+// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. voxel rows
+// 4w..4w+3) and store it as BF16. Two accumulator buffers alternate between
+// planes; the MMAs of plane z overlap the staging of input plane z+2.
+//
+// Operands are in the K-major no-swizzle core-matrix layout (8 rows x 16 B):
+//   input ring, 4 planes: [plane][k8][cell] with cell = cy*10 + cx of the
+//     10 x 18 halo tile, 16 B = 8 channels per entry. For tap (dy, dx) the
+//     A operand of the 128 voxels (row m = 8 y + x) starts at cell
+//     dy*10 + dx; 8-row groups (one voxel row) are 10 cells apart (SBO 160 B)
+//     and the two 8-channel halves of K = 16 one slice apart (LBO 2880 B).
+//   weights: [tap][k8][co] (16 B entries): B is COUT x 16 per MMA, 8-row
+//     groups 128 B apart (SBO), K halves COUT * 16 B apart (LBO).
+// Every wait is bounded; a CTA whose accumulator never arrives writes NaN
+// to its outputs (the solver then sees a non-finite residual and falls back)
+// and still frees its tensor memory.
+// ---------------------------------------------------------------------------
+constexpr int kUX = 8, kUY = 16;                 // voxels per CTA column (M = 128)
+constexpr int kUHX = kUX + 2, kUHY = kUY + 2;    // halo tile 10 x 18
+constexpr int kUCells = kUHX * kUHY;             // 180
+constexpr int kUThreads = 128;
+
+template <int CIN, int COUT>
+struct UmmaConv {
+    static constexpr int kSlot = (CIN / 8) * kUCells * 16;       // bytes of one staged plane
+    static constexpr int kWBytes = 27 * (CIN / 8) * COUT * 16;   // all taps' weights
+    static constexpr int kSmem = 4 * kSlot + kWBytes;
+    static constexpr int kTmemCols = 2 * COUT < 32 ? 32 : 2 * COUT;  // two accumulator buffers
+};
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version (bits 46-48 = 0b001); base offset 0, no swizzle
+    return d;
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity) {
+    for (long long spin = 0; spin < (1LL << 26); ++spin) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Reads N consecutive FP32 accumulator columns of this thread's TMEM lane.
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[N]);
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[N]) {
+    static_assert(N % 16 == 0, "16 columns per load");
+#pragma unroll
+    for (int c = 0; c < N; c += 16) {
+        float t[16];
+        tmem_ld<16>(taddr + c, t);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[c + i] = t[i];
+    }
+}
+
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *__restrict__ W, uint16_t *out,
+                                                       int nx, int ny, int nz, int kz) {
+    using G = UmmaConv<CIN, COUT>;
+    extern __shared__ __align__(1024) uint8_t usmem[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_mbar[2];
+    constexpr int K8 = CIN / 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kUX, y0 = blockIdx.y * kUY, z0 = blockIdx.z * kz;
+    const int z1 = min(z0 + kz, nz);
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(usmem);
+    uint8_t *ring = usmem;
+    uint8_t *wts = usmem + 4 * G::kSlot;
+    // weights [tap][k8][co] from W[co][tap][ci]
+    for (int idx = tid; idx < 27 * K8 * COUT; idx += kUThreads) {
+        const int co = idx % COUT, rest = idx / COUT;
+        const int k8 = rest % K8, t27 = rest / K8;
+        const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + t27) * CIN + k8 * 8);
+        *reinterpret_cast<uint4 *>(wts + ((t27 * K8 + k8) * COUT + co) * 16) = q;
+    }
+    auto stage = [&](int p) {  // input plane p into its ring slot, channels fastest
+        uint8_t *slot = ring + ((p + 4) & 3) * G::kSlot;
+        for (int idx = tid; idx < kUCells * K8; idx += kUThreads) {
+            const int k8 = idx % K8, cell = idx / K8;
+            const int cx = cell % kUHX, cy = cell / kUHX;
+            const uint4 q = load8<CIN, MODE>(src, x0 - 1 + cx, y0 - 1 + cy, p, nx, ny, nz, k8);
+            *reinterpret_cast<uint4 *>(slot + (k8 * kUCells + cell) * 16) = q;
+        }
+    };
+    stage(z0 - 1);
+    stage(z0);
+    if (z0 + 1 < z1 + 1) stage(z0 + 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst),
+                     "n"(G::kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const uint32_t mb0 = (uint32_t)__cvta_generic_to_shared(&s_mbar[0]);
+    const uint32_t mb1 = (uint32_t)__cvta_generic_to_shared(&s_mbar[1]);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+    // K-major, N = COUT, M = 128
+    constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((128u >> 4) << 24);
+    const int m = warp * 32 + lane;  // this thread's voxel row of the accumulator
+    const int vx = x0 + (m % kUX), vy = y0 + m / kUX;
+    bool ok = true;
+    for (int z = z0; z < z1; ++z) {
+        const int b = (z - z0) & 1;
+        const uint32_t dbuf = tmem + (uint32_t)(b * COUT);
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t acc = 0;
+#pragma unroll 1
+            for (int dz = 0; dz < 3; ++dz) {
+                const uint32_t slot = sbase + (uint32_t)(((z + dz - 1 + 4) & 3) * G::kSlot);
+#pragma unroll 1
+                for (int t9 = 0; t9 < 9; ++t9) {
+                    const int dy = t9 / 3, dx = t9 % 3, tap = dz * 9 + t9;
+#pragma unroll
+                    for (int kc = 0; kc < CIN / 16; ++kc) {
+                        const uint32_t a = slot + (uint32_t)(((dy * kUHX + dx) + 2 * kc * kUCells) * 16);
+                        const uint32_t w = sbase + 4 * G::kSlot + (uint32_t)((tap * K8 + 2 * kc) * COUT * 16);
+                        umma_f16(dbuf, umma_desc(a, kUCells * 16, kUHX * 16), umma_desc(w, COUT * 16, 128), kIdesc,
+                                 acc);
+                        acc = 1;
+                    }
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             b ? mb1 : mb0)
+                         : "memory");
+        }
+        if (z + 2 <= z1) stage(z + 2);  // overlaps the MMAs of plane z
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const bool arrived = mbar_wait_bounded(b ? mb1 : mb0, (uint32_t)(((z - z0) >> 1) & 1));
+        ok = ok && arrived;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float acc[COUT];
+        if (arrived) {
+            tmem_ld<COUT>(dbuf + ((uint32_t)(warp * 32) << 16), acc);
+        } else {
+#pragma unroll
+            for (int c = 0; c < COUT; ++c) acc[c] = __int_as_float(0x7fc00000);
+        }
+        if (vx < nx && vy < ny) {
+            uint16_t *o = out + (((long long)z * ny + vy) * nx + vx) * COUT;
+#pragma unroll
+            for (int c = 0; c < COUT; c += 8) {
+                uint4 q;
+                uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) h[e] = f2bf(acc[c + e]);
+                *reinterpret_cast<uint4 *>(o + c) = q;
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (!__syncthreads_and(ok)) break;  // a lost accumulator: stop issuing, free the tensor memory
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(G::kTmemCols));
+}
+
 // Planes per block of conv_tc_z: the largest of 8, 4, 2 that still gives
 // about two blocks per SM, else 1.
 int conv_planes(int nx, int ny, int nz) {
@@ -958,6 +1164,32 @@ cudaError_t launch_conv(const Src &s, const uint16_t *W, uint16_t *out, int nx, 
     }
     dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
     conv_tc<CIN, COUT, MODE><<<grid, kConvThreads, smem, st>>>(s, W, out, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+// The convolution of inference: on the 5th-generation tensor cores
+// (conv_umma) when FLURSYS_FCG_UMMA=1, else the mma.sync kernels.
+bool umma_enabled() {
+    const char *env = std::getenv("FLURSYS_FCG_UMMA");
+    return env && env[0] == '1';
+}
+
+template <int CIN, int COUT, int MODE>
+cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
+    using G = UmmaConv<CIN, COUT>;
+    if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             G::kSmem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const long long cols = (long long)((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY);
+    int kz = 1;  // planes per CTA: about four CTAs per SM, at least 4 planes where the grid allows
+    while (kz < nz && cols * ((nz + 2 * kz - 1) / (2 * kz)) >= 4 * 148) kz *= 2;
+    dim3 grid((nx + kUX - 1) / kUX, (ny + kUY - 1) / kUY, (nz + kz - 1) / kz);
+    conv_umma<CIN, COUT, MODE><<<grid, kUThreads, G::kSmem, st>>>(s, W, out, nx, ny, nz, kz);
     return cudaGetLastError();
 }
 
@@ -1122,11 +1354,11 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     }
     e = cudaGetLastError();
     const uint16_t *W = w.fwd;
-    if (e == cudaSuccess) e = launch_conv<16, 32, kPlain>(Src{ws.x2, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
-    if (e == cudaSuccess) e = launch_conv<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
-    if (e == cudaSuccess) e = launch_conv<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
-    if (e == cudaSuccess) e = launch_conv<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
-    if (e == cudaSuccess) e = launch_conv<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv_fwd<16, 32, kPlain>(Src{ws.x2, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
+    if (e == cudaSuccess) e = launch_conv_fwd<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv_fwd<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
+    if (e == cudaSuccess) e = launch_conv_fwd<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
+    if (e == cudaSuccess) e = launch_conv_fwd<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
     if (e == cudaSuccess) {
         dim3 grid((n2x + kOutCX - 1) / kOutCX, (n2y + kOutCY - 1) / kOutCY, n2z);
         net_out_interior<<<grid, kOutCX * kOutCY, 0, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz, w.out_params);

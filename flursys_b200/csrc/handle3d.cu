@@ -185,7 +185,7 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
         m.residual = q.residual;
         m.true_l2 = q.true_l2;
         m.initial_l2 = q.initial_l2;
-        m.device_error = 0;
+        m.device_error = q.device_error;
     }
     const PcgResultDev &r = *h->pcg.h_result;
     status = pcg_result_status(r, &h->err);

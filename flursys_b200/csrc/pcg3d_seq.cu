@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "pcg3d.cuh"
 #include "pcg3d_seq.cuh"
+#include "pcg3d_res.cuh"
 #include "tma.cuh"
 
 namespace flursys {
@@ -1553,10 +1554,19 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     plan.host_args = new SeqArgs(a);
     const char *v = std::getenv("FLURSYS_PCG_VARIANT");
     if (v && std::strcmp(v, "host") == 0) plan.host_iterations = 1;
+    // MIXED solves whose tiles fit one per SM run chip-resident (one
+    // cooperative launch per solve; FLURSYS_PCG_RESIDENT=0 keeps the graph).
+    if (e == cudaSuccess && precision == FLURSYS_PRECISION_MIXED && !a.cg1 && plan.host_iterations == 0) {
+        auto *rp = new Pcg3dResPlan();
+        if (pcg3d_res_plan(*rp, args, device)) plan.resident = rp;
+        else delete rp;
+        cudaGetLastError();  // a declined plan leaves no sticky error behind
+    }
     return e;
 }
 
 cudaError_t pcg3d_seq_launch(const Pcg3dSeqPlan &plan, cudaStream_t stream) {
+    if (plan.resident) return pcg3d_res_launch(*plan.resident, plan.state, stream);
     if (plan.host_iterations > 0) return pcg3d_seq_run_host(plan, stream);
     return cudaGraphLaunch(plan.exec, stream);
 }
@@ -1622,6 +1632,10 @@ cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t st) {
 }
 
 void pcg3d_seq_destroy(Pcg3dSeqPlan &plan) {
+    if (plan.resident) {
+        pcg3d_res_destroy(*plan.resident);
+        delete plan.resident;
+    }
     delete static_cast<SeqArgs *>(plan.host_args);
     if (plan.exec) cudaGraphExecDestroy(plan.exec);
     if (plan.graph) cudaGraphDestroy(plan.graph);

@@ -14,10 +14,13 @@ struct CgSeqState {
     long long iterations;
     int first, done, status, error, replace, pending_conv;
     unsigned counter;  // last-block arrival counter
-    unsigned pad;
+    unsigned device_error;  // DeviceError bits (a grid barrier of the resident solve gave up)
 };
 
+struct Pcg3dResPlan;
+
 struct Pcg3dSeqPlan {
+    Pcg3dResPlan *resident = nullptr;  // the chip-resident solve replaces the graph when it fits
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double *partials = nullptr;

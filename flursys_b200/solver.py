@@ -21,6 +21,8 @@ from typing import Optional
 import numpy as np
 
 from . import _abi
+
+_D = C.POINTER(C.c_double)
 from .cases import Case, CavityCase, SolverBoundaryOverrides
 
 
@@ -170,6 +172,11 @@ class _Handle:
         a = np.ascontiguousarray(values, dtype=np.float64).ravel()
         _check(self.lib, self.h, self.lib.flursys_cuda_upload(self.h, fid, _abi.dptr(a), a.size))
 
+    def snapshot_begin(self, fids) -> "Snapshot":
+        """Starts an asynchronous copy of the fields `fids` into page-locked
+        host arrays; the next steps run while it drains (Snapshot.wait())."""
+        return Snapshot(self, list(fids))
+
     def set_stream(self, stream_ptr: int) -> None:
         _check(self.lib, self.h, self.lib.flursys_cuda_set_stream(self.h, C.c_void_p(stream_ptr)))
 
@@ -178,6 +185,28 @@ class _Handle:
         t = C.c_double()
         self.lib.flursys_cuda_state(self.h, C.byref(s), C.byref(t))
         return s.value, t.value
+
+
+class Snapshot:
+    """A field snapshot draining on the handle's copy stream
+    (flursys_cuda_snapshot_begin / _wait). wait() returns {field id: array}."""
+
+    def __init__(self, handle: "_Handle", fids):
+        import torch  # page-locked host memory
+        self._h = handle
+        self.fids = fids
+        self._host = [torch.empty(handle.field_size(f), dtype=torch.float64).pin_memory() for f in fids]
+        ids = (C.c_int32 * len(fids))(*fids)
+        ptrs = (_D * len(fids))(*[C.cast(t.data_ptr(), _D) for t in self._host])
+        sizes = (C.c_size_t * len(fids))(*[t.numel() for t in self._host])
+        _check(handle.lib, handle.h, handle.lib.flursys_cuda_snapshot_begin(handle.h, ids, len(fids), ptrs, sizes))
+        self._done = False
+
+    def wait(self) -> dict:
+        if not self._done:
+            _check(self._h.lib, self._h.h, self._h.lib.flursys_cuda_snapshot_wait(self._h.h))
+            self._done = True
+        return {f: t.numpy() for f, t in zip(self.fids, self._host)}
 
 
 class LidDrivenCavity3DSolver:
@@ -432,20 +461,54 @@ class IncompressibleSolver:
         self.last_report = self._h.step(1)
         return SolverStep.from_report(self.last_report)
 
-    def run(self) -> RunSummary:
-        """run() (:368-499) without file output: steps until max_steps, t_end or steady."""
+    def run(self, write_output: bool = False) -> RunSummary:
+        """run() (:368-499): steps until max_steps, t_end or steady. With
+        `write_output`, every `output_every` steps (and at the end) a field
+        snapshot is taken on the device and drained to the host while the
+        next steps run; a writer thread turns it into frames/field_NNNNN.vtk
+        and field.csv / field.vtk of the last one (output.rs:31-125)."""
+        from concurrent.futures import ThreadPoolExecutor
         started = time.perf_counter()
         step, _ = self._h.state()
         rep = None
         converged = False
+        every = max(1, int(self.cfg.output_every)) if write_output else 1 << 20
+        pool = ThreadPoolExecutor(max_workers=1) if write_output else None
+        pending = []
+        if write_output:
+            os.makedirs(os.path.join(self.cfg.output_dir, "frames"), exist_ok=True)
+
+        def emit(pfu, frame):
+            fu = pfu.wait()
+            from . import output
+            output.write_legacy_vtk(os.path.join(self.cfg.output_dir, "frames", f"field_{frame:05d}.vtk"),
+                                    self.cfg.case.name(), self, fu)
+            return fu
+
+        frame = 0
         while step < self.cfg.max_steps:
-            rep = self._h.step(min(self.cfg.max_steps - step, 1 << 20))
+            chunk = min(self.cfg.max_steps - step, every - step % every)
+            rep = self._h.step(chunk)
             step = int(rep.iteration)
+            done = bool(rep.converged) or bool(rep.reached_end_time) or step >= self.cfg.max_steps
+            if write_output and (step % every == 0 or done):
+                pending.append(pool.submit(emit, self.field_update_async(), frame))
+                frame += 1
             if rep.converged:
                 converged = True
                 break
             if rep.reached_end_time:
                 break
+        if write_output:
+            last = None
+            for f in pending:
+                last = f.result()
+            pool.shutdown()
+            if last is not None:
+                from . import output
+                output.write_field_csv(os.path.join(self.cfg.output_dir, "field.csv"), self, last)
+                output.write_legacy_vtk(os.path.join(self.cfg.output_dir, "field.vtk"), self.cfg.case.name(), self,
+                                        last)
         self.last_report = rep
         return RunSummary(case_name=self.cfg.case.name(), steps=step, final_time=rep.time if rep else 0.0,
                           max_divergence=rep.continuity_residual if rep else 0.0,
@@ -458,6 +521,16 @@ class IncompressibleSolver:
                "vorticity": _abi.FIELD_VORTICITY, "u_cell": _abi.FIELD_U_CELL,
                "v_cell": _abi.FIELD_V_CELL, "temperature": _abi.FIELD_TEMPERATURE}[name]
         return self._h.download(fid)
+
+    def field_update_async(self) -> "PendingFieldUpdate":
+        """field_update() taken without stalling the solver: the fields are
+        copied on the device after the work already enqueued and drained to
+        page-locked host memory on a copy stream; .wait() gives the
+        FieldUpdate."""
+        fids = [_abi.FIELD_U, _abi.FIELD_V, _abi.FIELD_PRESSURE, _abi.FIELD_SPEED, _abi.FIELD_VORTICITY]
+        if self.cfg.physics.thermal.model == "constant-properties":
+            fids.append(_abi.FIELD_TEMPERATURE)
+        return PendingFieldUpdate(self, self._h.snapshot_begin(fids))
 
     def field_update(self) -> FieldUpdate:
         """field_update() (:563-586)."""
@@ -474,6 +547,26 @@ class IncompressibleSolver:
 
     def close(self) -> None:
         self._h.close()
+
+
+class PendingFieldUpdate:
+    """A FieldUpdate whose fields are still draining to the host."""
+
+    def __init__(self, solver: "IncompressibleSolver", snap: Snapshot):
+        self._solver = solver
+        self._snap = snap
+
+    def wait(self) -> FieldUpdate:
+        f = self._snap.wait()
+        cfg = self._solver.cfg
+        nx, ny = cfg.nx, cfg.ny
+        u = f[_abi.FIELD_U].reshape(ny, nx + 1)
+        v = f[_abi.FIELD_V].reshape(ny + 1, nx)
+        return FieldUpdate(nx=nx, ny=ny, pressure=f[_abi.FIELD_PRESSURE].copy(), speed=f[_abi.FIELD_SPEED].copy(),
+                           velocity_x=(0.5 * (u[:, :-1] + u[:, 1:])).ravel(),
+                           velocity_y=(0.5 * (v[:-1, :] + v[1:, :])).ravel(),
+                           vorticity=f[_abi.FIELD_VORTICITY].copy(), solid=cfg.case.solid_mask(nx, ny).ravel(),
+                           temperature=f[_abi.FIELD_TEMPERATURE].copy() if _abi.FIELD_TEMPERATURE in f else None)
 
 
 class BatchedIncompressibleSolver:

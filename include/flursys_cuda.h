@@ -300,6 +300,21 @@ int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream);
  * the capacity of `phase_ms` (4 used). No reference counterpart. */
 int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms, size_t n);
 
+/* Output overlapped with compute. No reference counterpart as an API: it
+ * serves the snapshots that field_update() / prepare_output() take between
+ * steps (incompressible.rs:563-586, output.rs:31-176) without stalling the
+ * solver. snapshot_begin copies `count` fields (FlursysFieldId; each
+ * host[i] holds sizes[i] doubles, ideally page-locked) into device snapshot
+ * buffers on the handle's stream, ordered after the work already enqueued,
+ * then drains them to the host buffers on a separate copy stream and
+ * returns at once; steps called after it run while the copy drains.
+ * snapshot_wait blocks until the host buffers hold the snapshot. One
+ * snapshot may be pending per handle (FLURSYS_ERR_INVALID_ARGUMENT
+ * otherwise); the host buffers must stay valid until snapshot_wait returns. */
+int32_t flursys_cuda_snapshot_begin(FlursysCudaHandle *h, const int32_t *field_ids, int32_t count,
+                                    double *const *host, const size_t *sizes);
+int32_t flursys_cuda_snapshot_wait(FlursysCudaHandle *h);
+
 /* Copies the last error message (NUL-terminated, truncated to `size`). */
 int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size);
 
@@ -312,7 +327,8 @@ int32_t flursys_cuda_global_error(char *buf, size_t size);
 /* Host-side fault injection for tests of the bounded device waits. No
  * reference counterpart. The next persistent 3D PCG launch (the kernel of
  * flursys_cuda_stencil_pcg with nz >= 2, of flursys_cuda_stencil_pcg_noalloc,
- * and of 3D handles configured with the persistent solver) waits at its grid
+ * of 3D handles configured with the persistent solver, and the chip-resident
+ * MIXED solve of 3D handles) waits at its grid
  * barriers for `extra_arrivals` blocks that were never launched, with a poll
  * limit of a few milliseconds; every wait gives up, the kernel returns, and
  * the call reports FLURSYS_ERR_TIMEOUT with the device context intact. The

@@ -1,0 +1,69 @@
+"""3D pressure PCG, MIXED precision, with the solver state resident on the
+chip (one cooperative launch per solve; the default where the grid's
+32 x 32 x tz tiles fit one per SM): against the FP64 oracle, against the
+graph-driven two-launch PCG (FLURSYS_PCG_RESIDENT=0), at its iteration cap,
+and with an injected grid-barrier fault."""
+import numpy as np
+import pytest
+
+from flursys_b200 import _abi
+from flursys_b200.solver import SolverError, _Handle
+
+from .test_gpu_cavity3d import FIELDS, MIXED_TOL, cfg3d
+from .test_gpu_pcg3d_variants import _vel_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(oracle, shape, steps, monkeypatch, resident=True, rtol=1e-8, max_iters=20000):
+    if not resident:
+        monkeypatch.setenv("FLURSYS_PCG_RESIDENT", "0")
+    cfg = cfg3d(oracle, *shape, rtol=rtol, precision=_abi.PRECISION_MIXED)
+    cfg.pressure_max_iters = max_iters
+    gpu = _Handle(cfg)
+    reps = [gpu.step(1) for _ in range(steps)]
+    fields = {fid: gpu.download(fid) for fid, _ in FIELDS}
+    monkeypatch.delenv("FLURSYS_PCG_RESIDENT", raising=False)
+    return reps, fields, gpu
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (48, 40, 36), (20, 70, 9), (64, 96, 50)])
+def test_resident_pcg_against_fp64_oracle(oracle, monkeypatch, shape):
+    ref = oracle.OracleSolver(cfg3d(oracle, *shape, rtol=1e-8))
+    steps = 4
+    ref_reps = [ref.step(1) for _ in range(steps)]
+    reps, fields, _ = _run(oracle, shape, steps, monkeypatch)
+    for a, b in zip(reps, ref_reps):
+        assert a.pressure_status == _abi.LINEAR_CONVERGED
+        assert a.pressure_true_relative_residual <= 1.0e-8 * 1.0001
+        assert abs(a.pressure_iterations - b.pressure_iterations) <= max(3, b.pressure_iterations // 50)
+    assert _vel_rel(fields, {fid: ref.get(fid) for fid, _ in FIELDS[:3]}) <= MIXED_TOL
+
+
+def test_resident_and_graph_paths_agree(oracle, monkeypatch):
+    shape = (48, 40, 32)  # > 100 iterations: residual replacements inside each solve
+    res, f1, _ = _run(oracle, shape, 3, monkeypatch)
+    seq, f2, _ = _run(oracle, shape, 3, monkeypatch, resident=False)
+    for a, b in zip(res, seq):
+        assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
+        assert b.pressure_iterations > 100
+        assert abs(a.pressure_iterations - b.pressure_iterations) <= 2
+    assert _vel_rel(f1, f2) <= MIXED_TOL
+
+
+def test_resident_iteration_cap(oracle, monkeypatch):
+    reps, fields, _ = _run(oracle, (32, 32, 32), 1, monkeypatch, rtol=1e-12, max_iters=37)
+    rep = reps[0]
+    assert rep.pressure_status == _abi.LINEAR_MAX_ITERATIONS
+    assert rep.pressure_iterations == 37
+    assert all(np.isfinite(v).all() for v in fields.values())
+
+
+def test_resident_barrier_timeout_is_reported(oracle, monkeypatch, cudalib):
+    reps, _, gpu = _run(oracle, (32, 32, 32), 1, monkeypatch)
+    assert cudalib.flursys_cuda_debug_inject_barrier_fault(1) == 0
+    with pytest.raises(SolverError) as e:
+        gpu.step(1)
+    assert e.value.status == _abi.ERR_TIMEOUT and "timed out" in str(e.value)
+    rep = gpu.step(1)  # the injection covered one launch; the context is intact
+    assert rep.pressure_status == _abi.LINEAR_CONVERGED

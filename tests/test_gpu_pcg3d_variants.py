@@ -60,7 +60,7 @@ def test_single_reduction_pcg_against_fp64_oracle(oracle, monkeypatch, shape, en
 def test_single_reduction_iterations_track_standard_pcg(oracle, monkeypatch):
     shape = (48, 40, 32)  # > 100 iterations: two residual replacements inside each solve
     one, f1 = _run(oracle, shape, 3, monkeypatch, {})
-    two, f2 = _run(oracle, shape, 3, monkeypatch, {"FLURSYS_PCG_CG1": "0"})
+    two, f2 = _run(oracle, shape, 3, monkeypatch, {"FLURSYS_PCG_CG1": "0", "FLURSYS_PCG_RESIDENT": "0"})
     for a, b in zip(one, two):
         assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
         assert b.pressure_iterations > 100
