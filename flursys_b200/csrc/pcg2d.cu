@@ -286,6 +286,11 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
         write_parts_max<4>(k, sync, v2, s_max, red);
         return sync();
     };
+    // Sums of the projected residual and solution over fluid cells, carried
+    // from one iteration to the next: the means that the projection of the
+    // updated x and r removes follow from them without another reduction,
+    //   sum(x + a (d - md)) = sum x,   sum(r - a q) = sum r - a sum q.
+    double s_r_prev = 0.0, s_x_prev = 0.0;
     auto read_residual_sums = [&](double &rr, double &rmax, double &rz) {
         double s4[4];
         read_sums_max<4>(k, sync, s4, rmax, red);
@@ -293,7 +298,9 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
         const double sz = s4[1], srz = s4[2], sr = s4[3];
         mz = proj ? sz / cnt : 0.0;
         rz = srz - mz * sr;  // r'.(z - mean z)
+        s_r_prev = sr;
     };
+    s_x_prev = m0[0] - cnt * mx;  // sum of x after the initial projection
     if (!residual_pass()) return;
     double rr, rmax;
     read_residual_sums(rr, rmax, rz_old);
@@ -393,57 +400,17 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
         if (fabs(dq) < 1.0e-30 || !isfinite(dq)) { error = FLURSYS_ERR_BREAKDOWN; break; }
         const double alpha = rz_old / dq;
         if (!isfinite(alpha)) { error = FLURSYS_ERR_BREAKDOWN; break; }
-        // ---- pass 2: updates (and their sums when projecting) ----
+        // ---- the means removed by the projection of the updated x and r ----
         double mr = 0.0;
         if (proj) {
-            double s_x = 0.0, s_r = 0.0;
-            if (plain) {
-                for (int c0 = k.c_begin + threadIdx.x; c0 < k.c_end; c0 += kU * kBlock) {
-                    double xv[kU], dv[kU];
-                    V rv[kU], qv[kU];
-#pragma unroll
-                    for (int u = 0; u < kU; ++u) {
-                        const int c = c0 + u * kBlock;
-                        const bool ok = c < k.c_end;
-                        xv[u] = ok ? x[c] : 0.0;
-                        dv[u] = ok ? double(dcur[c]) : 0.0;
-                        rv[u] = ok ? r[c] : V(0);
-                        qv[u] = ok ? q[c] : V(0);
-                    }
-#pragma unroll
-                    for (int u = 0; u < kU; ++u) {
-                        const int c = c0 + u * kBlock;
-                        if (c >= k.c_end) continue;
-                        const double xn = xv[u] + alpha * (dv[u] - md);
-                        const V rn = V(double(rv[u]) - alpha * double(qv[u]));
-                        x[c] = xn;
-                        r[c] = rn;
-                        s_x += xn;
-                        s_r += double(rn);
-                    }
-                }
-            } else {
-                for (int c = k.c_begin + threadIdx.x; c < k.c_end; c += kBlock) {
-                    if (ident(f, c)) continue;
-                    const double dc = double(dcur[c]) - md;
-                    const double xv = x[c] + alpha * dc;
-                    const V rv = V(double(r[c]) - alpha * double(q[c]));
-                    x[c] = xv;
-                    r[c] = rv;
-                    s_x += xv;
-                    s_r += double(rv);
-                }
-            }
-            double v[2] = {s_x, s_r};
-            write_parts<2>(k, sync, v, red);
-            if (!sync()) return;
-            double s2[2];
-            read_sums<2>(k, sync, s2, red);
-            mx = s2[0] / cnt;
-            mr = s2[1] / cnt;
+            mx = s_x_prev / cnt;
+            mr = (s_r_prev - alpha * s3[1]) / cnt;
         }
-        // ---- pass 3: projection, residual, z, r.z ----
-        double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0;
+        // ---- pass 2: update, projection, residual, z, r.z ----
+        // x += a (d - md) and r -= a q (FP32 r rounded as stored), then the
+        // means are removed: the arithmetic of an update pass followed by a
+        // projection pass, in one sweep.
+        double s_rr = 0.0, s_max = 0.0, s_z = 0.0, s_rz = 0.0, s_r = 0.0, s_x = 0.0;
         if (plain) {
             for (CellIter it = first_cell(k); it.c < k.c_end;) {
                 CellIter cs[kU];
@@ -456,8 +423,8 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
                     const int c = ok ? it.c : k.c_begin;
                     xv[u] = x[c];
                     rv0[u] = r[c];
-                    pv[u] = proj ? 0.0 : double(dcur[c]);
-                    qv[u] = proj ? V(0) : q[c];
+                    pv[u] = double(dcur[c]);
+                    qv[u] = q[c];
                     next_cell(k, it);
                 }
 #pragma unroll
@@ -466,8 +433,10 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
                     if (c >= k.c_end) continue;
                     double rv;
                     if (proj) {
-                        x[c] = xv[u] - mx;
-                        rv = double(V(double(rv0[u]) - mr));
+                        const double xn = (xv[u] + alpha * (pv[u] - md)) - mx;
+                        x[c] = xn;
+                        s_x += xn;
+                        rv = double(V(double(V(double(rv0[u]) - alpha * double(qv[u]))) - mr));
                     } else {
                         x[c] = xv[u] + alpha * pv[u];
                         rv = double(V(double(rv0[u]) - alpha * double(qv[u])));
@@ -497,8 +466,10 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
                 zv = rv;
             } else {
                 if (proj) {
-                    x[c] -= mx;
-                    rv = double(V(double(r[c]) - mr));
+                    const double xn = (x[c] + alpha * (double(dcur[c]) - md)) - mx;
+                    x[c] = xn;
+                    s_x += xn;
+                    rv = double(V(double(V(double(r[c]) - alpha * double(q[c]))) - mr));
                 } else {
                     x[c] += alpha * double(dcur[c]);
                     rv = double(V(double(r[c]) - alpha * double(q[c])));
@@ -515,12 +486,20 @@ __device__ void pcg_instance(Ctx &k, double *red, const Sync &sync) {
             s_rz += rv * double(V(zv));
         }
         {
-            double v[4] = {s_rr, s_z, s_rz, s_r};
-            write_parts_max<4>(k, sync, v, s_max, red);
+            double v[5] = {s_rr, s_z, s_rz, s_r, s_x};
+            write_parts_max<5>(k, sync, v, s_max, red);
         }
         if (!sync()) return;
         double rz_new;
-        read_residual_sums(rr, rmax, rz_new);
+        {
+            double s5[5];
+            read_sums_max<5>(k, sync, s5, rmax, red);
+            rr = s5[0];
+            mz = proj ? s5[1] / cnt : 0.0;
+            rz_new = s5[2] - mz * s5[3];
+            s_r_prev = s5[3];
+            s_x_prev = s5[4];
+        }
         residual = l2 ? sqrt(rr) : rmax;
         if (!isfinite(residual)) { error = FLURSYS_ERR_NON_FINITE; break; }
         bool conv = l2 ? (residual <= threshold) : (residual < threshold);

@@ -49,6 +49,7 @@ struct SeqGeo {
     int tiles_x, tiles_y, kc, chunks;  // tile / direct sweeps: 32 x 8 columns
     int tiles_yw, kcw, chunksw;        // warp sweep: 32 x (8 * kRyOperand) columns
     int tiles_xv, tiles_yv, kcv, chunksv;  // vector sweep: (32 W) x (8 kRyVec) columns
+    int kcp, chunksp;                      // staged sweep: the vector sweep's columns, longer chunks
     double ix2, iy2, iz2;
     double inv_diag[27];  // 1/diag by missing-neighbour class 9*mx + 3*my + mz
 };
@@ -79,7 +80,7 @@ struct SeqArgs {
     int nblocks_cg1;  // grid of its step kernel
 };
 
-enum SweepKind : int { kSweepWarp = 0, kSweepTile = 1, kSweepDirect = 2, kSweepVec = 3 };
+enum SweepKind : int { kSweepWarp = 0, kSweepTile = 1, kSweepDirect = 2, kSweepVec = 3, kSweepPipe = 4 };
 constexpr int kRyVec = 2;  // rows per lane of the vectorised operand pass
 constexpr int kRyOperand = 4;  // rows per lane of the warp sweep (FP32; half of it in FP64)
 
@@ -698,6 +699,202 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_vec(SeqArgs a) {
             for (int e = 0; e < W; ++e) { vs[e] = vs1[e]; vn[e] = vn1[e]; }
         }
     }
+    const double v[1] = {sdq};
+    if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
+    double o[1];
+    reduce_finish<1>(o, a.partials, red);
+    if (threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->counter = 0;
+        const double dq = o[0];
+        if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(w->rz_old / dq)) {
+            w->error = FLURSYS_ERR_BREAKDOWN;
+            w->done = 1;
+            w->alpha = 0.0;
+        } else {
+            w->alpha = w->rz_old / dq;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// seq_dir_pipe: the MIXED operand pass with its raw inputs staged through
+// shared memory by cp.async. A block owns the vector sweep's column tile
+// (128 cells of x by 16 rows) and marches a long chunk of planes; while
+// plane k is computed, the raw r and d_old of planes k+2 and k+3 are in
+// flight (a ring of kPipeSlots planes: the tile's 16 rows, the two y-halo
+// rows and the two x-halo columns), so the latency of the loads is hidden
+// by a whole plane of work and no register holds data in flight. The
+// arithmetic is that of seq_dir_vec: d = z + beta d_old formed for the
+// cells and their neighbours, q = A d with x neighbours by warp shuffle,
+// d.q accumulated in FP64; cells outside the grid are staged as zeros.
+// ---------------------------------------------------------------------------
+constexpr int kPipeX = 128, kPipeY = 16, kPipeSlots = 5;
+constexpr int kPipeRows = kPipeY + 2;                        // rows -1 .. 16
+constexpr int kPipeArr = kPipeRows * kPipeX + 2 * kPipeY;    // floats per array per slot (+ x halos)
+constexpr int kPipeSmem = kPipeSlots * 2 * kPipeArr * 4;      // bytes
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+
+__global__ void __launch_bounds__(kBlock, 2) seq_dir_pipe(SeqArgs a) {
+    extern __shared__ __align__(16) float pipe_smem[];
+    __shared__ double red[kSlots * (kBlock / 32)];
+    __shared__ float idg[27];
+    const SeqGeo &g = a.g;
+    if (threadIdx.x < 27) idg[threadIdx.x] = float(g.inv_diag[threadIdx.x]);
+    const CgSeqState *s = a.st;
+    if (s->done) return;  // uniform: the solve has finished
+    const bool first = s->first != 0;
+    const float beta = float(s->beta);
+    const int parity = (int)(s->iterations & 1);
+    const float *r = static_cast<const float *>(a.r);
+    float *dcur = static_cast<float *>(parity ? a.d1 : a.d0);
+    const float *dold = static_cast<const float *>(parity ? a.d0 : a.d1);
+    float *q = static_cast<float *>(a.q);
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int t = blockIdx.x;
+    const int ch = t % g.chunksp, col = t / g.chunksp;
+    const int i0 = (col % g.tiles_xv) * kPipeX;
+    const int j0 = (col / g.tiles_xv) * kPipeY;
+    const int k0 = ch * g.kcp, k1 = min(g.nz, k0 + g.kcp);
+    // staging of plane p into its ring slot (zeros outside the grid)
+    auto slot_of = [&](int p) { return pipe_smem + ((p - k0 + 1) % kPipeSlots) * 2 * kPipeArr; };
+    auto stage = [&](int p) {
+        float *sl = slot_of(p);
+        const bool pin = p >= 0 && p < g.nz;
+        for (int e = threadIdx.x; e < 2 * kPipeRows * (kPipeX / 4); e += kBlock) {
+            const int arr = e / (kPipeRows * (kPipeX / 4)), rem = e - arr * (kPipeRows * (kPipeX / 4));
+            const int ry = rem / (kPipeX / 4), c4 = rem - ry * (kPipeX / 4);
+            const int j = j0 + ry - 1, i = i0 + 4 * c4;
+            const bool ok = pin && j >= 0 && j < g.ny && i < g.nx && !(arr == 1 && first);
+            const float *base = arr ? dold : r;
+            const float *src = ok ? base + ((size_t)p * g.ny + j) * g.nx + i : base;
+            cp_async16(sl + arr * kPipeArr + ry * kPipeX + 4 * c4, src, ok);
+        }
+        if (threadIdx.x < 4 * kPipeY) {
+            const int arr = threadIdx.x / (2 * kPipeY), side = (threadIdx.x / kPipeY) & 1, y = threadIdx.x % kPipeY;
+            const int i = side ? i0 + kPipeX : i0 - 1, j = j0 + y;
+            const bool ok = pin && i >= 0 && i < g.nx && j < g.ny && !(arr == 1 && first);
+            const float *base = arr ? dold : r;
+            const float *src = ok ? base + ((size_t)p * g.ny + j) * g.nx + i : base;
+            cp_async4(sl + arr * kPipeArr + kPipeRows * kPipeX + side * kPipeY + y, src, ok);
+        }
+    };
+    double sdq = 0.0;
+    // prologue: planes k0 - 1 .. k0 + 2 (one commit group each)
+    for (int p = k0 - 1; p <= k0 + 2; ++p) {
+        if (p <= k1) stage(p);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    const int ib = i0 + lane * 4;
+    const bool inx = ib < g.nx;
+    const int ibc = inx ? ib : 0;
+    const float wx = float(g.ix2), wy = float(g.iy2), wz = float(g.iz2);
+    const float wxm0 = (inx && ib > 0) ? wx : 0.f, wxpL = (inx && ib + 4 < g.nx) ? wx : 0.f;
+    const int mx0 = miss(ibc, g.nx), mxL = miss(ibc + 3, g.nx);
+    const bool hw = lane == 0 && i0 > 0, he = lane == 31 && i0 + kPipeX < g.nx;
+    const int xh = hw ? i0 - 1 : (he ? i0 + kPipeX : 0);
+    const int mxh = miss(xh, g.nx);
+    const int row0 = j0 + wp * 2;  // this warp's two rows
+    // d of the lane's 4 cells of tile row ry (-1 .. 16) of plane p from the staged raw inputs
+    auto make4 = [&](const float *sl, int ry, int p, float (&out)[4]) {
+        const int row = j0 + ry;
+        if (row < 0 || row >= g.ny || p < 0 || p >= g.nz || !inx) {
+            out[0] = out[1] = out[2] = out[3] = 0.f;
+            return;
+        }
+        const float4 rv = *reinterpret_cast<const float4 *>(sl + (ry + 1) * kPipeX + lane * 4);
+        const float4 dv = *reinterpret_cast<const float4 *>(sl + kPipeArr + (ry + 1) * kPipeX + lane * 4);
+        const float rr[4] = {rv.x, rv.y, rv.z, rv.w}, dd[4] = {dv.x, dv.y, dv.z, dv.w};
+        const int cyz = 3 * miss(row, g.ny) + miss(p, g.nz);
+        const float mid = idg[cyz];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float id = mid;
+            if (e == 0 && mx0) id = idg[9 * mx0 + cyz];
+            if (e == 3 && mxL) id = idg[9 * mxL + cyz];
+            const float z = rr[e] * id;
+            out[e] = first ? z : float(z + beta * dd[e]);
+        }
+        if (p == 0 && row == 0 && ibc == 0) out[0] = 0.f;  // pinned cell
+    };
+    auto make_halo = [&](const float *sl, int y, int p) -> float {  // x-halo column cell of tile row y
+        const int row = j0 + y;
+        if (!(hw || he) || row >= g.ny || p < 0 || p >= g.nz) return 0.f;
+        if (p == 0 && row == 0 && xh == 0) return 0.f;
+        const int side = he ? 1 : 0;
+        const float rv = sl[kPipeRows * kPipeX + side * kPipeY + y];
+        const float dv = sl[kPipeArr + kPipeRows * kPipeX + side * kPipeY + y];
+        const float z = rv * idg[9 * mxh + 3 * miss(row, g.ny) + miss(p, g.nz)];
+        return first ? z : float(z + beta * dv);
+    };
+    float below[2][4], cur[2][4];
+    asm volatile("cp.async.wait_group 2;" ::: "memory");  // planes k0 - 1, k0 landed
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        make4(slot_of(k0 - 1), wp * 2 + m, k0 - 1, below[m]);
+        make4(slot_of(k0), wp * 2 + m, k0, cur[m]);
+    }
+    for (int k = k0; k < k1; ++k) {
+        if (k + 3 <= k1) stage(k + 3);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 2;" ::: "memory");  // planes up to k + 1 landed
+        __syncthreads();
+        const float *slk = slot_of(k), *sla = slot_of(k + 1);
+        float above[2][4], ys[4], yn[4];
+        make4(sla, wp * 2, k + 1, above[0]);
+        make4(sla, wp * 2 + 1, k + 1, above[1]);
+        make4(slk, wp * 2 - 1, k, ys);
+        make4(slk, wp * 2 + 2, k, yn);
+        const float hx0 = make_halo(slk, wp * 2, k), hx1 = make_halo(slk, wp * 2 + 1, k);
+        const float wzm = k > 0 ? wz : 0.f, wzp = k + 1 < g.nz ? wz : 0.f;
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int row = row0 + m;
+            float west = __shfl_up_sync(0xffffffffu, cur[m][3], 1);
+            float east = __shfl_down_sync(0xffffffffu, cur[m][0], 1);
+            const float hxm = m ? hx1 : hx0;
+            if (lane == 0) west = hw ? hxm : 0.f;
+            if (lane == 31) east = he ? hxm : 0.f;
+            if (!inx || row >= g.ny) continue;
+            const float wym = row > 0 ? wy : 0.f, wyp = row + 1 < g.ny ? wy : 0.f;
+            float dv[4], qv[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float wxm = e == 0 ? wxm0 : wx, wxp = e == 3 ? wxpL : wx;
+                const float xm = e == 0 ? west : cur[m][e > 0 ? e - 1 : 0];
+                const float xp = e == 3 ? east : cur[m][e < 3 ? e + 1 : 3];
+                const float ysv = m == 0 ? ys[e] : cur[0][e];
+                const float ynv = m == 1 ? yn[e] : cur[1][e];
+                const float c0 = cur[m][e];
+                float ax = (wxm + wxp + wym + wyp + wzm + wzp) * c0 -
+                           (wxm * xm + wxp * xp + wym * ysv + wyp * ynv + wzm * below[m][e] + wzp * above[m][e]);
+                if (k == 0 && row == 0 && ib + e == 0) ax = c0;  // identity row of the pinned cell
+                dv[e] = c0;
+                qv[e] = ax;
+                sdq += double(c0) * double(ax);
+            }
+            const size_t c = ((size_t)k * g.ny + row) * g.nx + ib;
+            *reinterpret_cast<float4 *>(dcur + c) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+            *reinterpret_cast<float4 *>(q + c) = make_float4(qv[0], qv[1], qv[2], qv[3]);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                below[m][e] = cur[m][e];
+                cur[m][e] = above[m][e];
+            }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     const double v[1] = {sdq};
     if (!reduce_arrive<1>(v, a.partials, &a.st->counter, red)) return;
     double o[1];
@@ -1336,8 +1533,10 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
     e = add_kernel(g, &n_init, nullptr, 0, (const void *)seq_init<V, MIXED>, a.nblocks_stencil, args);
     if (e == cudaSuccess) e = cudaGraphAddDependencies(g, &n_init, &n_while, 1);
     if (e != cudaSuccess) return e;
-    const void *dir_fn = a.sweep == kSweepVec ? (const void *)seq_dir_vec<V, MIXED, kRyVec>
-                                              : (const void *)seq_dir_spmv<V, MIXED>;
+    const void *dir_fn = a.sweep == kSweepVec    ? (const void *)seq_dir_vec<V, MIXED, kRyVec>
+                         : (MIXED && a.sweep == kSweepPipe) ? (const void *)seq_dir_pipe
+                                                            : (const void *)seq_dir_spmv<V, MIXED>;
+    const unsigned dir_smem = (MIXED && a.sweep == kSweepPipe) ? (unsigned)kPipeSmem : 0u;
     cudaGraphNode_t prev{};
     for (int u = 0; u < unroll; ++u) {
         cudaGraphConditionalHandle hr;
@@ -1348,7 +1547,7 @@ cudaError_t build(Pcg3dSeqPlan &plan, SeqArgs &a) {
         if (u == 0) a.h_replace = hr;  // the argument block of the nodes outside the body
         void *uargs[] = {&au};
         cudaGraphNode_t n_dir, n_upd, n_if;
-        e = add_kernel(body, &n_dir, u ? &prev : nullptr, u ? 1 : 0, dir_fn, a.nblocks_dir, uargs);
+        e = add_kernel(body, &n_dir, u ? &prev : nullptr, u ? 1 : 0, dir_fn, a.nblocks_dir, uargs, dir_smem);
         if (e == cudaSuccess)
             e = add_kernel(body, &n_upd, &n_dir, 1, (const void *)seq_update<V, MIXED>, a.nblocks_point, uargs);
         if (e != cudaSuccess) return e;
@@ -1485,6 +1684,13 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     g.tiles_xv = (g.nx + 32 * wv - 1) / (32 * wv);
     g.tiles_yv = (g.ny + TY * kRyVec - 1) / (TY * kRyVec);
     chunking((long long)g.tiles_xv * g.tiles_yv, &g.kcv, &g.chunksv);
+    {   // staged sweep: one wave of two blocks per SM, long chunks (the ring's
+        // three extra planes are re-read per chunk)
+        const long long cols = (long long)g.tiles_xv * g.tiles_yv;
+        long long chunks = std::max(1LL, std::min<long long>(g.nz, (long long)sms * 2 / std::max(1LL, cols)));
+        g.kcp = (int)((g.nz + chunks - 1) / chunks);
+        g.chunksp = (g.nz + g.kcp - 1) / g.kcp;
+    }
     // pointwise grid: 4 blocks per SM (measured on B200: 32.5 us per iteration
     // at 128^3 against 34.4 with 8, equal at 256^3); the environment variable
     // FLURSYS_PCG_POINT_BLOCKS_PER_SM overrides it
@@ -1500,7 +1706,8 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.max_iters = args.max_iters;
     a.replace_every = args.replace_every > 0 ? args.replace_every : 50;
     const int nb = std::max({a.nblocks_stencil, a.nblocks_point, g.tiles_x * g.tiles_yw * g.chunksw,
-                             g.tiles_xv * g.tiles_yv * g.chunksv, g.tiles_x * g.tiles_y * ((g.nz + 3) / 4)});
+                             g.tiles_xv * g.tiles_yv * g.chunksv, g.tiles_xv * g.tiles_yv * g.chunksp,
+                             g.tiles_x * g.tiles_y * ((g.nz + 3) / 4)});
     cudaError_t e = cudaMalloc(&plan.partials, sizeof(double) * kSlots * nb);
     if (e == cudaSuccess) e = cudaMalloc(&plan.state, sizeof(CgSeqState));
     if (e == cudaSuccess) e = cudaMemset(plan.state, 0, sizeof(CgSeqState));
@@ -1511,13 +1718,21 @@ cudaError_t pcg3d_seq_plan(Pcg3dSeqPlan &plan, const Pcg3dArgs &args, int precis
     a.graph = 1;
     const char *st = std::getenv("FLURSYS_STENCIL");
     const bool vec_ok = g.nx % wv == 0;
-    a.sweep = vec_ok ? kSweepVec : kSweepTile;
+    // MIXED takes the staged sweep (FLURSYS_STENCIL=vec selects the register
+    // sweep); FP64 the register sweep
+    a.sweep = vec_ok ? (precision == FLURSYS_PRECISION_MIXED ? kSweepPipe : kSweepVec) : kSweepTile;
+    if (st && std::strcmp(st, "vec") == 0 && vec_ok) a.sweep = kSweepVec;
     if (st && std::strcmp(st, "direct") == 0) a.sweep = kSweepDirect;
     if (st && std::strcmp(st, "tiled") == 0) a.sweep = kSweepTile;
     if (st && std::strcmp(st, "warp") == 0) a.sweep = kSweepWarp;
     a.nblocks_dir = a.sweep == kSweepWarp ? g.tiles_x * g.tiles_yw * g.chunksw
                   : a.sweep == kSweepVec  ? g.tiles_xv * g.tiles_yv * g.chunksv
+                  : a.sweep == kSweepPipe ? g.tiles_xv * g.tiles_yv * g.chunksp
                                           : a.nblocks_stencil;
+    if (a.sweep == kSweepPipe) {
+        e = cudaFuncSetAttribute((const void *)seq_dir_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, kPipeSmem);
+        if (e != cudaSuccess) return e;
+    }
     // FLURSYS_PCG_CG1=1 selects the single-reduction variant for MIXED when
     // the TMA maps can be made (nx % 4 == 0); FLURSYS_CG1_TZ=4 selects
     // 4-plane tiles (8 by default). It is not the default: on B200 at 128^3
@@ -1608,6 +1823,7 @@ cudaError_t pcg3d_seq_run_host(const Pcg3dSeqPlan &plan, cudaStream_t st) {
         for (int j = 0; j < 16; ++j) {
             if (mixed) {
                 if (a.sweep == kSweepVec) seq_dir_vec<float, true, kRyVec><<<a.nblocks_dir, kBlock, 0, st>>>(a);
+                else if (a.sweep == kSweepPipe) seq_dir_pipe<<<a.nblocks_dir, kBlock, kPipeSmem, st>>>(a);
                 else seq_dir_spmv<float, true><<<a.nblocks_dir, kBlock, 0, st>>>(a);
                 seq_update<float, true><<<a.nblocks_point, kBlock, 0, st>>>(a);
                 seq_fold<<<a.nblocks_point, kBlock, 0, st>>>(a);

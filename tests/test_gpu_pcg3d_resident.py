@@ -67,3 +67,21 @@ def test_resident_barrier_timeout_is_reported(oracle, monkeypatch, cudalib):
     assert e.value.status == _abi.ERR_TIMEOUT and "timed out" in str(e.value)
     rep = gpu.step(1)  # the injection covered one launch; the context is intact
     assert rep.pressure_status == _abi.LINEAR_CONVERGED
+
+
+@pytest.mark.parametrize("shape", [(64, 40, 48), (132, 20, 12)])  # partial x tiles; short chunks
+def test_staged_operand_pass_matches_register_pass(oracle, monkeypatch, shape):
+    # graph path (not resident): the cp.async-staged operand kernel (default
+    # for MIXED) against the register-prefetch kernel (FLURSYS_STENCIL=vec)
+    monkeypatch.setenv("FLURSYS_STENCIL", "vec")
+    vec, f2, _ = _run(oracle, shape, 3, monkeypatch, resident=False)
+    monkeypatch.delenv("FLURSYS_STENCIL")
+    pipe, f1, _ = _run(oracle, shape, 3, monkeypatch, resident=False)
+    for a, b in zip(pipe, vec):
+        assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
+        assert abs(a.pressure_iterations - b.pressure_iterations) <= 2
+    assert _vel_rel(f1, f2) <= MIXED_TOL
+    ref = oracle.OracleSolver(cfg3d(oracle, *shape, rtol=1e-8))
+    for _ in range(3):
+        ref.step(1)
+    assert _vel_rel(f1, {fid: ref.get(fid) for fid, _ in FIELDS[:3]}) <= MIXED_TOL
