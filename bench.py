@@ -120,12 +120,18 @@ def pcg_bytes_per_launch(n_cells: int, iterations: int, precision: str, replace_
     return float(n_cells) * (24 + 80 * iterations + 16)
 
 
-def launches_per_step(iterations: int, precision: str, replace_every: int = 50) -> int:
+def launches_per_step(iterations: int, precision: str, resident: bool, replace_every: int = 50,
+                      unroll: int = 8) -> int:
     """Kernels of one 3D step: predictor (3), rhs, correction, diagnostics (2),
-    and the solve graph: init, operand + update per iteration, fold + replace
-    per FP64 replacement, pending fold, final check."""
+    and the pressure solve: one cooperative launch when it runs chip-resident;
+    otherwise the solve graph's init, operand + update for each iteration of
+    every loop body entered (`unroll` iterations per body), fold + replace per
+    FP64 replacement, pending fold and final check."""
+    if resident:
+        return 7 + 1
+    bodies = -(-max(iterations, 1) // unroll)
     nrep = iterations // replace_every + 1 if precision == "mixed" else 0
-    return 7 + 1 + 2 * iterations + 2 * nrep + (1 if precision == "mixed" else 0) + 1
+    return 7 + 1 + 2 * bodies * unroll + 2 * nrep + (1 if precision == "mixed" else 0) + 1
 
 
 class ClockSampler:
@@ -388,6 +394,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     h = _Handle(c)
     h.set_stream(stream.cuda_stream)
+    resident = h.solve_kind() == _abi.SOLVE_RESIDENT
     n_cells = n ** 3
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
@@ -450,7 +457,8 @@ def run_ours(args):
             "true_relative_residual_max": max(true_rel),
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": hbytes,
                     "d2h_bytes_per_step": hbytes + report_bytes},
-            "gpu_launches": sum(launches_per_step(i, precision) for i in its),
+            "gpu_launches": sum(launches_per_step(i, precision, resident) for i in its),
+            "pressure_solve": "chip-resident cooperative PCG" if resident else "graph-driven PCG",
             "clocks": clocks,
         }
         line["roofline"] = roofline(n_cells, its, solve_ms, precision)

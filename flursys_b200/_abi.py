@@ -51,6 +51,7 @@ FIELD_U, FIELD_V, FIELD_W, FIELD_PRESSURE, FIELD_RHS = 0, 1, 2, 3, 4
 FIELD_U_STAR, FIELD_V_STAR, FIELD_W_STAR = 5, 6, 7
 FIELD_SPEED, FIELD_VORTICITY, FIELD_U_CELL, FIELD_V_CELL = 8, 9, 10, 11
 FIELD_TEMPERATURE = 12
+SOLVE_GRAPH, SOLVE_RESIDENT, SOLVE_PERSISTENT, SOLVE_SOR, SOLVE_FCG = 0, 1, 2, 3, 4
 
 
 class LinearSolverOptions(C.Structure):
@@ -280,6 +281,7 @@ SIGNATURES = {
     "flursys_cuda_snapshot_begin": (C.c_int32, [_P, C.POINTER(C.c_int32), C.c_int32, C.POINTER(_D),
                                                 C.POINTER(C.c_size_t)]),
     "flursys_cuda_snapshot_wait": (C.c_int32, [_P]),
+    "flursys_cuda_solve_kind": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
     "flursys_cuda_csr_cg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,
                                         C.POINTER(LinearSolverOptions), C.POINTER(LinearSolveReport)]),
     "flursys_cuda_csr_pcg": (C.c_int32, [C.c_int64, C.c_int64, _I64P, _I64P, _D, _D, _D,

@@ -455,6 +455,17 @@ int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms
     return FLURSYS_OK;
 }
 
+int32_t flursys_cuda_solve_kind(const FlursysCudaHandle *h, int32_t *kind) {
+    if (!h || !kind) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (h->cfg.dimension != 3) { g_error = "the solve kind describes 3D handles"; return FLURSYS_ERR_INVALID_ARGUMENT; }
+    if (h->cfg.pressure_solver == FLURSYS_PRESSURE_FCG) *kind = FLURSYS_SOLVE_FCG;
+    else if (h->cfg.pressure_solver == FLURSYS_PRESSURE_SOR) *kind = FLURSYS_SOLVE_SOR;
+    else if (!h->use_seq) *kind = FLURSYS_SOLVE_PERSISTENT;
+    else if (h->seq.resident) *kind = FLURSYS_SOLVE_RESIDENT;
+    else *kind = FLURSYS_SOLVE_GRAPH;
+    return FLURSYS_OK;
+}
+
 int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size) {
     copy_msg(h ? h->err : g_error, buf, size);
     return FLURSYS_OK;

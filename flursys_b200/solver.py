@@ -172,6 +172,12 @@ class _Handle:
         a = np.ascontiguousarray(values, dtype=np.float64).ravel()
         _check(self.lib, self.h, self.lib.flursys_cuda_upload(self.h, fid, _abi.dptr(a), a.size))
 
+    def solve_kind(self) -> int:
+        """FlursysSolveKind of a 3D handle's pressure solve."""
+        k = C.c_int32()
+        _check(self.lib, self.h, self.lib.flursys_cuda_solve_kind(self.h, C.byref(k)))
+        return int(k.value)
+
     def snapshot_begin(self, fids) -> "Snapshot":
         """Starts an asynchronous copy of the fields `fids` into page-locked
         host arrays; the next steps run while it drains (Snapshot.wait())."""

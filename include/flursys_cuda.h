@@ -315,6 +315,17 @@ int32_t flursys_cuda_snapshot_begin(FlursysCudaHandle *h, const int32_t *field_i
                                     double *const *host, const size_t *sizes);
 int32_t flursys_cuda_snapshot_wait(FlursysCudaHandle *h);
 
+/* Which implementation runs the pressure solve of a 3D handle (diagnostic;
+ * no reference counterpart): FlursysSolveKind. */
+typedef enum FlursysSolveKind {
+    FLURSYS_SOLVE_GRAPH = 0,      /* PCG as a kernel sequence in one CUDA graph (2 kernels per iteration) */
+    FLURSYS_SOLVE_RESIDENT = 1,   /* PCG as one cooperative launch with its state on the chip */
+    FLURSYS_SOLVE_PERSISTENT = 2, /* PCG as one cooperative launch streaming its vectors */
+    FLURSYS_SOLVE_SOR = 3,        /* red-black SOR */
+    FLURSYS_SOLVE_FCG = 4         /* learned-preconditioner flexible CG */
+} FlursysSolveKind;
+int32_t flursys_cuda_solve_kind(const FlursysCudaHandle *h, int32_t *kind);
+
 /* Copies the last error message (NUL-terminated, truncated to `size`). */
 int32_t flursys_cuda_last_error(const FlursysCudaHandle *h, char *buf, size_t size);
 
