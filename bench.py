@@ -712,17 +712,20 @@ def case_pcg(args) -> dict:
     from flursys_b200.solver import _Handle
     _, c = workload_config(args.size, args.precision)
     c.pressure_max_iters = args.iters
+    from flursys_b200 import _abi
     hd = _Handle(c)
     rows = []
     for s in range(args.steps):
         rep = hd.step(1)
         ph = (C.c_double * 4)()
         hd.lib.flursys_cuda_solver_profile(hd.h, ph, 4)
+        kind = hd.solve_kind()
+        names = (["halo+direction", "operator", "reduce+barrier", "update+replacement"]
+                 if kind == _abi.SOLVE_RESIDENT else ["stencil", "pointwise", "barrier+reduce", "replacement"])
         its = max(1, rep.pressure_iterations)
-        rows.append({"step": s + 1, "iterations": int(rep.pressure_iterations), "solve_ms": rep.pressure_solve_ms,
-                     "us_per_iteration": 1000.0 * rep.pressure_solve_ms / its,
-                     "phase_us_per_iteration": {k: 1000.0 * ph[i] / its for i, k in enumerate(
-                         ["stencil", "pointwise", "barrier+reduce", "replacement"])}})
+        rows.append({"step": s + 1, "solve_kind": int(kind), "iterations": int(rep.pressure_iterations),
+                     "solve_ms": rep.pressure_solve_ms, "us_per_iteration": 1000.0 * rep.pressure_solve_ms / its,
+                     "phase_us_per_iteration": {k: 1000.0 * ph[i] / its for i, k in enumerate(names)}})
     hd.close()
     return {"case": "pcg", "size": args.size, "steps": rows, "sm_mhz_after": sm_clock_mhz()}
 

@@ -45,11 +45,19 @@ constexpr int kCols = RX * RY / kResBlock;  // columns per thread
 constexpr int kResMaxTz = 16;
 constexpr int HX = RX + 2, HY = RY + 2;
 constexpr int kResSlots = 4;
+// face values per thread: two 32 x 32 z-faces and four 32 x tz side faces
+constexpr int kHaloPer = (2 * RX * RY + 4 * RX * kResMaxTz + kResBlock - 1) / kResBlock;
 
 __device__ __forceinline__ int rmiss(int i, int n) { return (i == 0) + (i == n - 1); }
 
 size_t res_smem_bytes(int tz) {
     return sizeof(float) * ((size_t)HX * HY * (tz + 2) + 2 * (size_t)RX * RY * tz);
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 // Grid barrier of the resident solve; a failure is recorded in the state.
@@ -62,12 +70,14 @@ struct ResCtx {
     float *dsm, *dxs, *qs;
     double *red;
     int round;
+    unsigned long long t_reduce;  // block 0, thread 0: time in grid reductions
 };
 
 // Sums NS values (and, with MAX, the maximum of one more) over the grid.
 // Every block obtains the same bits. Returns false when the barrier failed.
 template <int NS, bool MAX>
 __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &mx) {
+    const unsigned long long t0 = gtimer();
     block_reduce_n<kResBlock, NS, MAX>(v, mx, c.red);
     const int nb = gridDim.x;
     double *P = c.a.partials + (size_t)(c.round & 1) * nb * kResSlots;
@@ -106,6 +116,7 @@ __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &
     for (int k = 0; k < NS; ++k) v[k] = c.red[k];
     if (MAX) mx = c.red[NS];
     __syncthreads();
+    c.t_reduce += gtimer() - t0;
     return true;
 }
 
@@ -124,7 +135,8 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
     float *dsm = smem;                                      // (tz + 2) x HY x HX
     float *dxs = smem + (size_t)HX * HY * (tz_full + 2);   // tz x RY x RX
     float *qs = dxs + (size_t)RX * RY * tz_full;           // tz x RY x RX
-    ResCtx c{a, dsm, dxs, qs, red, 0};
+    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull};
+    unsigned long long t_halo = 0, t_op = 0, t_upd = 0;
     const int b = blockIdx.x;
     const int i0 = (b % a.ntx) * RX, j0 = ((b / a.ntx) % a.nty) * RY, k0 = (b / (a.ntx * a.nty)) * a.tz;
     const int kz = min(a.tz, a.nz - k0);
@@ -247,24 +259,40 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
     const int nhalo = 2 * RX * RY + 4 * RX * kz;
     while (!done) {
         // ---- d = z + beta d_old on the halo (neighbours' r faces) and the tile ----
+        const unsigned long long t0 = gtimer();
         const float fb = float(beta);
-        for (int s = threadIdx.x; s < nhalo; s += kResBlock) {
+        // every face value this thread needs is requested before any is used
+        float hv[kHaloPer];
+        int hslot[kHaloPer], hcls[kHaloPer];
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) {
+            const int s = threadIdx.x + u * kResBlock;
+            hslot[u] = -1;
+            hv[u] = 0.f;
+            hcls[u] = 0;
+            if (s >= nhalo) continue;
             int xx, yy, kk;
             if (s < 2 * RX * RY) {
                 const int t = s & (RX * RY - 1);
                 xx = t & 31; yy = t >> 5; kk = s < RX * RY ? -1 : kz;
             } else {
-                const int t = s - 2 * RX * RY, f = t / (RX * kz), u = t - f * (RX * kz);
-                const int p = u & 31, q = u >> 5;
+                const int t = s - 2 * RX * RY, f = t / (RX * kz), w = t - f * (RX * kz);
+                const int p = w & 31, q = w >> 5;
                 if (f < 2) { xx = p; yy = f == 0 ? -1 : RY; kk = q; }
                 else { yy = p; xx = f == 2 ? -1 : RX; kk = q; }
             }
             const int gi = i0 + xx, gj = j0 + yy, gk = k0 + kk;
             if (gi < 0 || gi >= a.nx || gj < 0 || gj >= a.ny || gk < 0 || gk >= a.nz) continue;
             const int cc = (gk * a.ny + gj) * a.nx + gi;
-            const int slot = ((kk + 1) * HY + yy + 1) * HX + xx + 1;
-            const int cls = 9 * rmiss(gi, a.nx) + 3 * rmiss(gj, a.ny) + rmiss(gk, a.nz);
-            dsm[slot] = make_d(__ldcg(a.rface + cc), dsm[slot], idgf[cls], cc == 0, first, fb);
+            hslot[u] = ((kk + 1) * HY + yy + 1) * HX + xx + 1;
+            hcls[u] = cc == 0 ? -1 : 9 * rmiss(gi, a.nx) + 3 * rmiss(gj, a.ny) + rmiss(gk, a.nz);
+            hv[u] = __ldcg(a.rface + cc);
+        }
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) {
+            if (hslot[u] < 0) continue;
+            const int sl = hslot[u];
+            dsm[sl] = make_d(hv[u], dsm[sl], idgf[hcls[u] < 0 ? 0 : hcls[u]], hcls[u] < 0, first, fb);
         }
 #pragma unroll
         for (int h = 0; h < kCols; ++h) {
@@ -278,6 +306,8 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
             }
         }
         __syncthreads();
+        const unsigned long long t1 = gtimer();
+        t_halo += t1 - t0;
         // ---- q = A d on the tile, d.q ----
         double sdq[1] = {0.0};
 #pragma unroll
@@ -301,7 +331,9 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
             }
         }
         double unused = 0.0;
+        t_op += gtimer() - t1;
         if (!grid_reduce<1, false>(c, sdq, unused)) return;
+        const unsigned long long t2 = gtimer();
         const double dq = sdq[0];
         if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(rz_old / dq)) {
             error = FLURSYS_ERR_BREAKDOWN;
@@ -328,6 +360,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
             }
         }
         publish();
+        t_upd += gtimer() - t2;
         if (!grid_reduce<2, true>(c, s2, mx)) return;
         iterations += 1;
         double res = l2 ? sqrt(s2[0]) : mx;
@@ -340,6 +373,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
         double rz = s2[1];
         if (conv || (iterations % a.replace_every) == 0) {
             // ---- FP64 residual replacement ----
+            const unsigned long long t3 = gtimer();
             fold();
             if (!res_sync(a)) return;
             double s3[2] = {0.0, 0.0};
@@ -355,6 +389,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
             }
             conv = stop_ok(res, threshold);
             rz = s3[1];
+            t_upd += gtimer() - t3;
         }
         if (conv) {
             status = FLURSYS_LINEAR_CONVERGED;
@@ -384,6 +419,10 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
         w->threshold = threshold;
         w->true_l2 = sqrt(st[0]);
         w->done = 1;
+        w->phase_ns[0] = t_halo;
+        w->phase_ns[1] = t_op;
+        w->phase_ns[2] = c.t_reduce;
+        w->phase_ns[3] = t_upd;
     }
 }
 

@@ -15,6 +15,10 @@ struct CgSeqState {
     int first, done, status, error, replace, pending_conv;
     unsigned counter;  // last-block arrival counter
     unsigned device_error;  // DeviceError bits (a grid barrier of the resident solve gave up)
+    // resident solve, as seen by block 0 (ns): [0] halo and direction update,
+    // [1] operator pass, [2] grid barriers and reductions, [3] update and
+    // residual replacements
+    unsigned long long phase_ns[4];
 };
 
 struct Pcg3dResPlan;

@@ -36,7 +36,12 @@ def test_resident_pcg_against_fp64_oracle(oracle, monkeypatch, shape):
     for a, b in zip(reps, ref_reps):
         assert a.pressure_status == _abi.LINEAR_CONVERGED
         assert a.pressure_true_relative_residual <= 1.0e-8 * 1.0001
-        assert abs(a.pressure_iterations - b.pressure_iterations) <= max(3, b.pressure_iterations // 50)
+        # MIXED accepts convergence only at an FP64 residual replacement
+        # (every 50 iterations) and its FP32 vectors drift from the FP64
+        # recurrence, so it may take up to one replacement interval plus a
+        # quarter more iterations than the FP64 oracle, never fewer.
+        assert b.pressure_iterations - 3 <= a.pressure_iterations
+        assert a.pressure_iterations <= b.pressure_iterations + 50 + b.pressure_iterations // 4
     assert _vel_rel(fields, {fid: ref.get(fid) for fid, _ in FIELDS[:3]}) <= MIXED_TOL
 
 
