@@ -23,6 +23,23 @@
 // of the returned pressure. Every block computes every reduction in the
 // same fixed order, so all blocks take the same decisions.
 //
+// Two forms share the tile layout. The two-reduction form above serves
+// every stop rule. For the L2 stop rule the single-reduction form
+// (pcg3d_res1_kernel) needs one grid barrier per iteration: the halo keeps
+// its own copy of r (in the registers of the threads that own the halo
+// cells), the faces of q = A d are exchanged instead of those of r, and one
+// reduction carries (r,r), (r,z), (d,q), (q,q), (q,Mq), (q,r), (q,z) and
+// max|r| of the same iteration. alpha = (r,z)/(d,q) uses the directly summed
+// (r,z); the (r,z) and ||r||^2 of the next residual r - alpha q come from
+// the exact expansions (r,z) - 2 alpha (q,z) + alpha^2 (q,Mq) and
+// (r,r) - 2 alpha (q,r) + alpha^2 (q,q) of the summed products, so beta and
+// the stop test are decided where the reference's PCG decides them, and the
+// next reduction sums (r,z) directly again (no recurrence accumulates). The
+// vector updates are FP32 fused multiply-adds with alpha rounded to FP32,
+// the same alpha for the increment and the residual (so the two stay
+// consistent); dots and scalars stay FP64, each product formed from the
+// FP32 factors widened once per cell.
+//
 // Every grid-barrier wait is bounded; a barrier that gives up sets the
 // timeout bit in CgSeqState::device_error and the blocks return.
 #include <cuda_runtime.h>
@@ -44,7 +61,7 @@ constexpr int kResBlock = 512;            // threads; each owns columns (tx, ty)
 constexpr int kCols = RX * RY / kResBlock;  // columns per thread
 constexpr int kResMaxTz = 16;
 constexpr int HX = RX + 2, HY = RY + 2;
-constexpr int kResSlots = 4;
+constexpr int kResSlots = 8;  // partial sums per block and reduction (7 sums and a maximum at most)
 // face values per thread: two 32 x 32 z-faces and four 32 x tz side faces
 constexpr int kHaloPer = (2 * RX * RY + 4 * RX * kResMaxTz + kResBlock - 1) / kResBlock;
 
@@ -77,6 +94,7 @@ struct ResCtx {
 // Every block obtains the same bits. Returns false when the barrier failed.
 template <int NS, bool MAX>
 __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &mx) {
+    static_assert(NS + (MAX ? 1 : 0) <= kResSlots && NS + (MAX ? 1 : 0) <= kResBlock / 32, "reduction width");
     const unsigned long long t0 = gtimer();
     block_reduce_n<kResBlock, NS, MAX>(v, mx, c.red);
     const int nb = gridDim.x;
@@ -88,28 +106,21 @@ __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &
         if (MAX) P[blockIdx.x * kResSlots + NS] = mx;
     }
     if (!res_sync(c.a)) return false;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-#pragma unroll
-        for (int k = 0; k < NS; ++k) {
-            double t = 0.0;
-            for (int b = lane; b < nb; b += 32) t += __ldcg(P + b * kResSlots + k);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-            v[k] = t;
+    // warp k sums value k over the blocks (every block in the same order)
+    const int wk = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (wk < NS + (MAX ? 1 : 0)) {
+        const bool is_max = MAX && wk == NS;
+        double t = 0.0;
+        for (int b = lane; b < nb; b += 32) {
+            const double p = __ldcg(P + b * kResSlots + wk);
+            t = is_max ? fmax(t, p) : t + p;
         }
-        if (MAX) {
-            double t = 0.0;
-            for (int b = lane; b < nb; b += 32) t = fmax(t, __ldcg(P + b * kResSlots + NS));
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
-            mx = t;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double p = __shfl_xor_sync(0xffffffffu, t, o);
+            t = is_max ? fmax(t, p) : t + p;
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NS; ++k) c.red[k] = v[k];
-            if (MAX) c.red[NS] = mx;
-        }
+        if (lane == 0) c.red[wk] = t;
     }
     __syncthreads();
 #pragma unroll
@@ -127,7 +138,7 @@ __device__ __forceinline__ float make_d(float r, float dold, float idg, bool pin
     return first ? z : __fmaf_rn(beta, dold, z);
 }
 
-__global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_constant__ ResArgs a) {
+__global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_constant__ ResArgs a) {
     extern __shared__ float smem[];
     __shared__ double red[8 * (kResBlock / 32)];
     __shared__ float idgf[27];
@@ -218,7 +229,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
 #pragma unroll
             for (int kk = 0; kk < kResMaxTz; ++kk) {
                 if (kk >= kz) continue;
-                if (face_col[h] || kk == 0 || kk == kz - 1) a.rface[col[h] + (k0 + kk) * a.nxy] = r[h][kk];
+                if (face_col[h] || kk == 0 || kk == kz - 1) a.face0[col[h] + (k0 + kk) * a.nxy] = r[h][kk];
             }
         }
     };
@@ -286,7 +297,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
             const int cc = (gk * a.ny + gj) * a.nx + gi;
             hslot[u] = ((kk + 1) * HY + yy + 1) * HX + xx + 1;
             hcls[u] = cc == 0 ? -1 : 9 * rmiss(gi, a.nx) + 3 * rmiss(gj, a.ny) + rmiss(gk, a.nz);
-            hv[u] = __ldcg(a.rface + cc);
+            hv[u] = __ldcg(a.face0 + cc);
         }
 #pragma unroll
         for (int u = 0; u < kHaloPer; ++u) {
@@ -426,6 +437,337 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res_kernel(const __grid_co
     }
 }
 
+
+// Single-reduction form for the L2 stop rule (see the file comment).
+__global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_constant__ ResArgs a) {
+    extern __shared__ float smem[];
+    __shared__ double red[8 * (kResBlock / 32)];
+    __shared__ float idgf[27];
+    const int tz_full = a.tz;
+    float *dsm = smem;                                      // (tz + 2) x HY x HX
+    float *dxs = smem + (size_t)HX * HY * (tz_full + 2);   // tz x RY x RX
+    float *qs = dxs + (size_t)RX * RY * tz_full;           // tz x RY x RX
+    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull};
+    unsigned long long t_halo = 0, t_op = 0, t_upd = 0;
+    const int b = blockIdx.x;
+    const int i0 = (b % a.ntx) * RX, j0 = ((b / a.ntx) % a.nty) * RY, k0 = (b / (a.ntx * a.nty)) * a.tz;
+    const int kz = min(a.tz, a.nz - k0);
+    const int tx = threadIdx.x & 31;
+    int ty[kCols], col[kCols], cls_xy[kCols];
+    bool in[kCols], pcol[kCols], face_col[kCols];
+    float wxy[kCols][4];  // x-, x+, y-, y+ operator weights (0 at a wall)
+#pragma unroll
+    for (int h = 0; h < kCols; ++h) {
+        ty[h] = (threadIdx.x >> 5) + h * (kResBlock / 32);
+        const int i = i0 + tx, j = j0 + ty[h];
+        in[h] = i < a.nx && j < a.ny;
+        col[h] = in[h] ? j * a.nx + i : 0;
+        pcol[h] = in[h] && col[h] == 0;
+        face_col[h] = tx == 0 || tx == RX - 1 || ty[h] == 0 || ty[h] == RY - 1;
+        cls_xy[h] = in[h] ? 9 * rmiss(i, a.nx) + 3 * rmiss(j, a.ny) : 0;
+        wxy[h][0] = in[h] && i > 0 ? a.wx : 0.f;
+        wxy[h][1] = in[h] && i + 1 < a.nx ? a.wx : 0.f;
+        wxy[h][2] = in[h] && j > 0 ? a.wy : 0.f;
+        wxy[h][3] = in[h] && j + 1 < a.ny ? a.wy : 0.f;
+    }
+    auto own = [&](int h, int kk) { return ((kk + 1) * HY + ty[h] + 1) * HX + tx + 1; };
+    auto loc = [&](int h, int kk) { return (kk * RY + ty[h]) * RX + tx; };
+
+    // The halo cells this thread keeps: shared-memory slot | class << 16
+    // (class 27: the pinned cell), global index; -1 when none.
+    int hpk[kHaloPer], hcc[kHaloPer];
+    const int nhalo = 2 * RX * RY + 4 * RX * kz;
+#pragma unroll
+    for (int u = 0; u < kHaloPer; ++u) {
+        const int s = threadIdx.x + u * kResBlock;
+        hpk[u] = -1;
+        hcc[u] = 0;
+        if (s >= nhalo) continue;
+        int xx, yy, kk;
+        if (s < 2 * RX * RY) {
+            const int t = s & (RX * RY - 1);
+            xx = t & 31; yy = t >> 5; kk = s < RX * RY ? -1 : kz;
+        } else {
+            const int t = s - 2 * RX * RY, f = t / (RX * kz), w = t - f * (RX * kz);
+            const int p = w & 31, q = w >> 5;
+            if (f < 2) { xx = p; yy = f == 0 ? -1 : RY; kk = q; }
+            else { yy = p; xx = f == 2 ? -1 : RX; kk = q; }
+        }
+        const int gi = i0 + xx, gj = j0 + yy, gk = k0 + kk;
+        if (gi < 0 || gi >= a.nx || gj < 0 || gj >= a.ny || gk < 0 || gk >= a.nz) continue;
+        const int cc = (gk * a.ny + gj) * a.nx + gi;
+        const int cls = cc == 0 ? 27 : 9 * rmiss(gi, a.nx) + 3 * rmiss(gj, a.ny) + rmiss(gk, a.nz);
+        hpk[u] = (((kk + 1) * HY + yy + 1) * HX + xx + 1) | (cls << 16);
+        hcc[u] = cc;
+    }
+
+    if (threadIdx.x < 27) idgf[threadIdx.x] = a.inv_diag_f[threadIdx.x];
+    for (int s = threadIdx.x; s < HX * HY * (tz_full + 2); s += kResBlock) dsm[s] = 0.f;
+    for (int s = threadIdx.x; s < RX * RY * tz_full; s += kResBlock) dxs[s] = 0.f;
+    __syncthreads();
+
+    float r[kCols][kResMaxTz];
+    float hr[kHaloPer];
+#pragma unroll
+    for (int h = 0; h < kCols; ++h)
+#pragma unroll
+        for (int kk = 0; kk < kResMaxTz; ++kk) r[h][kk] = 0.f;
+#pragma unroll
+    for (int u = 0; u < kHaloPer; ++u) hr[u] = 0.f;
+    int fr = 0;  // face exchanges so far; exchange f uses buffer f & 1
+    auto face = [&](int f) { return (f & 1) ? a.face1 : a.face0; };
+
+    // r = b - A x in FP64 (b = -rhs) on the tile, rounded to FP32, with the
+    // sums of the rounded r; with `final_pass` only the FP64 sum of (b - A x)^2.
+    auto residual = [&](double &srr, double &srz, double &smax, bool final_pass) {
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+            const double wxm = wxy[h][0] != 0.f ? a.ix2 : 0.0, wxp = wxy[h][1] != 0.f ? a.ix2 : 0.0;
+            const double wym = wxy[h][2] != 0.f ? a.iy2 : 0.0, wyp = wxy[h][3] != 0.f ? a.iy2 : 0.0;
+#pragma unroll
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                const int k = k0 + kk;
+                const int cc = col[h] + k * a.nxy;
+                const bool pin = pcol[h] && k == 0;
+                auto xv = [&](int idx) -> double { return idx == 0 ? 0.0 : __ldcg(a.x + idx); };
+                const double cur = pin ? 0.0 : __ldcg(a.x + cc);
+                const double wzm = k > 0 ? a.iz2 : 0.0, wzp = k + 1 < a.nz ? a.iz2 : 0.0;
+                const double xm = wxm != 0.0 ? xv(cc - 1) : 0.0, xp = wxp != 0.0 ? xv(cc + 1) : 0.0;
+                const double ym = wym != 0.0 ? xv(cc - a.nx) : 0.0, yp = wyp != 0.0 ? xv(cc + a.nx) : 0.0;
+                const double zm = k > 0 ? xv(cc - a.nxy) : 0.0, zp = k + 1 < a.nz ? xv(cc + a.nxy) : 0.0;
+                const double ax = (wxm + wxp + wym + wyp + wzm + wzp) * cur -
+                                  (wxm * xm + wxp * xp + wym * ym + wyp * yp + wzm * zm + wzp * zp);
+                const double t = pin ? 0.0 : -__ldg(a.rhs + cc) - ax;
+                if (final_pass) {
+                    srr += t * t;
+                    continue;
+                }
+                const float rv = float(t);
+                r[h][kk] = rv;
+                const double rd = double(rv);
+                srr += rd * rd;
+                srz += rd * rd * (pin ? 1.0 : a.inv_diag[cls_xy[h] + rmiss(k, a.nz)]);
+                smax = fmax(smax, fabs(rd));
+            }
+        }
+    };
+    // The tile's face values of r, then (after the next grid barrier) the
+    // halo's r from the neighbours' faces.
+    auto publish_r = [&](float *fb) {
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+#pragma unroll
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                if (face_col[h] || kk == 0 || kk == kz - 1) fb[col[h] + (k0 + kk) * a.nxy] = r[h][kk];
+            }
+        }
+    };
+    auto fetch_halo_r = [&](const float *fb) {
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u)
+            if (hpk[u] >= 0) hr[u] = __ldcg(fb + hcc[u]);
+    };
+    auto fold = [&]() {
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+            for (int kk = 0; kk < kz; ++kk) {
+                const int cc = col[h] + (k0 + kk) * a.nxy;
+                if (cc == 0) a.x[0] = 0.0;
+                else a.x[cc] += double(dxs[loc(h, kk)]);
+                dxs[loc(h, kk)] = 0.f;
+            }
+        }
+    };
+
+    // ---- initial residual and its halo ----
+    if (b == 0 && threadIdx.x == 0) a.x[0] = 0.0;
+    if (!res_sync(a)) return;
+    double s0[2] = {0.0, 0.0};
+    double m0 = 0.0;
+    residual(s0[0], s0[1], m0, false);
+    publish_r(face(fr));
+    if (!grid_reduce<2, true>(c, s0, m0)) return;
+    fetch_halo_r(face(fr));
+    ++fr;
+    const double initial_l2 = sqrt(s0[0]);
+    const double initial = initial_l2;
+    const double threshold = a.atol + a.rtol * initial;
+    double residual_v = initial, beta = 0.0;
+    bool first = true;
+    long long iterations = 0;
+    int status = initial <= threshold ? FLURSYS_LINEAR_CONVERGED : FLURSYS_LINEAR_MAX_ITERATIONS;
+    int error = 0;
+    bool done = status == FLURSYS_LINEAR_CONVERGED || a.max_iters <= 0;
+
+    while (!done) {
+        // ---- d = z + beta d_old on the tile and its halo ----
+        const unsigned long long t0 = gtimer();
+        const float fb = float(beta);
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) {
+            if (hpk[u] < 0) continue;
+            const int sl = hpk[u] & 0xffff, cls = hpk[u] >> 16;
+            dsm[sl] = make_d(hr[u], dsm[sl], idgf[cls == 27 ? 0 : cls], cls == 27, first, fb);
+        }
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+#pragma unroll
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                const int k = k0 + kk;
+                const int sl = own(h, kk);
+                dsm[sl] = make_d(r[h][kk], dsm[sl], idgf[cls_xy[h] + rmiss(k, a.nz)], pcol[h] && k == 0, first, fb);
+            }
+        }
+        __syncthreads();
+        const unsigned long long t1 = gtimer();
+        t_halo += t1 - t0;
+        // ---- q = A d on the tile, q's faces out, and the sums ----
+        // S: (r,r), (r,z), (d,q), (q,q), (q,Mq), (q,r), (q,z)
+        double S[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        float rmax = 0.f;
+        float *fq = face(fr);
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+            const float *w = wxy[h];
+            double crr = 0.0, cqq = 0.0, cqr = 0.0, cdq = 0.0;  // the column's cells
+            double err = 0.0, eqq = 0.0, eqr = 0.0;              // its cells on a z wall
+            float below = dsm[own(h, -1)], cur = dsm[own(h, 0)];
+#pragma unroll
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                const int k = k0 + kk;
+                const int sp = own(h, kk);
+                const float above = dsm[sp + HX * HY];
+                const float wzm = k > 0 ? a.wz : 0.f, wzp = k + 1 < a.nz ? a.wz : 0.f;
+                float ax = (w[0] + w[1] + w[2] + w[3] + wzm + wzp) * cur -
+                           (w[0] * dsm[sp - 1] + w[1] * dsm[sp + 1] + w[2] * dsm[sp - HX] + w[3] * dsm[sp + HX] +
+                            wzm * below + wzp * above);
+                if (pcol[h] && k == 0) ax = cur;  // identity row of the pinned cell
+                qs[loc(h, kk)] = ax;
+                if (face_col[h] || kk == 0 || kk == kz - 1) fq[col[h] + k * a.nxy] = ax;
+                const double rd = double(r[h][kk]), qd = double(ax), dd = double(cur);
+                const double rr = rd * rd, qq = qd * qd, qr = qd * rd;
+                crr += rr; cqq += qq; cqr += qr;
+                cdq = fma(dd, qd, cdq);
+                if (k == 0 || k == a.nz - 1) { err += rr; eqq += qq; eqr += qr; }
+                rmax = fmaxf(rmax, fabsf(r[h][kk]));
+                below = cur;
+                cur = above;
+            }
+            // Jacobi weights: the column's class inside, its z-wall class at k = 0, nz - 1
+            const double wm = a.inv_diag[cls_xy[h]], we = a.inv_diag[cls_xy[h] + 1] - wm;
+            S[0] += crr;
+            S[1] += wm * crr + we * err;
+            S[2] += cdq;
+            S[3] += cqq;
+            S[4] += wm * cqq + we * eqq;
+            S[5] += cqr;
+            S[6] += wm * cqr + we * eqr;
+        }
+        double mx = double(rmax);
+        const unsigned long long t2 = gtimer();
+        t_op += t2 - t1;
+        if (!grid_reduce<7, true>(c, S, mx)) return;
+        const unsigned long long t3 = gtimer();
+        const double rz = S[1], dq = S[2];
+        if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(rz / dq)) {
+            error = FLURSYS_ERR_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / dq;
+        const double rr_next = S[0] - 2.0 * alpha * S[5] + alpha * alpha * S[3];
+        double rz_next = S[1] - 2.0 * alpha * S[6] + alpha * alpha * S[4];
+        // ---- dx += alpha d, r -= alpha q on the tile and the halo ----
+        const float af = float(alpha);
+        const float *fqr = face(fr);
+        ++fr;
+        float hq[kHaloPer];
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) hq[u] = hpk[u] >= 0 ? __ldcg(fqr + hcc[u]) : 0.f;
+#pragma unroll
+        for (int h = 0; h < kCols; ++h) {
+            if (!in[h]) continue;
+#pragma unroll
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                const int l = loc(h, kk);
+                dxs[l] = __fmaf_rn(af, dsm[own(h, kk)], dxs[l]);
+                r[h][kk] = __fmaf_rn(-af, qs[l], r[h][kk]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) hr[u] = __fmaf_rn(-af, hq[u], hr[u]);
+        iterations += 1;
+        double res = sqrt(fmax(rr_next, 0.0));
+        residual_v = res;
+        if (!isfinite(res)) {
+            error = FLURSYS_ERR_NON_FINITE;
+            break;
+        }
+        bool conv = res <= threshold;
+        if (conv || (iterations % a.replace_every) == 0) {
+            // ---- FP64 residual replacement ----
+            fold();
+            if (!res_sync(a)) return;
+            double s3[2] = {0.0, 0.0};
+            double m3 = 0.0;
+            residual(s3[0], s3[1], m3, false);
+            publish_r(face(fr));
+            if (!grid_reduce<2, true>(c, s3, m3)) return;
+            fetch_halo_r(face(fr));
+            ++fr;
+            res = sqrt(s3[0]);
+            residual_v = res;
+            if (!isfinite(res)) {
+                error = FLURSYS_ERR_NON_FINITE;
+                break;
+            }
+            conv = res <= threshold;
+            rz_next = s3[1];
+        }
+        t_upd += gtimer() - t3;
+        if (conv) {
+            status = FLURSYS_LINEAR_CONVERGED;
+            break;
+        }
+        if (fabs(rz) < 1.0e-30 || iterations >= a.max_iters) break;
+        beta = rz_next / rz;
+        first = false;
+    }
+    // ---- fold a pending increment, then the FP64 ||b - A x||_2 ----
+    if (status != FLURSYS_LINEAR_CONVERGED) fold();
+    if (!res_sync(a)) return;
+    double st[1] = {0.0};
+    double d0 = 0.0, d1 = 0.0;
+    residual(st[0], d0, d1, true);
+    double unused = 0.0;
+    if (!grid_reduce<1, false>(c, st, unused)) return;
+    if (b == 0 && threadIdx.x == 0) {
+        CgSeqState *w = a.st;
+        w->error = error;
+        w->status = status;
+        w->iterations = iterations;
+        w->initial = initial;
+        w->initial_l2 = initial_l2;
+        w->residual = residual_v;
+        w->threshold = threshold;
+        w->true_l2 = sqrt(st[0]);
+        w->done = 1;
+        w->phase_ns[0] = t_halo;
+        w->phase_ns[1] = t_op;
+        w->phase_ns[2] = c.t_reduce;
+        w->phase_ns[3] = t_upd;
+    }
+}
+
 }  // namespace
 
 bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
@@ -449,10 +791,13 @@ bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
     a.ntz = (a.nz + a.tz - 1) / a.tz;
     plan.grid = (int)(cols * a.ntz);
     plan.smem = res_smem_bytes(a.tz);
-    if (cudaFuncSetAttribute((const void *)pcg3d_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)plan.smem) != cudaSuccess)
+    // one reduction per iteration for the L2 stop rule (FLURSYS_PCG_RESIDENT=2
+    // keeps the two-reduction form)
+    plan.single = args.stop_rule == FLURSYS_STOP_REL_L2 && !(env && std::strcmp(env, "2") == 0);
+    plan.kernel = plan.single ? (const void *)pcg3d_res1_kernel : (const void *)pcg3d_res2_kernel;
+    if (cudaFuncSetAttribute(plan.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) != cudaSuccess)
         return false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg3d_res_kernel, kResBlock, plan.smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, kResBlock, plan.smem) != cudaSuccess ||
         per_sm < 1 || plan.grid > per_sm * sms)
         return false;
     a.ix2 = args.ix2; a.iy2 = args.iy2; a.iz2 = args.iz2;
@@ -466,7 +811,8 @@ bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
     }
     a.x = args.x;
     a.rhs = args.rhs;
-    a.rface = static_cast<float *>(args.r);
+    a.face0 = static_cast<float *>(args.r);
+    a.face1 = static_cast<float *>(args.q);
     a.stop_rule = args.stop_rule;
     a.tol = args.tol; a.atol = args.atol; a.rtol = args.rtol;
     a.max_iters = args.max_iters;
@@ -491,8 +837,7 @@ cudaError_t pcg3d_res_launch(const Pcg3dResPlan &plan, CgSeqState *state, cudaSt
     if (e == cudaSuccess) e = cudaMemsetAsync(state, 0, sizeof(CgSeqState), stream);
     void *params[] = {&a};
     if (e == cudaSuccess)
-        e = cudaLaunchCooperativeKernel((const void *)pcg3d_res_kernel, dim3(plan.grid), dim3(kResBlock), params,
-                                        plan.smem, stream);
+        e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.grid), dim3(kResBlock), params, plan.smem, stream);
     return e;
 }
 

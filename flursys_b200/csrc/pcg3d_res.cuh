@@ -22,7 +22,7 @@ struct ResArgs {
     double inv_diag[27];   // the same weights widened to FP64 (for r.z)
     double *x;             // FP64 pressure, updated in place
     const double *rhs;     // the system is A x = -rhs
-    float *rface;          // n floats: residual faces exchanged between tiles
+    float *face0, *face1;  // n floats each: tile faces exchanged between tiles (alternating buffers)
     double *partials;      // 2 * grid * 4 partial sums
     GridBarrier *bar;
     int barrier_extra;     // arrivals beyond the grid (an injected barrier fault; 0 otherwise)
@@ -37,14 +37,16 @@ struct ResArgs {
 struct Pcg3dResPlan {
     bool enabled = false;
     ResArgs args{};
+    bool single = false;             // single-reduction form (L2 stop rule)
+    const void *kernel = nullptr;    // the launched kernel
     int grid = 0;
     size_t smem = 0;
     double *partials = nullptr;
     GridBarrier *barrier = nullptr;
 };
 
-// Sets up the resident solve for `args` (MIXED work vectors: args.r is the
-// FP32 face-exchange buffer); false when the grid does not fit one tile per
+// Sets up the resident solve for `args` (MIXED work vectors: args.r and
+// args.q are the FP32 face-exchange buffers); false when the grid does not fit one tile per
 // SM, the device cannot hold a tile, or FLURSYS_PCG_RESIDENT=0.
 bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device);
 // One solve; the result is written to *state (CgSeqState fields error,

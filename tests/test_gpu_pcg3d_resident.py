@@ -1,8 +1,16 @@
 """3D pressure PCG, MIXED precision, with the solver state resident on the
 chip (one cooperative launch per solve; the default where the grid's
 32 x 32 x tz tiles fit one per SM): against the FP64 oracle, against the
-graph-driven two-launch PCG (FLURSYS_PCG_RESIDENT=0), at its iteration cap,
-and with an injected grid-barrier fault."""
+graph-driven two-launch PCG (FLURSYS_PCG_RESIDENT=0), single-reduction form
+(the default for the L2 stop rule) against the two-reduction form
+(FLURSYS_PCG_RESIDENT=2, and every other stop rule), at its iteration cap,
+and with an injected grid-barrier fault.
+
+Iteration counts of two MIXED solves that differ only in rounding (another
+summation order of a dot product, alpha rounded to FP32 for the vector
+updates) are compared within a few percent: near its attainable accuracy
+the FP32 recurrence amplifies such differences, and convergence is accepted
+only at an FP64 residual replacement."""
 import numpy as np
 import pytest
 
@@ -15,11 +23,19 @@ from .test_gpu_pcg3d_variants import _vel_rel
 pytestmark = pytest.mark.gpu
 
 
-def _run(oracle, shape, steps, monkeypatch, resident=True, rtol=1e-8, max_iters=20000):
-    if not resident:
+def _close_iterations(a, b):
+    return abs(a - b) <= 3 + max(a, b) // 25
+
+
+def _run(oracle, shape, steps, monkeypatch, resident=True, rtol=1e-8, max_iters=20000, rule=_abi.STOP_REL_L2):
+    if resident is False:
         monkeypatch.setenv("FLURSYS_PCG_RESIDENT", "0")
-    cfg = cfg3d(oracle, *shape, rtol=rtol, precision=_abi.PRECISION_MIXED)
+    elif resident == "two":
+        monkeypatch.setenv("FLURSYS_PCG_RESIDENT", "2")
+    cfg = cfg3d(oracle, *shape, rtol=rtol, precision=_abi.PRECISION_MIXED, rule=rule)
     cfg.pressure_max_iters = max_iters
+    if rule != _abi.STOP_REL_L2:
+        cfg.pressure_tolerance = rtol
     gpu = _Handle(cfg)
     reps = [gpu.step(1) for _ in range(steps)]
     fields = {fid: gpu.download(fid) for fid, _ in FIELDS}
@@ -52,8 +68,34 @@ def test_resident_and_graph_paths_agree(oracle, monkeypatch):
     for a, b in zip(res, seq):
         assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
         assert b.pressure_iterations > 100
-        assert abs(a.pressure_iterations - b.pressure_iterations) <= 2
+        assert _close_iterations(a.pressure_iterations, b.pressure_iterations)
     assert _vel_rel(f1, f2) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("shape", [(48, 40, 32), (64, 96, 50)])
+def test_single_and_two_reduction_forms_agree(oracle, monkeypatch, shape):
+    one, f1, g1 = _run(oracle, shape, 3, monkeypatch)
+    two, f2, g2 = _run(oracle, shape, 3, monkeypatch, resident="two")
+    assert g1.solve_kind() == g2.solve_kind() == _abi.SOLVE_RESIDENT
+    for a, b in zip(one, two):
+        assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
+        assert a.pressure_true_relative_residual <= 1.0e-8 * 1.0001
+        assert _close_iterations(a.pressure_iterations, b.pressure_iterations)
+    assert _vel_rel(f1, f2) <= MIXED_TOL
+
+
+def test_max_norm_stop_rule_runs_resident_two_reduction_form(oracle, monkeypatch):
+    shape = (40, 36, 28)
+    cfg = cfg3d(oracle, *shape, rule=_abi.STOP_ABS_INF)
+    cfg.pressure_tolerance = 1e-7
+    ref = oracle.OracleSolver(cfg)
+    ref_reps = [ref.step(1) for _ in range(3)]
+    reps, fields, gpu = _run(oracle, shape, 3, monkeypatch, rtol=1e-7, rule=_abi.STOP_ABS_INF)
+    assert gpu.solve_kind() == _abi.SOLVE_RESIDENT
+    for a, b in zip(reps, ref_reps):
+        assert a.pressure_status == _abi.LINEAR_CONVERGED
+        assert b.pressure_iterations - 3 <= a.pressure_iterations <= b.pressure_iterations + 50 + b.pressure_iterations // 4
+    assert _vel_rel(fields, {fid: ref.get(fid) for fid, _ in FIELDS[:3]}) <= MIXED_TOL
 
 
 def test_resident_iteration_cap(oracle, monkeypatch):
@@ -84,7 +126,7 @@ def test_staged_operand_pass_matches_register_pass(oracle, monkeypatch, shape):
     pipe, f1, _ = _run(oracle, shape, 3, monkeypatch, resident=False)
     for a, b in zip(pipe, vec):
         assert a.pressure_status == b.pressure_status == _abi.LINEAR_CONVERGED
-        assert abs(a.pressure_iterations - b.pressure_iterations) <= 2
+        assert _close_iterations(a.pressure_iterations, b.pressure_iterations)
     assert _vel_rel(f1, f2) <= MIXED_TOL
     ref = oracle.OracleSolver(cfg3d(oracle, *shape, rtol=1e-8))
     for _ in range(3):
