@@ -62,6 +62,8 @@ constexpr int kCols = RX * RY / kResBlock;  // columns per thread
 constexpr int kResMaxTz = 16;
 constexpr int HX = RX + 2, HY = RY + 2;
 constexpr int kResSlots = 8;  // partial sums per block and reduction (7 sums and a maximum at most)
+constexpr int kResMaxBlocks = 160;                    // one block per SM
+constexpr int kResPerLane = (kResMaxBlocks + 31) / 32;  // partials per lane in a grid reduction
 // face values per thread: two 32 x 32 z-faces and four 32 x tz side faces
 constexpr int kHaloPer = (2 * RX * RY + 4 * RX * kResMaxTz + kResBlock - 1) / kResBlock;
 
@@ -77,9 +79,42 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-// Grid barrier of the resident solve; a failure is recorded in the state.
+// Grid barrier of the resident solve: one arrival ticket per block on a
+// counter that only grows (cleared before each launch); barrier number t
+// is complete when the counter reaches (t + 1) * nblocks, so the arrival
+// is a single atomic and the wait polls the same word. The wait is
+// bounded; a failure sets the timeout bit in the barrier's error word and
+// in the state, and every block leaves at its next barrier.
 __device__ __forceinline__ bool res_sync(const ResArgs &a) {
-    return grid_sync_report(a.bar, gridDim.x + (unsigned)a.barrier_extra, &a.st->device_error, a.spin_limit);
+    const unsigned nblocks = gridDim.x + (unsigned)a.barrier_extra;
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        unsigned *cnt = &a.bar->count;
+        unsigned old;
+        asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
+        const unsigned target = (old / nblocks + 1u) * nblocks;
+        int ok = 1;
+        long long spins = 0;
+        for (;;) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(cnt) : "memory");
+            if ((int)(cur - target) >= 0) break;
+            if ((++spins & 63) == 0) {
+                const unsigned err = *(volatile unsigned *)&a.bar->error;
+                if (err != 0u || spins > a.spin_limit) {
+                    atomicOr(&a.bar->error, (unsigned)kDevErrBarrierTimeout);
+                    atomicOr(&a.st->device_error, (unsigned)kDevErrBarrierTimeout);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
 }
 
 struct ResCtx {
@@ -110,11 +145,16 @@ __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &
     const int wk = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (wk < NS + (MAX ? 1 : 0)) {
         const bool is_max = MAX && wk == NS;
-        double t = 0.0;
-        for (int b = lane; b < nb; b += 32) {
-            const double p = __ldcg(P + b * kResSlots + wk);
-            t = is_max ? fmax(t, p) : t + p;
+        // every partial this lane needs is requested before the first is used
+        double p[kResPerLane];
+#pragma unroll
+        for (int u = 0; u < kResPerLane; ++u) {
+            const int b = lane + 32 * u;
+            p[u] = b < nb ? __ldcg(P + b * kResSlots + wk) : 0.0;
         }
+        double t = 0.0;
+#pragma unroll
+        for (int u = 0; u < kResPerLane; ++u) t = is_max ? fmax(t, p[u]) : t + p[u];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double p = __shfl_xor_sync(0xffffffffu, t, o);
@@ -790,6 +830,7 @@ bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
     if (a.tz > kResMaxTz) return false;
     a.ntz = (a.nz + a.tz - 1) / a.tz;
     plan.grid = (int)(cols * a.ntz);
+    if (plan.grid > kResMaxBlocks) return false;
     plan.smem = res_smem_bytes(a.tz);
     // one reduction per iteration for the L2 stop rule (FLURSYS_PCG_RESIDENT=2
     // keeps the two-reduction form)
