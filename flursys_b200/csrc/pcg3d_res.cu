@@ -127,11 +127,11 @@ struct ResCtx {
 
 // Sums NS values (and, with MAX, the maximum of one more) over the grid.
 // Every block obtains the same bits. Returns false when the barrier failed.
-template <int NS, bool MAX>
+template <int BLK, int NS, bool MAX>
 __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &mx) {
-    static_assert(NS + (MAX ? 1 : 0) <= kResSlots && NS + (MAX ? 1 : 0) <= kResBlock / 32, "reduction width");
+    static_assert(NS + (MAX ? 1 : 0) <= kResSlots && NS + (MAX ? 1 : 0) <= BLK / 32, "reduction width");
     const unsigned long long t0 = gtimer();
-    block_reduce_n<kResBlock, NS, MAX>(v, mx, c.red);
+    block_reduce_n<BLK, NS, MAX>(v, mx, c.red);
     const int nb = gridDim.x;
     double *P = c.a.partials + (size_t)(c.round & 1) * nb * kResSlots;
     ++c.round;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
     double smax = 0.0;
     residual(sums[0], sums[1], smax, false);
     publish();
-    if (!grid_reduce<2, true>(c, sums, smax)) return;
+    if (!grid_reduce<kResBlock, 2, true>(c, sums, smax)) return;
     const bool l2 = a.stop_rule == FLURSYS_STOP_REL_L2;
     auto stop_ok = [&](double res, double thr) { return l2 ? res <= thr : res < thr; };
     const double initial_l2 = sqrt(sums[0]);
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
         }
         double unused = 0.0;
         t_op += gtimer() - t1;
-        if (!grid_reduce<1, false>(c, sdq, unused)) return;
+        if (!grid_reduce<kResBlock, 1, false>(c, sdq, unused)) return;
         const unsigned long long t2 = gtimer();
         const double dq = sdq[0];
         if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(rz_old / dq)) {
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
         }
         publish();
         t_upd += gtimer() - t2;
-        if (!grid_reduce<2, true>(c, s2, mx)) return;
+        if (!grid_reduce<kResBlock, 2, true>(c, s2, mx)) return;
         iterations += 1;
         double res = l2 ? sqrt(s2[0]) : mx;
         residual_v = res;
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
             double m3 = 0.0;
             residual(s3[0], s3[1], m3, false);
             publish();
-            if (!grid_reduce<2, true>(c, s3, m3)) return;
+            if (!grid_reduce<kResBlock, 2, true>(c, s3, m3)) return;
             res = l2 ? sqrt(s3[0]) : m3;
             residual_v = res;
             if (!isfinite(res)) {
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
     double d0 = 0.0, d1 = 0.0;
     residual(st[0], d0, d1, true);
     double unused = 0.0;
-    if (!grid_reduce<1, false>(c, st, unused)) return;
+    if (!grid_reduce<kResBlock, 1, false>(c, st, unused)) return;
     if (b == 0 && threadIdx.x == 0) {
         CgSeqState *w = a.st;
         w->error = error;
@@ -479,9 +479,12 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
 
 
 // Single-reduction form for the L2 stop rule (see the file comment).
-__global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_constant__ ResArgs a) {
+template <int BLK, bool COL32>
+__global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constant__ ResArgs a) {
+    constexpr int kC = RX * RY / BLK;                                       // columns per thread
+    constexpr int kHP = (2 * RX * RY + 4 * RX * kResMaxTz + BLK - 1) / BLK;  // halo cells per thread
     extern __shared__ float smem[];
-    __shared__ double red[8 * (kResBlock / 32)];
+    __shared__ double red[8 * (BLK / 32)];
     __shared__ float idgf[27];
     const int tz_full = a.tz;
     float *dsm = smem;                                      // (tz + 2) x HY x HX
@@ -493,12 +496,12 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     const int i0 = (b % a.ntx) * RX, j0 = ((b / a.ntx) % a.nty) * RY, k0 = (b / (a.ntx * a.nty)) * a.tz;
     const int kz = min(a.tz, a.nz - k0);
     const int tx = threadIdx.x & 31;
-    int ty[kCols], col[kCols], cls_xy[kCols];
-    bool in[kCols], pcol[kCols], face_col[kCols];
-    float wxy[kCols][4];  // x-, x+, y-, y+ operator weights (0 at a wall)
+    int ty[kC], col[kC], cls_xy[kC];
+    bool in[kC], pcol[kC], face_col[kC];
+    float wxy[kC][4];  // x-, x+, y-, y+ operator weights (0 at a wall)
 #pragma unroll
-    for (int h = 0; h < kCols; ++h) {
-        ty[h] = (threadIdx.x >> 5) + h * (kResBlock / 32);
+    for (int h = 0; h < kC; ++h) {
+        ty[h] = (threadIdx.x >> 5) + h * (BLK / 32);
         const int i = i0 + tx, j = j0 + ty[h];
         in[h] = i < a.nx && j < a.ny;
         col[h] = in[h] ? j * a.nx + i : 0;
@@ -515,11 +518,11 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
 
     // The halo cells this thread keeps: shared-memory slot | class << 16
     // (class 27: the pinned cell), global index; -1 when none.
-    int hpk[kHaloPer], hcc[kHaloPer];
+    int hpk[kHP], hcc[kHP];
     const int nhalo = 2 * RX * RY + 4 * RX * kz;
 #pragma unroll
-    for (int u = 0; u < kHaloPer; ++u) {
-        const int s = threadIdx.x + u * kResBlock;
+    for (int u = 0; u < kHP; ++u) {
+        const int s = threadIdx.x + u * BLK;
         hpk[u] = -1;
         hcc[u] = 0;
         if (s >= nhalo) continue;
@@ -542,18 +545,18 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     }
 
     if (threadIdx.x < 27) idgf[threadIdx.x] = a.inv_diag_f[threadIdx.x];
-    for (int s = threadIdx.x; s < HX * HY * (tz_full + 2); s += kResBlock) dsm[s] = 0.f;
-    for (int s = threadIdx.x; s < RX * RY * tz_full; s += kResBlock) dxs[s] = 0.f;
+    for (int s = threadIdx.x; s < HX * HY * (tz_full + 2); s += BLK) dsm[s] = 0.f;
+    for (int s = threadIdx.x; s < RX * RY * tz_full; s += BLK) dxs[s] = 0.f;
     __syncthreads();
 
-    float r[kCols][kResMaxTz];
-    float hr[kHaloPer];
+    float r[kC][kResMaxTz];
+    float hr[kHP];
 #pragma unroll
-    for (int h = 0; h < kCols; ++h)
+    for (int h = 0; h < kC; ++h)
 #pragma unroll
         for (int kk = 0; kk < kResMaxTz; ++kk) r[h][kk] = 0.f;
 #pragma unroll
-    for (int u = 0; u < kHaloPer; ++u) hr[u] = 0.f;
+    for (int u = 0; u < kHP; ++u) hr[u] = 0.f;
     int fr = 0;  // face exchanges so far; exchange f uses buffer f & 1
     auto face = [&](int f) { return (f & 1) ? a.face1 : a.face0; };
 
@@ -561,7 +564,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     // sums of the rounded r; with `final_pass` only the FP64 sum of (b - A x)^2.
     auto residual = [&](double &srr, double &srz, double &smax, bool final_pass) {
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
             const double wxm = wxy[h][0] != 0.f ? a.ix2 : 0.0, wxp = wxy[h][1] != 0.f ? a.ix2 : 0.0;
             const double wym = wxy[h][2] != 0.f ? a.iy2 : 0.0, wyp = wxy[h][3] != 0.f ? a.iy2 : 0.0;
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     // halo's r from the neighbours' faces.
     auto publish_r = [&](float *fb) {
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
 #pragma unroll
             for (int kk = 0; kk < kResMaxTz; ++kk) {
@@ -608,12 +611,12 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     };
     auto fetch_halo_r = [&](const float *fb) {
 #pragma unroll
-        for (int u = 0; u < kHaloPer; ++u)
+        for (int u = 0; u < kHP; ++u)
             if (hpk[u] >= 0) hr[u] = __ldcg(fb + hcc[u]);
     };
     auto fold = [&]() {
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
             for (int kk = 0; kk < kz; ++kk) {
                 const int cc = col[h] + (k0 + kk) * a.nxy;
@@ -631,7 +634,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     double m0 = 0.0;
     residual(s0[0], s0[1], m0, false);
     publish_r(face(fr));
-    if (!grid_reduce<2, true>(c, s0, m0)) return;
+    if (!grid_reduce<BLK, 2, true>(c, s0, m0)) return;
     fetch_halo_r(face(fr));
     ++fr;
     const double initial_l2 = sqrt(s0[0]);
@@ -649,13 +652,13 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
         const unsigned long long t0 = gtimer();
         const float fb = float(beta);
 #pragma unroll
-        for (int u = 0; u < kHaloPer; ++u) {
+        for (int u = 0; u < kHP; ++u) {
             if (hpk[u] < 0) continue;
             const int sl = hpk[u] & 0xffff, cls = hpk[u] >> 16;
             dsm[sl] = make_d(hr[u], dsm[sl], idgf[cls == 27 ? 0 : cls], cls == 27, first, fb);
         }
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
 #pragma unroll
             for (int kk = 0; kk < kResMaxTz; ++kk) {
@@ -673,12 +676,16 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
         double S[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         float rmax = 0.f;
         float *fq = face(fr);
+        const bool zlo = k0 == 0, zhi = k0 + kz == a.nz;  // the tile holds the plane k = 0 / k = nz - 1
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
             const float *w = wxy[h];
-            double crr = 0.0, cqq = 0.0, cqr = 0.0, cdq = 0.0;  // the column's cells
-            double err = 0.0, eqq = 0.0, eqr = 0.0;              // its cells on a z wall
+            // Jacobi weights: the column's class inside, its z-wall class at k = 0, nz - 1
+            const double wm = a.inv_diag[cls_xy[h]], we = a.inv_diag[cls_xy[h] + 1] - wm;
+            // the column's sums: FP32 over its tz cells (COL32) or FP64 per cell
+            double crr = 0.0, cqq = 0.0, cqr = 0.0, cdq = 0.0;
+            float frr = 0.f, fqq = 0.f, fqr = 0.f, fdq = 0.f;
             float below = dsm[own(h, -1)], cur = dsm[own(h, 0)];
 #pragma unroll
             for (int kk = 0; kk < kResMaxTz; ++kk) {
@@ -693,29 +700,44 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
                 if (pcol[h] && k == 0) ax = cur;  // identity row of the pinned cell
                 qs[loc(h, kk)] = ax;
                 if (face_col[h] || kk == 0 || kk == kz - 1) fq[col[h] + k * a.nxy] = ax;
-                const double rd = double(r[h][kk]), qd = double(ax), dd = double(cur);
-                const double rr = rd * rd, qq = qd * qd, qr = qd * rd;
-                crr += rr; cqq += qq; cqr += qr;
-                cdq = fma(dd, qd, cdq);
-                if (k == 0 || k == a.nz - 1) { err += rr; eqq += qq; eqr += qr; }
+                if (COL32) {
+                    const float rv = r[h][kk];
+                    frr = __fmaf_rn(rv, rv, frr);
+                    fqq = __fmaf_rn(ax, ax, fqq);
+                    fqr = __fmaf_rn(ax, rv, fqr);
+                    fdq = __fmaf_rn(cur, ax, fdq);
+                } else {
+                    const double rd = double(r[h][kk]), qd = double(ax), dd = double(cur);
+                    crr = fma(rd, rd, crr);
+                    cqq = fma(qd, qd, cqq);
+                    cqr = fma(qd, rd, cqr);
+                    cdq = fma(dd, qd, cdq);
+                }
+                if ((kk == 0 && zlo) || (kk == kz - 1 && zhi)) {  // a z-wall cell: its class weight
+                    const double rd = double(r[h][kk]), qd = double(ax);
+                    S[1] = fma(we, rd * rd, S[1]);
+                    S[4] = fma(we, qd * qd, S[4]);
+                    S[6] = fma(we, qd * rd, S[6]);
+                }
                 rmax = fmaxf(rmax, fabsf(r[h][kk]));
                 below = cur;
                 cur = above;
             }
-            // Jacobi weights: the column's class inside, its z-wall class at k = 0, nz - 1
-            const double wm = a.inv_diag[cls_xy[h]], we = a.inv_diag[cls_xy[h] + 1] - wm;
+            if (COL32) {
+                crr = double(frr); cqq = double(fqq); cqr = double(fqr); cdq = double(fdq);
+            }
             S[0] += crr;
-            S[1] += wm * crr + we * err;
+            S[1] = fma(wm, crr, S[1]);
             S[2] += cdq;
             S[3] += cqq;
-            S[4] += wm * cqq + we * eqq;
+            S[4] = fma(wm, cqq, S[4]);
             S[5] += cqr;
-            S[6] += wm * cqr + we * eqr;
+            S[6] = fma(wm, cqr, S[6]);
         }
         double mx = double(rmax);
         const unsigned long long t2 = gtimer();
         t_op += t2 - t1;
-        if (!grid_reduce<7, true>(c, S, mx)) return;
+        if (!grid_reduce<BLK, 7, true>(c, S, mx)) return;
         const unsigned long long t3 = gtimer();
         const double rz = S[1], dq = S[2];
         if (fabs(dq) < 1.0e-30 || !isfinite(dq) || !isfinite(rz / dq)) {
@@ -729,11 +751,11 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
         const float af = float(alpha);
         const float *fqr = face(fr);
         ++fr;
-        float hq[kHaloPer];
+        float hq[kHP];
 #pragma unroll
-        for (int u = 0; u < kHaloPer; ++u) hq[u] = hpk[u] >= 0 ? __ldcg(fqr + hcc[u]) : 0.f;
+        for (int u = 0; u < kHP; ++u) hq[u] = hpk[u] >= 0 ? __ldcg(fqr + hcc[u]) : 0.f;
 #pragma unroll
-        for (int h = 0; h < kCols; ++h) {
+        for (int h = 0; h < kC; ++h) {
             if (!in[h]) continue;
 #pragma unroll
             for (int kk = 0; kk < kResMaxTz; ++kk) {
@@ -744,7 +766,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
             }
         }
 #pragma unroll
-        for (int u = 0; u < kHaloPer; ++u) hr[u] = __fmaf_rn(-af, hq[u], hr[u]);
+        for (int u = 0; u < kHP; ++u) hr[u] = __fmaf_rn(-af, hq[u], hr[u]);
         iterations += 1;
         double res = sqrt(fmax(rr_next, 0.0));
         residual_v = res;
@@ -761,7 +783,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
             double m3 = 0.0;
             residual(s3[0], s3[1], m3, false);
             publish_r(face(fr));
-            if (!grid_reduce<2, true>(c, s3, m3)) return;
+            if (!grid_reduce<BLK, 2, true>(c, s3, m3)) return;
             fetch_halo_r(face(fr));
             ++fr;
             res = sqrt(s3[0]);
@@ -789,7 +811,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res1_kernel(const __grid_c
     double d0 = 0.0, d1 = 0.0;
     residual(st[0], d0, d1, true);
     double unused = 0.0;
-    if (!grid_reduce<1, false>(c, st, unused)) return;
+    if (!grid_reduce<BLK, 1, false>(c, st, unused)) return;
     if (b == 0 && threadIdx.x == 0) {
         CgSeqState *w = a.st;
         w->error = error;
@@ -835,10 +857,17 @@ bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
     // one reduction per iteration for the L2 stop rule (FLURSYS_PCG_RESIDENT=2
     // keeps the two-reduction form)
     plan.single = args.stop_rule == FLURSYS_STOP_REL_L2 && !(env && std::strcmp(env, "2") == 0);
-    plan.kernel = plan.single ? (const void *)pcg3d_res1_kernel : (const void *)pcg3d_res2_kernel;
+    // column sums of the dot products in FP32 (default) or every product in
+    // FP64 (FLURSYS_PCG_RES_DOTS=64)
+    const char *denv = std::getenv("FLURSYS_PCG_RES_DOTS");
+    plan.col32 = !(denv && std::atoi(denv) == 64);
+    plan.block = kResBlock;
+    plan.kernel = !plan.single ? (const void *)pcg3d_res2_kernel
+                  : plan.col32 ? (const void *)pcg3d_res1_kernel<kResBlock, true>
+                               : (const void *)pcg3d_res1_kernel<kResBlock, false>;
     if (cudaFuncSetAttribute(plan.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) != cudaSuccess)
         return false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, kResBlock, plan.smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.kernel, plan.block, plan.smem) != cudaSuccess ||
         per_sm < 1 || plan.grid > per_sm * sms)
         return false;
     a.ix2 = args.ix2; a.iy2 = args.iy2; a.iz2 = args.iz2;
@@ -878,7 +907,7 @@ cudaError_t pcg3d_res_launch(const Pcg3dResPlan &plan, CgSeqState *state, cudaSt
     if (e == cudaSuccess) e = cudaMemsetAsync(state, 0, sizeof(CgSeqState), stream);
     void *params[] = {&a};
     if (e == cudaSuccess)
-        e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.grid), dim3(kResBlock), params, plan.smem, stream);
+        e = cudaLaunchCooperativeKernel(plan.kernel, dim3(plan.grid), dim3(plan.block), params, plan.smem, stream);
     return e;
 }
 

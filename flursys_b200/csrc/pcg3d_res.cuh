@@ -39,6 +39,8 @@ struct Pcg3dResPlan {
     ResArgs args{};
     bool single = false;             // single-reduction form (L2 stop rule)
     const void *kernel = nullptr;    // the launched kernel
+    int block = 512;                 // its threads per block
+    bool col32 = true;               // dot products: FP32 column sums, FP64 across columns
     int grid = 0;
     size_t smem = 0;
     double *partials = nullptr;
