@@ -728,10 +728,11 @@ def case_pcg(args) -> dict:
     rows = []
     for s in range(args.steps):
         rep = hd.step(1)
-        ph = (C.c_double * 4)()
-        hd.lib.flursys_cuda_solver_profile(hd.h, ph, 4)
+        ph = (C.c_double * 6)()
+        hd.lib.flursys_cuda_solver_profile(hd.h, ph, 6)
         kind = hd.solve_kind()
-        names = (["halo+direction", "operator", "reduce+barrier", "update+replacement"]
+        names = (["halo+direction", "operator", "reduce+barrier", "update+replacement", "barrier_wait",
+                  "slowest_block_work"]
                  if kind == _abi.SOLVE_RESIDENT else ["stencil", "pointwise", "barrier+reduce", "replacement"])
         its = max(1, rep.pressure_iterations)
         rows.append({"step": s + 1, "solve_kind": int(kind), "iterations": int(rep.pressure_iterations),

@@ -451,7 +451,7 @@ int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream) {
 int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms, size_t n) {
     if (!h || !phase_ms) { g_error = "null argument"; return FLURSYS_ERR_INVALID_ARGUMENT; }
     const PcgResultDev *r = h->pcg.h_result;
-    for (size_t i = 0; i < n && i < 4; ++i) phase_ms[i] = r ? 1e-6 * (double)r->phase_ns[i] : 0.0;
+    for (size_t i = 0; i < n && i < 6; ++i) phase_ms[i] = r ? 1e-6 * (double)r->phase_ns[i] : 0.0;
     return FLURSYS_OK;
 }
 

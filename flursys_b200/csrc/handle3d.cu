@@ -186,7 +186,7 @@ int32_t step3d(FlursysCudaHandle *h, FlursysStepReport *rep) {
         m.true_l2 = q.true_l2;
         m.initial_l2 = q.initial_l2;
         m.device_error = q.device_error;
-        for (int i = 0; i < 4; ++i) m.phase_ns[i] = q.phase_ns[i];
+        for (int i = 0; i < 6; ++i) m.phase_ns[i] = q.phase_ns[i];
     }
     const PcgResultDev &r = *h->pcg.h_result;
     status = pcg_result_status(r, &h->err);

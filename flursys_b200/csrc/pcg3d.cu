@@ -489,6 +489,7 @@ __global__ void __launch_bounds__(kBlock, 3) pcg3d_kernel(Pcg3dArgs a, Geo g) {
         res->initial_l2 = initial_l2;
         res->device_error = bar->error;
         for (int p = 0; p < 4; ++p) res->phase_ns[p] = tph[p];
+        res->phase_ns[4] = res->phase_ns[5] = 0;
     }
 }
 

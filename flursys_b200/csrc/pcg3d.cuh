@@ -20,8 +20,9 @@ struct PcgResultDev {
     unsigned device_error;  // DeviceError bits
     unsigned pad;
     // Nanoseconds block 0 spent in: [0] stencil passes, [1] pointwise passes,
-    // [2] grid barriers + partial reductions, [3] residual replacements.
-    unsigned long long phase_ns[4];
+    // [2] grid barriers + partial reductions, [3] residual replacements;
+    // [4], [5] are used by the chip-resident solve only.
+    unsigned long long phase_ns[6];
 };
 
 struct Pcg3dArgs {

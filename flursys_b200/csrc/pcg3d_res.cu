@@ -85,11 +85,12 @@ __device__ __forceinline__ unsigned long long gtimer() {
 // is a single atomic and the wait polls the same word. The wait is
 // bounded; a failure sets the timeout bit in the barrier's error word and
 // in the state, and every block leaves at its next barrier.
-__device__ __forceinline__ bool res_sync(const ResArgs &a) {
+__device__ __forceinline__ bool res_sync(const ResArgs &a, unsigned long long *wait_ns = nullptr) {
     const unsigned nblocks = gridDim.x + (unsigned)a.barrier_extra;
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
+        const unsigned long long tw = wait_ns ? gtimer() : 0ull;
         unsigned *cnt = &a.bar->count;
         unsigned old;
         asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
@@ -111,6 +112,7 @@ __device__ __forceinline__ bool res_sync(const ResArgs &a) {
             }
         }
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        if (wait_ns) *wait_ns += gtimer() - tw;
         s_ok = ok;
     }
     __syncthreads();
@@ -122,7 +124,8 @@ struct ResCtx {
     float *dsm, *dxs, *qs;
     double *red;
     int round;
-    unsigned long long t_reduce;  // block 0, thread 0: time in grid reductions
+    unsigned long long t_reduce;  // thread 0: time in grid reductions
+    unsigned long long t_wait;    // thread 0: time waiting inside their grid barriers
 };
 
 // Sums NS values (and, with MAX, the maximum of one more) over the grid.
@@ -140,7 +143,7 @@ __device__ __forceinline__ bool grid_reduce(ResCtx &c, double (&v)[NS], double &
         for (int k = 0; k < NS; ++k) P[blockIdx.x * kResSlots + k] = v[k];
         if (MAX) P[blockIdx.x * kResSlots + NS] = mx;
     }
-    if (!res_sync(c.a)) return false;
+    if (!res_sync(c.a, &c.t_wait)) return false;
     // warp k sums value k over the blocks (every block in the same order)
     const int wk = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (wk < NS + (MAX ? 1 : 0)) {
@@ -186,7 +189,7 @@ __global__ void __launch_bounds__(kResBlock, 1) pcg3d_res2_kernel(const __grid_c
     float *dsm = smem;                                      // (tz + 2) x HY x HX
     float *dxs = smem + (size_t)HX * HY * (tz_full + 2);   // tz x RY x RX
     float *qs = dxs + (size_t)RX * RY * tz_full;           // tz x RY x RX
-    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull};
+    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull, 0ull};
     unsigned long long t_halo = 0, t_op = 0, t_upd = 0;
     const int b = blockIdx.x;
     const int i0 = (b % a.ntx) * RX, j0 = ((b / a.ntx) % a.nty) * RY, k0 = (b / (a.ntx * a.nty)) * a.tz;
@@ -490,7 +493,7 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
     float *dsm = smem;                                      // (tz + 2) x HY x HX
     float *dxs = smem + (size_t)HX * HY * (tz_full + 2);   // tz x RY x RX
     float *qs = dxs + (size_t)RX * RY * tz_full;           // tz x RY x RX
-    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull};
+    ResCtx c{a, dsm, dxs, qs, red, 0, 0ull, 0ull};
     unsigned long long t_halo = 0, t_op = 0, t_upd = 0;
     const int b = blockIdx.x;
     const int i0 = (b % a.ntx) * RX, j0 = ((b / a.ntx) % a.nty) * RY, k0 = (b / (a.ntx * a.nty)) * a.tz;
@@ -827,7 +830,9 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
         w->phase_ns[1] = t_op;
         w->phase_ns[2] = c.t_reduce;
         w->phase_ns[3] = t_upd;
+        w->phase_ns[4] = c.t_wait;
     }
+    if (threadIdx.x == 0) atomicMax(&a.st->phase_ns[5], t_halo + t_op + t_upd);
 }
 
 }  // namespace

@@ -17,8 +17,9 @@ struct CgSeqState {
     unsigned device_error;  // DeviceError bits (a grid barrier of the resident solve gave up)
     // resident solve, as seen by block 0 (ns): [0] halo and direction update,
     // [1] operator pass, [2] grid barriers and reductions, [3] update and
-    // residual replacements
-    unsigned long long phase_ns[4];
+    // residual replacements, [4] block 0's waits in grid barriers, [5] the
+    // largest [0] + [1] + [3] of any block (the slowest block's work)
+    unsigned long long phase_ns[6];
 };
 
 struct Pcg3dResPlan;

@@ -299,9 +299,11 @@ int32_t flursys_cuda_set_stream(FlursysCudaHandle *h, void *stream);
  * reductions, [3] FP64 residual replacements (as seen by block 0). For the
  * chip-resident 3D solve (FLURSYS_SOLVE_RESIDENT) the split is [0] face
  * exchange and direction update, [1] operator pass, [2] grid reductions and
- * barriers, [3] vector updates and residual replacements; the graph-driven
- * 3D solve records none (all zero). `n` is the capacity of `phase_ms`
- * (4 used). No reference counterpart. */
+ * barriers, [3] vector updates and residual replacements, [4] block 0's
+ * waits inside grid barriers, [5] the largest [0] + [1] + [3] of any block
+ * (the slowest block's work); the graph-driven 3D solve records none (all
+ * zero). `n` is the capacity of `phase_ms` (up to 6 used). No reference
+ * counterpart. */
 int32_t flursys_cuda_solver_profile(const FlursysCudaHandle *h, double *phase_ms, size_t n);
 
 /* Output overlapped with compute. No reference counterpart as an API: it
