@@ -932,7 +932,10 @@ int grid_1d(long long n, int per = 256) { return (int)std::max<long long>(1, std
 // commits them to an mbarrier, and the four warps read the accumulator back
 // with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. voxel rows
 // 4w..4w+3) and store it as BF16. Two accumulator buffers alternate between
-// planes; the MMAs of plane z overlap the staging of input plane z+2.
+// planes, and the loop is a software pipeline: while the MMAs of plane z
+// run, the CTA stages input plane z + 2, queues the MMAs of plane z + 1
+// into the other buffer, and only then waits for plane z and stores it, so
+// the tensor pipe has the next plane's work queued during every epilogue.
 //
 // Operands are in the K-major no-swizzle core-matrix layout (8 rows x 16 B):
 //   input ring, 4 planes: [plane][k8][cell] with cell = cy*10 + cx of the
@@ -1035,18 +1038,34 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
         const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + t27) * CIN + k8 * 8);
         *reinterpret_cast<uint4 *>(wts + ((t27 * K8 + k8) * COUT + co) * 16) = q;
     }
-    auto stage = [&](int p) {  // input plane p into its ring slot, channels fastest
+    // input plane p into its ring slot, channels fastest; every load of a
+    // thread is issued before its first store
+    constexpr int kItems = (kUCells * K8 + kUThreads - 1) / kUThreads;
+    auto stage = [&](int p) {
         uint8_t *slot = ring + ((p + 4) & 3) * G::kSlot;
-        for (int idx = tid; idx < kUCells * K8; idx += kUThreads) {
-            const int k8 = idx % K8, cell = idx / K8;
-            const int cx = cell % kUHX, cy = cell / kUHX;
-            const uint4 q = load8<CIN, MODE>(src, x0 - 1 + cx, y0 - 1 + cy, p, nx, ny, nz, k8);
-            *reinterpret_cast<uint4 *>(slot + (k8 * kUCells + cell) * 16) = q;
+        uint4 v[kItems];
+#pragma unroll
+        for (int u = 0; u < kItems; ++u) {
+            const int idx = tid + u * kUThreads;
+            v[u] = make_uint4(0, 0, 0, 0);
+            if (idx < kUCells * K8) {
+                const int k8 = idx % K8, cell = idx / K8;
+                const int cx = cell % kUHX, cy = cell / kUHX;
+                v[u] = load8<CIN, MODE>(src, x0 - 1 + cx, y0 - 1 + cy, p, nx, ny, nz, k8);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kItems; ++u) {
+            const int idx = tid + u * kUThreads;
+            if (idx < kUCells * K8) {
+                const int k8 = idx % K8, cell = idx / K8;
+                *reinterpret_cast<uint4 *>(slot + (k8 * kUCells + cell) * 16) = v[u];
+            }
         }
     };
     stage(z0 - 1);
     stage(z0);
-    if (z0 + 1 < z1 + 1) stage(z0 + 1);
+    if (z0 + 1 <= z1) stage(z0 + 1);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 0) {
         const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
@@ -1067,43 +1086,54 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
     // K-major, N = COUT, M = 128
     constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((128u >> 4) << 24);
+    // The 27 x CIN/16 MMAs of output plane z into accumulator buffer b, then
+    // their commit to that buffer's mbarrier (one thread). Descriptors are
+    // formed once per input plane; each tap and K chunk adds a constant
+    // offset to the start-address field (addresses stay below 2^18 bytes, so
+    // the 14-bit field cannot carry).
+    auto issue = [&](int z, int b) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t dbuf = tmem + (uint32_t)(b * COUT);
+        const uint64_t wdesc = umma_desc(sbase + 4 * G::kSlot, COUT * 16, 128);
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz) {
+            const uint64_t adesc = umma_desc(sbase + (uint32_t)(((z + dz - 1 + 4) & 3) * G::kSlot), kUCells * 16, kUHX * 16);
+#pragma unroll
+            for (int t9 = 0; t9 < 9; ++t9) {
+#pragma unroll
+                for (int kc = 0; kc < CIN / 16; ++kc) {
+                    const int dy = t9 / 3, dx = t9 % 3, tap = dz * 9 + t9;
+                    const uint64_t a = adesc + (uint64_t)((((dy * kUHX + dx) + 2 * kc * kUCells) * 16) >> 4);
+                    const uint64_t w = wdesc + (uint64_t)((((tap * K8 + 2 * kc) * COUT) * 16) >> 4);
+                    umma_f16(dbuf, a, w, kIdesc, (dz | t9 | kc) ? 1u : 0u);
+                }
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b ? mb1 : mb0)
+                     : "memory");
+    };
+    if (tid == 0 && z0 < z1) issue(z0, 0);
     const int m = warp * 32 + lane;  // this thread's voxel row of the accumulator
     const int vx = x0 + (m % kUX), vy = y0 + m / kUX;
     bool ok = true;
+    int failed_z = -1;
     for (int z = z0; z < z1; ++z) {
         const int b = (z - z0) & 1;
-        const uint32_t dbuf = tmem + (uint32_t)(b * COUT);
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t acc = 0;
-#pragma unroll 1
-            for (int dz = 0; dz < 3; ++dz) {
-                const uint32_t slot = sbase + (uint32_t)(((z + dz - 1 + 4) & 3) * G::kSlot);
-#pragma unroll 1
-                for (int t9 = 0; t9 < 9; ++t9) {
-                    const int dy = t9 / 3, dx = t9 % 3, tap = dz * 9 + t9;
-#pragma unroll
-                    for (int kc = 0; kc < CIN / 16; ++kc) {
-                        const uint32_t a = slot + (uint32_t)(((dy * kUHX + dx) + 2 * kc * kUCells) * 16);
-                        const uint32_t w = sbase + 4 * G::kSlot + (uint32_t)((tap * K8 + 2 * kc) * COUT * 16);
-                        umma_f16(dbuf, umma_desc(a, kUCells * 16, kUHX * 16), umma_desc(w, COUT * 16, 128), kIdesc,
-                                 acc);
-                        acc = 1;
-                    }
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             b ? mb1 : mb0)
-                         : "memory");
-        }
-        if (z + 2 <= z1) stage(z + 2);  // overlaps the MMAs of plane z
+        // Plane z + 2 goes to the slot of plane z - 2, whose last reader (the
+        // MMAs of plane z - 1) finished before the previous epilogue; the
+        // MMAs of plane z (planes z - 1 .. z + 1) run meanwhile.
+        if (z + 2 <= z1) stage(z + 2);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        // The MMAs of plane z + 1 (into the other buffer, free since the
+        // epilogue of plane z - 1) queue behind those of plane z.
+        if (tid == 0 && z + 1 < z1) issue(z + 1, b ^ 1);
         const bool arrived = mbar_wait_bounded(b ? mb1 : mb0, (uint32_t)(((z - z0) >> 1) & 1));
         ok = ok && arrived;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         float acc[COUT];
         if (arrived) {
-            tmem_ld<COUT>(dbuf + ((uint32_t)(warp * 32) << 16), acc);
+            tmem_ld<COUT>(tmem + (uint32_t)(b * COUT) + ((uint32_t)(warp * 32) << 16), acc);
         } else {
 #pragma unroll
             for (int c = 0; c < COUT; ++c) acc[c] = __int_as_float(0x7fc00000);
@@ -1120,8 +1150,16 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (!__syncthreads_and(ok)) break;  // a lost accumulator: stop issuing, free the tensor memory
+        if (!__syncthreads_and(ok)) {  // a lost accumulator: stop, free the tensor memory
+            failed_z = z;
+            break;
+        }
+    }
+    // the group issued for the plane after a lost accumulator gets its own
+    // (bounded) wait before the tensor memory is freed
+    if (tid == 0 && failed_z >= 0 && failed_z + 1 < z1) {
+        const int zz = failed_z + 1;
+        (void)mbar_wait_bounded(((zz - z0) & 1) ? mb1 : mb0, (uint32_t)(((zz - z0) >> 1) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
