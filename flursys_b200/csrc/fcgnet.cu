@@ -1216,16 +1216,33 @@ template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
     using G = UmmaConv<CIN, COUT>;
     if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
-    static bool configured = false;
-    if (!configured) {
+    static int slots = 0;  // resident CTAs per device (per instantiation)
+    if (!slots) {
         cudaError_t e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              G::kSmem);
+        int dev = 0, sms = 0, per_sm = 0;
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_umma<CIN, COUT, MODE>, kUThreads, G::kSmem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        slots = std::max(1, sms * std::max(1, per_sm));
     }
+    // Planes per CTA: the longest march (fewest weight loads and halo planes
+    // per output plane) whose grid still fills its last wave of resident
+    // CTAs to 85% or more; otherwise the one that fills it best.
     const long long cols = (long long)((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY);
-    int kz = 1;  // planes per CTA: about four CTAs per SM, at least 4 planes where the grid allows
-    while (kz < nz && cols * ((nz + 2 * kz - 1) / (2 * kz)) >= 4 * 148) kz *= 2;
+    int kz = 1;
+    double best = -1.0;
+    for (int t = 1; t <= nz; t *= 2) {
+        const long long ctas = cols * ((nz + t - 1) / t);
+        const long long waves = (ctas + slots - 1) / slots;
+        const double fill = double(ctas) / double(waves * slots);
+        if (fill >= 0.85 || fill > best + 1e-9) {
+            if (fill >= 0.85 || best < 0.85) kz = t;
+            best = std::max(best, fill);
+        }
+    }
     dim3 grid((nx + kUX - 1) / kUX, (ny + kUY - 1) / kUY, (nz + kz - 1) / kz);
     conv_umma<CIN, COUT, MODE><<<grid, kUThreads, G::kSmem, st>>>(s, W, out, nx, ny, nz, kz);
     return cudaGetLastError();
@@ -1281,12 +1298,13 @@ long long net_param_count() { return net_param_offset(kNetLayers); }
 cudaError_t NetWorkspace::ensure(int nx_, int ny_, int nz_, bool training_) {
     const long long v1 = (long long)nx_ * ny_ * nz_, v2 = v1 / 8, v3 = v1 / 64, v4 = v1 / 512;
     // element counts (BF16) of every tensor, in declaration order
-    // (inference fuses the full-resolution layers and the pool / up-add
-    // inputs, so it keeps x2, a2, a3, a4, b3 and b2 only)
+    // (inference fuses the full-resolution layers, so it keeps x2, a2, a3,
+    // a4, b3, b2 and, for the tensor-memory convolutions that stage plain
+    // tensors, the pooled / up-added inputs x3, x5, x6)
     const long long tr = training_ ? 1 : 0;
     const long long sizes[24] = {
-        tr * v1 * 16, v2 * 16, v2 * 32, tr * v3 * 32, v3 * 64, tr * v4 * 64, v4 * 64,  // a1 x2 a2 x3 a3 x4 a4
-        tr * v3 * 64, v3 * 32, tr * v2 * 32, v2 * 16, tr * v1 * 16,                    // x5 b3 x6 b2 x7
+        tr * v1 * 16, v2 * 16, v2 * 32, v3 * 32, v3 * 64, tr * v4 * 64, v4 * 64,  // a1 x2 a2 x3 a3 x4 a4
+        v3 * 64, v3 * 32, v2 * 32, v2 * 16, tr * v1 * 16,                         // x5 b3 x6 b2 x7
         v1 * 16, v2 * 32, v3 * 64, v4 * 64, v3 * 32, v2 * 16,                          // g7 g6 g5 g4 g3 g2
         v2 * 16, v3 * 32, v4 * 64, 0, 0, 0};                                           // gb2 gb3 ga4
     const int ntensor = training_ ? 21 : 12;
@@ -1393,10 +1411,23 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     e = cudaGetLastError();
     const uint16_t *W = w.fwd;
     if (e == cudaSuccess) e = launch_conv_fwd<16, 32, kPlain>(Src{ws.x2, nullptr}, W + net_param_offset(1), ws.a2, n2x, n2y, n2z, st);
-    if (e == cudaSuccess) e = launch_conv_fwd<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
-    if (e == cudaSuccess) e = launch_conv_fwd<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
-    if (e == cudaSuccess) e = launch_conv_fwd<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
-    if (e == cudaSuccess) e = launch_conv_fwd<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
+    if (umma_enabled()) {
+        // The tensor-memory convolutions stage plain tensors: pool and up-add
+        // run as their own passes (same FP32 sums and BF16 rounding as the
+        // fused staging of the mma.sync kernels, so the operands are equal).
+        if (e == cudaSuccess) e = launch_pool<32>(ws.a2, ws.x3, n3x, n3y, n3z, 0.125f, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<32, 64, kPlain>(Src{ws.x3, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
+        if (e == cudaSuccess) e = launch_upadd<64>(ws.a4, ws.a3, ws.x5, n3x, n3y, n3z, 1.f, 0, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<64, 32, kPlain>(Src{ws.x5, nullptr}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
+        if (e == cudaSuccess) e = launch_upadd<32>(ws.b3, ws.a2, ws.x6, n2x, n2y, n2z, 1.f, 0, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<32, 16, kPlain>(Src{ws.x6, nullptr}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
+    } else {
+        if (e == cudaSuccess) e = launch_conv_fwd<32, 64, kPool>(Src{ws.a2, nullptr}, W + net_param_offset(2), ws.a3, n3x, n3y, n3z, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<64, 64, kPool>(Src{ws.a3, nullptr}, W + net_param_offset(3), ws.a4, n4x, n4y, n4z, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<64, 32, kUpAdd>(Src{ws.a3, ws.a4}, W + net_param_offset(4), ws.b3, n3x, n3y, n3z, st);
+        if (e == cudaSuccess) e = launch_conv_fwd<32, 16, kUpAdd>(Src{ws.a2, ws.b3}, W + net_param_offset(5), ws.b2, n2x, n2y, n2z, st);
+    }
     if (e == cudaSuccess) {
         dim3 grid((n2x + kOutCX - 1) / kOutCX, (n2y + kOutCY - 1) / kOutCY, n2z);
         net_out_interior<<<grid, kOutCX * kOutCY, 0, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz, w.out_params);
