@@ -163,68 +163,94 @@ __global__ void __launch_bounds__(kPw) fcg_shift(double *x, const FcgScalars *sc
     for (long long c = blockIdx.x * (long long)kPw + threadIdx.x; c < n; c += (long long)gridDim.x * kPw) x[c] -= s;
 }
 
-// q = A~ d (Neumann form, FP32); partials d.q and d.r.
-__global__ void __launch_bounds__(kBX * kBY) fcg_spmv(Geo3 g, const float *__restrict__ d, const float *__restrict__ r,
-                                                      float *q, double *partials) {
-    const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5), k = blockIdx.z;
-    double v[2] = {0.0, 0.0};
-    if (i < g.nx && j < g.ny) {
-        const long long c = ((long long)k * g.ny + j) * g.nx + i;
-        const float dc = d[c];
-        const long long sy = g.nx, sz = (long long)g.nx * g.ny;
-        const float qv = apply7<float>(g, i, j, k, g.wx, g.wy, g.wz, dc, [&](int a, int b, int e) {
-            return d[c + a + b * sy + e * sz];
-        });
-        q[c] = qv;
-        v[0] = double(dc) * double(qv);
-        v[1] = double(dc) * double(r[c]);
-    }
-    const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    write_partials(partials, blk, v, 2);
-}
-
 // Diagonal of the Neumann-form operator at (i, j, k).
 __device__ __forceinline__ float diag7(const Geo3 &g, int i, int j, int k) {
     return g.wx * float((i > 0) + (i + 1 < g.nx)) + g.wy * float((j > 0) + (j + 1 < g.ny)) +
            g.wz * float((k > 0) + (k + 1 < g.nz));
 }
 
-// Smoothing passes of the preconditioner (damped Jacobi on A~, weight omega):
-//   pre   z_out = omega D^-1 r,  r_out = r - A~ z_out
-//   post  z_out = z_in + omega D^-1 (r - A~ z_in)
-// `pre` needs z_out at the neighbours, so it evaluates omega D^-1 r there.
-template <bool PRE>
-__global__ void __launch_bounds__(kBX * kBY) fcg_smooth(Geo3 g, const float *__restrict__ r,
-                                                        const float *__restrict__ z_in, float *z_out, float *r_out,
-                                                        float omega) {
-    const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5), k = blockIdx.z;
+// Smoothing passes of the preconditioner (damped Jacobi on A~, weight omega),
+// pre: z = omega D^-1 r and r - A~ z; post: z_in + omega D^-1 (r - A~ z_in),
+// and the operator pass, all as z-marching forms of the FP32 stencil passes
+// of one FCG iteration. A block
+// owns a 32 x kBY column of cells over kMZ planes; each thread keeps the
+// operand of the plane below, its own and the one above in registers, so a
+// plane is read from memory once per block (x and y neighbours come through
+// L1), and the block's partial sums are reduced once, after the march. The
+// arithmetic per cell is that of apply7 / diag7 in the same order.
+// ---------------------------------------------------------------------------
+constexpr int kMZ = 16;  // planes per marching block
+
+// q = A~ d (Neumann form, FP32); partials d.q and d.r.
+__global__ void __launch_bounds__(kBX * kBY) fcg_spmv_m(Geo3 g, const float *__restrict__ d,
+                                                        const float *__restrict__ r, float *q, double *partials) {
+    const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * kMZ, k1 = min(g.nz, k0 + kMZ);
+    double v[2] = {0.0, 0.0};
+    if (i < g.nx && j < g.ny) {
+        const long long sy = g.nx, sz = (long long)g.nx * g.ny;
+        long long c = ((long long)k0 * g.ny + j) * g.nx + i;
+        float below = k0 > 0 ? d[c - sz] : 0.f, cur = d[c];
+        for (int k = k0; k < k1; ++k, c += sz) {
+            const float above = k + 1 < g.nz ? d[c + sz] : 0.f;
+            const float qv = apply7<float>(g, i, j, k, g.wx, g.wy, g.wz, cur, [&](int a, int b, int e) {
+                return e < 0 ? below : (e > 0 ? above : d[c + a + b * sy]);
+            });
+            q[c] = qv;
+            v[0] += double(cur) * double(qv);
+            v[1] += double(cur) * double(r[c]);
+            below = cur;
+            cur = above;
+        }
+    }
+    const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    write_partials(partials, blk, v, 2);
+}
+
+// Pre-smoothing: z_out = omega D^-1 r, r_out = r - A~ z_out.
+__global__ void __launch_bounds__(kBX * kBY) fcg_presmooth_m(Geo3 g, const float *__restrict__ r, float *z_out,
+                                                             float *r_out, float omega) {
+    const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * kMZ, k1 = min(g.nz, k0 + kMZ);
     if (i >= g.nx || j >= g.ny) return;
-    const long long c = ((long long)k * g.ny + j) * g.nx + i;
     const long long sy = g.nx, sz = (long long)g.nx * g.ny;
-    auto zv = [&](int a, int b, int e) -> float {
-        const long long m = c + a + b * sy + e * sz;
-        if (!PRE) return z_in[m];
-        return omega * r[m] / diag7(g, i + a, j + b, k + e);
-    };
-    const float dg = diag7(g, i, j, k);
-    const float zc = zv(0, 0, 0);
-    const float az = apply7<float>(g, i, j, k, g.wx, g.wy, g.wz, zc, zv);
-    const float res = r[c] - az;
-    if (PRE) {
-        z_out[c] = zc;
-        r_out[c] = res;
-    } else {
-        z_out[c] = zc + omega * res / dg;
+    long long c = ((long long)k0 * g.ny + j) * g.nx + i;
+    auto zat = [&](long long m, int ii, int jj, int kk) { return omega * r[m] / diag7(g, ii, jj, kk); };
+    float below = k0 > 0 ? zat(c - sz, i, j, k0 - 1) : 0.f, cur = zat(c, i, j, k0);
+    for (int k = k0; k < k1; ++k, c += sz) {
+        const float above = k + 1 < g.nz ? zat(c + sz, i, j, k + 1) : 0.f;
+        const float az = apply7<float>(g, i, j, k, g.wx, g.wy, g.wz, cur, [&](int a, int b, int e) {
+            return e < 0 ? below : (e > 0 ? above : zat(c + a + b * sy, i + a, j + b, k));
+        });
+        z_out[c] = cur;
+        r_out[c] = r[c] - az;
+        below = cur;
+        cur = above;
     }
 }
 
-// a += b (the coarse correction joins the pre-smoothed part).
-__global__ void __launch_bounds__(kPw) fcg_add(float *a, const float *b, long long n4) {
-    for (long long t = blockIdx.x * (long long)kPw + threadIdx.x; t < n4; t += (long long)gridDim.x * kPw) {
-        float4 u = reinterpret_cast<float4 *>(a)[t];
-        const float4 v = reinterpret_cast<const float4 *>(b)[t];
-        u.x += v.x; u.y += v.y; u.z += v.z; u.w += v.w;
-        reinterpret_cast<float4 *>(a)[t] = u;
+// Post-smoothing of z_in = z_pre + z_net (the coarse correction joins the
+// pre-smoothed part on the fly): z_out = z_in + omega D^-1 (r - A~ z_in).
+__global__ void __launch_bounds__(kBX * kBY) fcg_postsmooth_m(Geo3 g, const float *__restrict__ r,
+                                                              const float *__restrict__ z_pre,
+                                                              const float *__restrict__ z_net, float *z_out,
+                                                              float omega) {
+    const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5);
+    const int k0 = blockIdx.z * kMZ, k1 = min(g.nz, k0 + kMZ);
+    if (i >= g.nx || j >= g.ny) return;
+    const long long sy = g.nx, sz = (long long)g.nx * g.ny;
+    long long c = ((long long)k0 * g.ny + j) * g.nx + i;
+    auto zin = [&](long long m) { return z_pre[m] + z_net[m]; };
+    float below = k0 > 0 ? zin(c - sz) : 0.f, cur = zin(c);
+    for (int k = k0; k < k1; ++k, c += sz) {
+        const float above = k + 1 < g.nz ? zin(c + sz) : 0.f;
+        const float az = apply7<float>(g, i, j, k, g.wx, g.wy, g.wz, cur, [&](int a, int b, int e) {
+            return e < 0 ? below : (e > 0 ? above : zin(c + a + b * sy));
+        });
+        const float res = r[c] - az;
+        z_out[c] = cur + omega * res / diag7(g, i, j, k);
+        below = cur;
+        cur = above;
     }
 }
 
@@ -454,6 +480,8 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     const long long n = (long long)nx * ny * nz, n4 = n / 4;
     const dim3 sgrid((nx + kBX - 1) / kBX, (ny + kBY - 1) / kBY, nz), sblock(kBX * kBY);
     const int nsb = (int)(sgrid.x * sgrid.y * sgrid.z), npw = pw_grid(n4);
+    const dim3 mgrid(sgrid.x, sgrid.y, (nz + kMZ - 1) / kMZ);  // z-marching passes
+    const int nmb = (int)(mgrid.x * mgrid.y * mgrid.z);
     double net_ms = 0.0;
     auto sync_scalars = [&]() -> cudaError_t {
         cudaError_t m = cudaMemcpyAsync(f.h_sc, f.sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, st);
@@ -489,13 +517,13 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
             cudaEventRecord(f.e1, st);
             return m;
         }
-        fcg_smooth<true><<<sgrid, sblock, 0, st>>>(g, f.r, nullptr, f.t2, f.t1, omega);  // t2 = z0, t1 = r - A z0
+        fcg_presmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.t1, omega);  // t2 = z0, t1 = r - A z0
         cudaEventRecord(f.e0, st);
-        m = net_apply(net->w, net->ws, nx, ny, nz, h2, f.t1, f.z, st);                 // z = N(r1)
+        m = net_apply(net->w, net->ws, nx, ny, nz, h2, f.t1, f.z, st);   // z = N(r1)
         cudaEventRecord(f.e1, st);
         if (m != cudaSuccess) return m;
-        fcg_add<<<npw, kPw, 0, st>>>(f.t2, f.z, n4);                                     // t2 = z0 + N(r1)
-        fcg_smooth<false><<<sgrid, sblock, 0, st>>>(g, f.r, f.t2, f.z, nullptr, omega);  // z = post-smoothed
+        fcg_postsmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.z, f.t1, omega);  // t1 = post-smoothed z0 + N(r1)
+        std::swap(f.z, f.t1);                                                      // z = the preconditioned residual
         return cudaGetLastError();
     };
     e = residual();
@@ -540,8 +568,8 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
             fcg_dots<<<npw, kPw, 0, st>>>(f.z, ds, n4, f.partials);
             fcg_finalize_dots<<<1, 1024, 0, st>>>(f.partials, npw, ds, f.sc, inv_n);
             fcg_direction<<<npw, kPw, 0, st>>>(f.z, dcur, ds, f.sc, n4);
-            fcg_spmv<<<sgrid, sblock, 0, st>>>(g, dcur, f.r, qcur, f.partials);
-            fcg_finalize<<<1, 1024, 0, st>>>(f.partials, nsb, kFinSpmv, f.sc, slot);
+            fcg_spmv_m<<<mgrid, sblock, 0, st>>>(g, dcur, f.r, qcur, f.partials);
+            fcg_finalize<<<1, 1024, 0, st>>>(f.partials, nmb, kFinSpmv, f.sc, slot);
             fcg_update<<<npw, kPw, 0, st>>>(x, f.r, dcur, qcur, f.sc, n4, f.partials);
             fcg_finalize<<<1, 1024, 0, st>>>(f.partials, npw, kFinRR, f.sc, 0);
             e = cudaGetLastError();

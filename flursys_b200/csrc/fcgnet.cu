@@ -1216,11 +1216,11 @@ template <int CIN, int COUT, int MODE>
 cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
     using G = UmmaConv<CIN, COUT>;
     if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
-    static int slots = 0;  // resident CTAs per device (per instantiation)
+    static int slots = 0, per_sm = 0;  // resident CTAs per device and per SM (per instantiation)
     if (!slots) {
         cudaError_t e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              G::kSmem);
-        int dev = 0, sms = 0, per_sm = 0;
+        int dev = 0, sms = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess)
@@ -1228,13 +1228,19 @@ cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int 
         if (e != cudaSuccess) return e;
         slots = std::max(1, sms * std::max(1, per_sm));
     }
-    // Planes per CTA: the longest march (fewest weight loads and halo planes
-    // per output plane) whose grid still fills its last wave of resident
-    // CTAs to 85% or more; otherwise the one that fills it best.
+    // Planes per CTA. Where several CTAs share an SM: the longest march that
+    // still leaves about four CTAs per resident slot over the launch
+    // (measured on B200: longer marches with fewer CTAs ran up to 2x slower).
+    // Where one CTA fills an SM (the weights of all taps take most of the
+    // shared memory): the longest march whose grid fills its last wave to
+    // 85% or more, so the weights are loaded once per many planes.
     const long long cols = (long long)((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY);
     int kz = 1;
-    double best = -1.0;
-    for (int t = 1; t <= nz; t *= 2) {
+    if (per_sm > 1) {
+        while (kz < nz && cols * ((nz + 2 * kz - 1) / (2 * kz)) >= 4LL * (slots / per_sm)) kz *= 2;
+    }
+    double best = per_sm > 1 ? 2.0 : -1.0;
+    for (int t = 1; t <= nz && per_sm == 1; t *= 2) {
         const long long ctas = cols * ((nz + t - 1) / t);
         const long long waves = (ctas + slots - 1) / slots;
         const double fill = double(ctas) / double(waves * slots);
