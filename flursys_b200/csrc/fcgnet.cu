@@ -1218,15 +1218,21 @@ cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int 
     if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
     static int slots = 0, per_sm = 0;  // resident CTAs per device and per SM (per instantiation)
     if (!slots) {
+        // the largest shared-memory carveout, so that as many CTAs as fit
+        // by shared and tensor memory share an SM
         cudaError_t e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              G::kSmem);
-        int dev = 0, sms = 0;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        int dev = 0, sms = 0, smem_sm = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv_umma<CIN, COUT, MODE>, kUThreads, G::kSmem);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         if (e != cudaSuccess) return e;
-        slots = std::max(1, sms * std::max(1, per_sm));
+        const int by_smem = smem_sm / (G::kSmem + 2048);  // + static and reserved shared memory per CTA
+        per_sm = std::max(1, std::min(by_smem, 512 / G::kTmemCols));
+        slots = std::max(1, sms * per_sm);
     }
     // Planes per CTA. Where several CTAs share an SM: the longest march that
     // still leaves about four CTAs per resident slot over the launch
