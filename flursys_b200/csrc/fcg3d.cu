@@ -163,23 +163,26 @@ __global__ void __launch_bounds__(kPw) fcg_shift(double *x, const FcgScalars *sc
     for (long long c = blockIdx.x * (long long)kPw + threadIdx.x; c < n; c += (long long)gridDim.x * kPw) x[c] -= s;
 }
 
-// Diagonal of the Neumann-form operator at (i, j, k).
-__device__ __forceinline__ float diag7(const Geo3 &g, int i, int j, int k) {
-    return g.wx * float((i > 0) + (i + 1 < g.nx)) + g.wy * float((j > 0) + (j + 1 < g.ny)) +
-           g.wz * float((k > 0) + (k + 1 < g.nz));
-}
-
-// Smoothing passes of the preconditioner (damped Jacobi on A~, weight omega),
-// pre: z = omega D^-1 r and r - A~ z; post: z_in + omega D^-1 (r - A~ z_in),
-// and the operator pass, all as z-marching forms of the FP32 stencil passes
-// of one FCG iteration. A block
-// owns a 32 x kBY column of cells over kMZ planes; each thread keeps the
-// operand of the plane below, its own and the one above in registers, so a
-// plane is read from memory once per block (x and y neighbours come through
-// L1), and the block's partial sums are reduced once, after the march. The
-// arithmetic per cell is that of apply7 / diag7 in the same order.
-// ---------------------------------------------------------------------------
+// Smoothing passes of the preconditioner (damped Jacobi on A~, weight
+// omega; pre: z = omega D^-1 r and r - A~ z; post: z_in + omega D^-1
+// (r - A~ z_in)) and the operator pass, as z-marching FP32 stencil passes.
+// A block owns a 32 x kBY column of cells over kMZ planes; each thread keeps
+// the operand of the plane below, its own and the one above in registers,
+// so a plane is read from memory once per block (x and y neighbours come
+// through L1), and the block's partial sums are reduced once, after the
+// march. The operator arithmetic per cell is that of apply7, in its order.
 constexpr int kMZ = 16;  // planes per marching block
+
+// omega / diag of the Neumann-form operator by missing-neighbour class
+// 9 mx + 3 my + mz (FP32, formed in FP64 on the host), so the smoothing
+// passes multiply instead of dividing.
+struct SmoothW {
+    float winv[27];
+};
+__device__ __forceinline__ int miss3(int i, int n) { return (i == 0) + (i == n - 1); }
+__device__ __forceinline__ float winv_at(const SmoothW &w, const Geo3 &g, int i, int j, int k) {
+    return w.winv[9 * miss3(i, g.nx) + 3 * miss3(j, g.ny) + miss3(k, g.nz)];
+}
 
 // q = A~ d (Neumann form, FP32); partials d.q and d.r.
 __global__ void __launch_bounds__(kBX * kBY) fcg_spmv_m(Geo3 g, const float *__restrict__ d,
@@ -209,13 +212,13 @@ __global__ void __launch_bounds__(kBX * kBY) fcg_spmv_m(Geo3 g, const float *__r
 
 // Pre-smoothing: z_out = omega D^-1 r, r_out = r - A~ z_out.
 __global__ void __launch_bounds__(kBX * kBY) fcg_presmooth_m(Geo3 g, const float *__restrict__ r, float *z_out,
-                                                             float *r_out, float omega) {
+                                                             float *r_out, const __grid_constant__ SmoothW w) {
     const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5);
     const int k0 = blockIdx.z * kMZ, k1 = min(g.nz, k0 + kMZ);
     if (i >= g.nx || j >= g.ny) return;
     const long long sy = g.nx, sz = (long long)g.nx * g.ny;
     long long c = ((long long)k0 * g.ny + j) * g.nx + i;
-    auto zat = [&](long long m, int ii, int jj, int kk) { return omega * r[m] / diag7(g, ii, jj, kk); };
+    auto zat = [&](long long m, int ii, int jj, int kk) { return r[m] * winv_at(w, g, ii, jj, kk); };
     float below = k0 > 0 ? zat(c - sz, i, j, k0 - 1) : 0.f, cur = zat(c, i, j, k0);
     for (int k = k0; k < k1; ++k, c += sz) {
         const float above = k + 1 < g.nz ? zat(c + sz, i, j, k + 1) : 0.f;
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(kBX * kBY) fcg_presmooth_m(Geo3 g, const float
 __global__ void __launch_bounds__(kBX * kBY) fcg_postsmooth_m(Geo3 g, const float *__restrict__ r,
                                                               const float *__restrict__ z_pre,
                                                               const float *__restrict__ z_net, float *z_out,
-                                                              float omega) {
+                                                              const __grid_constant__ SmoothW w) {
     const int i = blockIdx.x * kBX + (threadIdx.x & 31), j = blockIdx.y * kBY + (threadIdx.x >> 5);
     const int k0 = blockIdx.z * kMZ, k1 = min(g.nz, k0 + kMZ);
     if (i >= g.nx || j >= g.ny) return;
@@ -248,7 +251,7 @@ __global__ void __launch_bounds__(kBX * kBY) fcg_postsmooth_m(Geo3 g, const floa
             return e < 0 ? below : (e > 0 ? above : zin(c + a + b * sy));
         });
         const float res = r[c] - az;
-        z_out[c] = cur + omega * res / diag7(g, i, j, k);
+        z_out[c] = cur + res * winv_at(w, g, i, j, k);
         below = cur;
         cur = above;
     }
@@ -508,7 +511,13 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     // damped-Jacobi post-smoothing (smooth = 0: the network alone).
     const char *smooth_env = std::getenv("FLURSYS_FCG_SMOOTH");
     const bool smooth = !(smooth_env && smooth_env[0] == '0');
-    const float omega = 0.8f;
+    const double omega = 0.8;
+    SmoothW sw{};
+    for (int t = 0; t < 27; ++t) {
+        const int mx = t / 9, my = (t / 3) % 3, mz = t % 3;
+        const double dg = (2 - mx) * g.wxd + (2 - my) * g.wyd + (2 - mz) * g.wzd;
+        sw.winv[t] = dg > 0.0 ? float(omega / dg) : 0.f;
+    }
     auto precondition = [&]() -> cudaError_t {
         cudaError_t m = cudaSuccess;
         if (!smooth) {
@@ -517,12 +526,12 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
             cudaEventRecord(f.e1, st);
             return m;
         }
-        fcg_presmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.t1, omega);  // t2 = z0, t1 = r - A z0
+        fcg_presmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.t1, sw);  // t2 = z0, t1 = r - A z0
         cudaEventRecord(f.e0, st);
         m = net_apply(net->w, net->ws, nx, ny, nz, h2, f.t1, f.z, st);   // z = N(r1)
         cudaEventRecord(f.e1, st);
         if (m != cudaSuccess) return m;
-        fcg_postsmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.z, f.t1, omega);  // t1 = post-smoothed z0 + N(r1)
+        fcg_postsmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.z, f.t1, sw);  // t1 = post-smoothed z0 + N(r1)
         std::swap(f.z, f.t1);                                                      // z = the preconditioned residual
         return cudaGetLastError();
     };

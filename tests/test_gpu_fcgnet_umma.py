@@ -1,7 +1,7 @@
 """The learned preconditioner's convolutions on the 5th-generation tensor
-cores (tcgen05.mma with the accumulator in tensor memory, selected by
-FLURSYS_FCG_UMMA=1) against the mma.sync kernels and the numpy oracle of the
-network, and inside the flexible CG."""
+cores (tcgen05.mma with the accumulator in tensor memory; the default,
+FLURSYS_FCG_UMMA=0 selects mma.sync) against the mma.sync kernels and the
+numpy oracle of the network, and inside the flexible CG."""
 import os
 
 import numpy as np
