@@ -731,7 +731,8 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 // in two launches. net_out_interior applies the interior-class stencil to
 // every cell: one thread per coarse cell computes its 2 x 2 x 2 fine cells,
 // reading their 6 x 6 x 6 window of r once (float2, conflict-free) from a
-// shared tile of one coarse layer and the 27 coarse neighbours of b2 once;
+// shared tile of one coarse layer and the 27 coarse neighbours of b2 once
+// from the block's staged BF16 neighbourhood (zeros outside the grid);
 // all taps are unrolled, so the weights (a by-value parameter) are
 // constant-bank operands. net_out_boundary then adds, on the cells of the
 // six faces, h2 * (K125[class] - K125[interior]) * r, the taps of c7 that
@@ -739,12 +740,18 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 constexpr int kOutCX = 32, kOutCY = 8;                       // coarse cells per block
 constexpr int kOutWX = 2 * kOutCX + 4, kOutWY = 2 * kOutCY + 4, kOutWZ = 6;  // fine window
 constexpr int kFusedInterior = 13;                            // class 1 + 3 * 1 + 9 * 1
+constexpr int kOutBX = kOutCX + 2, kOutBY = kOutCY + 2;       // coarse neighbourhood of a block
+constexpr int kOutBwin = 3 * kOutBY * 2 * kOutBX;             // its 16-byte units (two per coarse cell)
+constexpr int kOutBwinBytes = kOutBwin * 16;
 __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float *__restrict__ r,
                                                                     const uint16_t *__restrict__ b2,
                                                                     const double *scale_ptr, double h2, float *out,
                                                                     int nx, int ny, int nz,
                                                                     const __grid_constant__ NetOutParams P) {
     __shared__ __align__(16) float win[kOutWZ][kOutWY][kOutWX];
+    // the block's coarse neighbourhood of b2, BF16, zero outside the grid:
+    // [layer Z-1..Z+1][row][channel half][column] in 16-byte units
+    extern __shared__ __align__(16) uint4 bwin[];
     const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
     const int X0 = blockIdx.x * kOutCX, Y0 = blockIdx.y * kOutCY, Z = blockIdx.z;
     const int x0 = 2 * X0 - 2, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
@@ -753,6 +760,15 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
         const int x = x0 + wx, y = y0 + wy, z = z0 + wz;
         win[wz][wy][wx] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
                               ? __ldg(r + ((long long)z * ny + y) * nx + x) : 0.f;
+    }
+    for (int i = threadIdx.x; i < kOutBwin; i += blockDim.x) {
+        const int bx = i % kOutBX, h = (i / kOutBX) & 1, row = i / (2 * kOutBX);
+        const int by = row % kOutBY, bz = row / kOutBY;
+        const int Xn = X0 - 1 + bx, Yn = Y0 - 1 + by, Zn = Z - 1 + bz;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (Xn >= 0 && Yn >= 0 && Zn >= 0 && Xn < cx && Yn < cy && Zn < cz)
+            v = __ldg(reinterpret_cast<const uint4 *>(b2 + (((long long)Zn * cy + Yn) * cx + Xn) * 16) + h);
+        bwin[i] = v;
     }
     __syncthreads();
     const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
@@ -798,17 +814,16 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
         for (int oy = -1; oy <= 1; ++oy)
 #pragma unroll
             for (int ox = -1; ox <= 1; ++ox) {
-                const int Xn = X + ox, Yn = Y + oy, Zn = Z + oz;
-                if (Xn < 0 || Yn < 0 || Zn < 0 || Xn >= cx || Yn >= cy || Zn >= cz) continue;
-                const uint4 *src = reinterpret_cast<const uint4 *>(b2 + (((long long)Zn * cy + Yn) * cx + Xn) * 16);
-                const uint4 qa = __ldg(src), qb = __ldg(src + 1);
-                const uint16_t *ha = reinterpret_cast<const uint16_t *>(&qa);
-                const uint16_t *hb = reinterpret_cast<const uint16_t *>(&qb);
+                // neighbours outside the grid are staged as zeros (they add nothing)
+                const uint4 *src = bwin + ((oz + 1) * kOutBY + ty + 1 + oy) * 2 * kOutBX + tx + 1 + ox;
+                const uint4 qa = src[0], qb = src[kOutBX];
+                // BF16 pairs unpacked word by word (one integer op per value)
+                const uint32_t wv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
                 float bv[16];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    bv[j] = bf2f(ha[j]);
-                    bv[8 + j] = bf2f(hb[j]);
+                    bv[2 * j] = __uint_as_float(wv[j] << 16);
+                    bv[2 * j + 1] = __uint_as_float(wv[j] & 0xffff0000u);
                 }
 #pragma unroll
                 for (int fz = 0; fz < 2; ++fz)
@@ -1444,7 +1459,14 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     }
     if (e == cudaSuccess) {
         dim3 grid((n2x + kOutCX - 1) / kOutCX, (n2y + kOutCY - 1) / kOutCY, n2z);
-        net_out_interior<<<grid, kOutCX * kOutCY, 0, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz, w.out_params);
+        static bool configured = false;
+        if (!configured) {
+            e = cudaFuncSetAttribute(net_out_interior, cudaFuncAttributeMaxDynamicSharedMemorySize, kOutBwinBytes);
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        net_out_interior<<<grid, kOutCX * kOutCY, kOutBwinBytes, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz,
+                                                                       w.out_params);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
