@@ -691,11 +691,19 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
     const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
     const int X0 = blockIdx.x * kInCX, Y0 = blockIdx.y * kInCY, Z = blockIdx.z;
     const int x0 = 2 * X0 - 1, y0 = 2 * Y0 - 1, z0 = 2 * Z - 1;
-    for (int i = threadIdx.x; i < kInWZ * kInWY * kInWX; i += blockDim.x) {
-        const int wx = i % kInWX, wy = (i / kInWX) % kInWY, wz = i / (kInWX * kInWY);
-        const int x = x0 + wx, y = y0 + wy, z = z0 + wz;
-        win[wz][wy][wx] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
-                              ? __ldg(r + ((long long)z * ny + y) * nx + x) : 0.f;
+    {  // one window row per warp at a time, lanes along x
+        const int lane = threadIdx.x & 31;
+        for (int row = threadIdx.x >> 5; row < kInWZ * kInWY; row += blockDim.x >> 5) {
+            const int wz = row / kInWY, wy = row - wz * kInWY;
+            const int y = y0 + wy, z = z0 + wz;
+            const bool yz = y >= 0 && z >= 0 && y < ny && z < nz;
+            const float *src = r + ((long long)(yz ? z : 0) * ny + (yz ? y : 0)) * nx;
+#pragma unroll
+            for (int wx = lane; wx < kInWX; wx += 32) {
+                const int x = x0 + wx;
+                win[wz][wy][wx] = yz && x >= 0 && x < nx ? __ldg(src + x) : 0.f;
+            }
+        }
     }
     __syncthreads();
     const int tx = threadIdx.x % kInCX, ty = threadIdx.x / kInCX;
@@ -755,20 +763,34 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
     const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
     const int X0 = blockIdx.x * kOutCX, Y0 = blockIdx.y * kOutCY, Z = blockIdx.z;
     const int x0 = 2 * X0 - 2, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
-    for (int i = threadIdx.x; i < kOutWZ * kOutWY * kOutWX; i += blockDim.x) {
-        const int wx = i % kOutWX, wy = (i / kOutWX) % kOutWY, wz = i / (kOutWX * kOutWY);
-        const int x = x0 + wx, y = y0 + wy, z = z0 + wz;
-        win[wz][wy][wx] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
-                              ? __ldg(r + ((long long)z * ny + y) * nx + x) : 0.f;
-    }
-    for (int i = threadIdx.x; i < kOutBwin; i += blockDim.x) {
-        const int bx = i % kOutBX, h = (i / kOutBX) & 1, row = i / (2 * kOutBX);
-        const int by = row % kOutBY, bz = row / kOutBY;
-        const int Xn = X0 - 1 + bx, Yn = Y0 - 1 + by, Zn = Z - 1 + bz;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (Xn >= 0 && Yn >= 0 && Zn >= 0 && Xn < cx && Yn < cy && Zn < cz)
-            v = __ldg(reinterpret_cast<const uint4 *>(b2 + (((long long)Zn * cy + Yn) * cx + Xn) * 16) + h);
-        bwin[i] = v;
+    {  // one window row per warp at a time: r as float2 along x (x0 and nx are
+       // even, so a pair is inside or outside the grid as a whole), then the
+       // b2 neighbourhood row by row
+        const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        for (int row = threadIdx.x >> 5; row < kOutWZ * kOutWY; row += nw) {
+            const int wz = row / kOutWY, wy = row - wz * kOutWY;
+            const int y = y0 + wy, z = z0 + wz;
+            const bool yz = y >= 0 && z >= 0 && y < ny && z < nz;
+            const float2 *src = reinterpret_cast<const float2 *>(r + ((long long)(yz ? z : 0) * ny + (yz ? y : 0)) * nx);
+            float2 *dst = reinterpret_cast<float2 *>(&win[wz][wy][0]);
+#pragma unroll
+            for (int e = lane; e < kOutWX / 2; e += 32) {
+                const int x = x0 + 2 * e;
+                dst[e] = yz && x >= 0 && x < nx ? __ldg(src + (x >> 1)) : make_float2(0.f, 0.f);
+            }
+        }
+        for (int row = threadIdx.x >> 5; row < 3 * kOutBY * 2; row += nw) {
+            const int h = row & 1, byz = row >> 1;
+            const int bz = byz / kOutBY, by = byz - bz * kOutBY;
+            const int Yn = Y0 - 1 + by, Zn = Z - 1 + bz;
+            const bool yz = Yn >= 0 && Zn >= 0 && Yn < cy && Zn < cz;
+            const uint4 *src = reinterpret_cast<const uint4 *>(b2 + ((long long)(yz ? Zn : 0) * cy + (yz ? Yn : 0)) * cx * 16);
+#pragma unroll
+            for (int bx = lane; bx < kOutBX; bx += 32) {
+                const int Xn = X0 - 1 + bx;
+                bwin[row * kOutBX + bx] = yz && Xn >= 0 && Xn < cx ? __ldg(src + 2 * Xn + h) : make_uint4(0u, 0u, 0u, 0u);
+            }
+        }
     }
     __syncthreads();
     const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
