@@ -650,31 +650,27 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
     int error = 0;
     bool done = status == FLURSYS_LINEAR_CONVERGED || a.max_iters <= 0;
 
-    bool d_ready = false;  // the previous update pass already formed d
     while (!done) {
         // ---- d = z + beta d_old on the tile and its halo ----
         const unsigned long long t0 = gtimer();
-        if (!d_ready) {
-            const float fb = float(beta);
+        const float fb = float(beta);
 #pragma unroll
-            for (int u = 0; u < kHP; ++u) {
-                if (hpk[u] < 0) continue;
-                const int sl = hpk[u] & 0xffff, cls = hpk[u] >> 16;
-                dsm[sl] = make_d(hr[u], dsm[sl], idgf[cls == 27 ? 0 : cls], cls == 27, first, fb);
-            }
+        for (int u = 0; u < kHP; ++u) {
+            if (hpk[u] < 0) continue;
+            const int sl = hpk[u] & 0xffff, cls = hpk[u] >> 16;
+            dsm[sl] = make_d(hr[u], dsm[sl], idgf[cls == 27 ? 0 : cls], cls == 27, first, fb);
+        }
 #pragma unroll
-            for (int h = 0; h < kC; ++h) {
-                if (!in[h]) continue;
+        for (int h = 0; h < kC; ++h) {
+            if (!in[h]) continue;
 #pragma unroll
-                for (int kk = 0; kk < kResMaxTz; ++kk) {
-                    if (kk >= kz) continue;
-                    const int k = k0 + kk;
-                    const int sl = own(h, kk);
-                    dsm[sl] = make_d(r[h][kk], dsm[sl], idgf[cls_xy[h] + rmiss(k, a.nz)], pcol[h] && k == 0, first, fb);
-                }
+            for (int kk = 0; kk < kResMaxTz; ++kk) {
+                if (kk >= kz) continue;
+                const int k = k0 + kk;
+                const int sl = own(h, kk);
+                dsm[sl] = make_d(r[h][kk], dsm[sl], idgf[cls_xy[h] + rmiss(k, a.nz)], pcol[h] && k == 0, first, fb);
             }
         }
-        d_ready = false;
         __syncthreads();
         const unsigned long long t1 = gtimer();
         t_halo += t1 - t0;
@@ -754,14 +750,6 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
         const double alpha = rz / dq;
         const double rr_next = S[0] - 2.0 * alpha * S[5] + alpha * alpha * S[3];
         double rz_next = S[1] - 2.0 * alpha * S[6] + alpha * alpha * S[4];
-        // Every decision of this iteration is known before its update pass:
-        // when no residual replacement and no exit follows, the pass also
-        // forms the next direction (d_old is read once, for dx and for d).
-        double res = sqrt(fmax(rr_next, 0.0));
-        bool conv = res <= threshold;
-        const bool replace = conv || ((iterations + 1) % a.replace_every) == 0;
-        const bool fuse = isfinite(res) && !replace && !(fabs(rz) < 1.0e-30) && iterations + 1 < a.max_iters;
-        const float fbn = fuse ? float(rz_next / rz) : 0.f;
         // ---- dx += alpha d, r -= alpha q on the tile and the halo ----
         const float af = float(alpha);
         const float *fqr = face(fr);
@@ -776,31 +764,21 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
             for (int kk = 0; kk < kResMaxTz; ++kk) {
                 if (kk >= kz) continue;
                 const int l = loc(h, kk);
-                const int sl = own(h, kk);
-                const float dold = dsm[sl];
-                dxs[l] = __fmaf_rn(af, dold, dxs[l]);
+                dxs[l] = __fmaf_rn(af, dsm[own(h, kk)], dxs[l]);
                 r[h][kk] = __fmaf_rn(-af, qs[l], r[h][kk]);
-                if (fuse) {
-                    const int k = k0 + kk;
-                    dsm[sl] = make_d(r[h][kk], dold, idgf[cls_xy[h] + rmiss(k, a.nz)], pcol[h] && k == 0, false, fbn);
-                }
             }
         }
 #pragma unroll
-        for (int u = 0; u < kHP; ++u) {
-            hr[u] = __fmaf_rn(-af, hq[u], hr[u]);
-            if (fuse && hpk[u] >= 0) {
-                const int sl = hpk[u] & 0xffff, cls = hpk[u] >> 16;
-                dsm[sl] = make_d(hr[u], dsm[sl], idgf[cls == 27 ? 0 : cls], cls == 27, false, fbn);
-            }
-        }
+        for (int u = 0; u < kHP; ++u) hr[u] = __fmaf_rn(-af, hq[u], hr[u]);
         iterations += 1;
+        double res = sqrt(fmax(rr_next, 0.0));
         residual_v = res;
         if (!isfinite(res)) {
             error = FLURSYS_ERR_NON_FINITE;
             break;
         }
-        if (replace) {
+        bool conv = res <= threshold;
+        if (conv || (iterations % a.replace_every) == 0) {
             // ---- FP64 residual replacement ----
             fold();
             if (!res_sync(a)) return;
@@ -828,7 +806,6 @@ __global__ void __launch_bounds__(BLK, 1) pcg3d_res1_kernel(const __grid_constan
         if (fabs(rz) < 1.0e-30 || iterations >= a.max_iters) break;
         beta = rz_next / rz;
         first = false;
-        d_ready = fuse;
     }
     // ---- fold a pending increment, then the FP64 ||b - A x||_2 ----
     if (status != FLURSYS_LINEAR_CONVERGED) fold();
