@@ -43,6 +43,22 @@ constexpr int kPad = 8;                       // BF16 padding of a staged row
 enum StageMode { kPlain = 0, kPool = 1, kUpAdd = 2 };
 
 __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
+
+// Asynchronous global-to-shared copies of N = 4, 8 or 16 bytes; a copy with
+// `valid` false writes zeros (source size 0, the source address unread).
+template <int N>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    if (N == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(N), "r"(valid ? N : 0)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 __device__ __forceinline__ uint16_t f2bf(float f) {
     const __nv_bfloat16 h = __float2bfloat16_rn(f);
     return *reinterpret_cast<const uint16_t *>(&h);
@@ -691,7 +707,8 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
     const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
     const int X0 = blockIdx.x * kInCX, Y0 = blockIdx.y * kInCY, Z = blockIdx.z;
     const int x0 = 2 * X0 - 1, y0 = 2 * Y0 - 1, z0 = 2 * Z - 1;
-    {  // one window row per warp at a time, lanes along x
+    {  // one window row per warp at a time, lanes along x; every copy is in
+       // flight before the block waits
         const int lane = threadIdx.x & 31;
         for (int row = threadIdx.x >> 5; row < kInWZ * kInWY; row += blockDim.x >> 5) {
             const int wz = row / kInWY, wy = row - wz * kInWY;
@@ -701,9 +718,11 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 #pragma unroll
             for (int wx = lane; wx < kInWX; wx += 32) {
                 const int x = x0 + wx;
-                win[wz][wy][wx] = yz && x >= 0 && x < nx ? __ldg(src + x) : 0.f;
+                const bool ok = yz && x >= 0 && x < nx;
+                cp_async_zfill<4>(&win[wz][wy][wx], ok ? src + x : r, ok);
             }
         }
+        cp_async_wait_all();
     }
     __syncthreads();
     const int tx = threadIdx.x % kInCX, ty = threadIdx.x / kInCX;
@@ -765,7 +784,8 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
     const int x0 = 2 * X0 - 2, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
     {  // one window row per warp at a time: r as float2 along x (x0 and nx are
        // even, so a pair is inside or outside the grid as a whole), then the
-       // b2 neighbourhood row by row
+       // b2 neighbourhood row by row; every copy is in flight before the
+       // block waits
         const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
         for (int row = threadIdx.x >> 5; row < kOutWZ * kOutWY; row += nw) {
             const int wz = row / kOutWY, wy = row - wz * kOutWY;
@@ -776,7 +796,8 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
 #pragma unroll
             for (int e = lane; e < kOutWX / 2; e += 32) {
                 const int x = x0 + 2 * e;
-                dst[e] = yz && x >= 0 && x < nx ? __ldg(src + (x >> 1)) : make_float2(0.f, 0.f);
+                const bool ok = yz && x >= 0 && x < nx;
+                cp_async_zfill<8>(dst + e, ok ? src + (x >> 1) : src, ok);
             }
         }
         for (int row = threadIdx.x >> 5; row < 3 * kOutBY * 2; row += nw) {
@@ -788,9 +809,11 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
 #pragma unroll
             for (int bx = lane; bx < kOutBX; bx += 32) {
                 const int Xn = X0 - 1 + bx;
-                bwin[row * kOutBX + bx] = yz && Xn >= 0 && Xn < cx ? __ldg(src + 2 * Xn + h) : make_uint4(0u, 0u, 0u, 0u);
+                const bool ok = yz && Xn >= 0 && Xn < cx;
+                cp_async_zfill<16>(bwin + row * kOutBX + bx, ok ? src + 2 * Xn + h : src, ok);
             }
         }
+        cp_async_wait_all();
     }
     __syncthreads();
     const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
@@ -1080,6 +1103,22 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     constexpr int kItems = (kUCells * K8 + kUThreads - 1) / kUThreads;
     auto stage = [&](int p) {
         uint8_t *slot = ring + ((p + 4) & 3) * G::kSlot;
+        if (MODE == kPlain) {  // asynchronous copies, zero-filled outside the grid
+            const bool zin = p >= 0 && p < nz;
+#pragma unroll
+            for (int u = 0; u < kItems; ++u) {
+                const int idx = tid + u * kUThreads;
+                if (idx < kUCells * K8) {
+                    const int k8 = idx % K8, cell = idx / K8;
+                    const int x = x0 - 1 + cell % kUHX, y = y0 - 1 + cell / kUHX;
+                    const bool ok = zin && x >= 0 && y >= 0 && x < nx && y < ny;
+                    const uint16_t *g = ok ? src.in + (((long long)p * ny + y) * nx + x) * CIN + k8 * 8 : src.in;
+                    cp_async_zfill<16>(slot + (k8 * kUCells + cell) * 16, g, ok);
+                }
+            }
+            cp_async_wait_all();
+            return;
+        }
         uint4 v[kItems];
 #pragma unroll
         for (int u = 0; u < kItems; ++u) {
