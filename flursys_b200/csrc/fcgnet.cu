@@ -1103,22 +1103,6 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     constexpr int kItems = (kUCells * K8 + kUThreads - 1) / kUThreads;
     auto stage = [&](int p) {
         uint8_t *slot = ring + ((p + 4) & 3) * G::kSlot;
-        if (MODE == kPlain) {  // asynchronous copies, zero-filled outside the grid
-            const bool zin = p >= 0 && p < nz;
-#pragma unroll
-            for (int u = 0; u < kItems; ++u) {
-                const int idx = tid + u * kUThreads;
-                if (idx < kUCells * K8) {
-                    const int k8 = idx % K8, cell = idx / K8;
-                    const int x = x0 - 1 + cell % kUHX, y = y0 - 1 + cell / kUHX;
-                    const bool ok = zin && x >= 0 && y >= 0 && x < nx && y < ny;
-                    const uint16_t *g = ok ? src.in + (((long long)p * ny + y) * nx + x) * CIN + k8 * 8 : src.in;
-                    cp_async_zfill<16>(slot + (k8 * kUCells + cell) * 16, g, ok);
-                }
-            }
-            cp_async_wait_all();
-            return;
-        }
         uint4 v[kItems];
 #pragma unroll
         for (int u = 0; u < kItems; ++u) {
