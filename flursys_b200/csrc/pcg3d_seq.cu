@@ -764,27 +764,56 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_pipe(SeqArgs a) {
     const int i0 = (col % g.tiles_xv) * kPipeX;
     const int j0 = (col / g.tiles_xv) * kPipeY;
     const int k0 = ch * g.kcp, k1 = min(g.nz, k0 + g.kcp);
-    // staging of plane p into its ring slot (zeros outside the grid)
+    // staging of plane p into its ring slot (zeros outside the grid). The
+    // copies a thread issues are the same for every plane, so their shared
+    // offsets and in-plane global offsets (-1 outside the grid in x or y)
+    // are formed once: item u copies 16 bytes of row ry (-1 .. 16) and
+    // column group c4 of array arr (0 r, 1 d_old).
     auto slot_of = [&](int p) { return pipe_smem + ((p - k0 + 1) % kPipeSlots) * 2 * kPipeArr; };
-    auto stage = [&](int p) {
-        float *sl = slot_of(p);
-        const bool pin = p >= 0 && p < g.nz;
-        for (int e = threadIdx.x; e < 2 * kPipeRows * (kPipeX / 4); e += kBlock) {
+    constexpr int kStageN = 2 * kPipeRows * (kPipeX / 4);
+    constexpr int kStageItems = (kStageN + kBlock - 1) / kBlock;
+    int soff[kStageItems], goff[kStageItems];
+    unsigned dmask = 0u;  // bit u: item u copies d_old
+#pragma unroll
+    for (int u = 0; u < kStageItems; ++u) {
+        const int e = threadIdx.x + u * kBlock;
+        soff[u] = 0;
+        goff[u] = -2;  // -2: no item
+        if (e < kStageN) {
             const int arr = e / (kPipeRows * (kPipeX / 4)), rem = e - arr * (kPipeRows * (kPipeX / 4));
             const int ry = rem / (kPipeX / 4), c4 = rem - ry * (kPipeX / 4);
             const int j = j0 + ry - 1, i = i0 + 4 * c4;
-            const bool ok = pin && j >= 0 && j < g.ny && i < g.nx && !(arr == 1 && first);
-            const float *base = arr ? dold : r;
-            const float *src = ok ? base + ((size_t)p * g.ny + j) * g.nx + i : base;
-            cp_async16(sl + arr * kPipeArr + ry * kPipeX + 4 * c4, src, ok);
+            soff[u] = arr * kPipeArr + ry * kPipeX + 4 * c4;
+            goff[u] = (j >= 0 && j < g.ny && i < g.nx) ? j * g.nx + i : -1;
+            if (arr) dmask |= 1u << u;
         }
-        if (threadIdx.x < 4 * kPipeY) {
-            const int arr = threadIdx.x / (2 * kPipeY), side = (threadIdx.x / kPipeY) & 1, y = threadIdx.x % kPipeY;
-            const int i = side ? i0 + kPipeX : i0 - 1, j = j0 + y;
-            const bool ok = pin && i >= 0 && i < g.nx && j < g.ny && !(arr == 1 && first);
-            const float *base = arr ? dold : r;
-            const float *src = ok ? base + ((size_t)p * g.ny + j) * g.nx + i : base;
-            cp_async4(sl + arr * kPipeArr + kPipeRows * kPipeX + side * kPipeY + y, src, ok);
+    }
+    int hsoff = 0, hgoff = -2;  // the x-halo copy of threads < 4 kPipeY
+    bool hd = false;
+    if (threadIdx.x < 4 * kPipeY) {
+        const int arr = threadIdx.x / (2 * kPipeY), side = (threadIdx.x / kPipeY) & 1, y = threadIdx.x % kPipeY;
+        const int i = side ? i0 + kPipeX : i0 - 1, j = j0 + y;
+        hsoff = arr * kPipeArr + kPipeRows * kPipeX + side * kPipeY + y;
+        hgoff = (i >= 0 && i < g.nx && j < g.ny) ? j * g.nx + i : -1;
+        hd = arr != 0;
+    }
+    const size_t nxy = (size_t)g.nx * g.ny;
+    auto stage = [&](int p) {
+        float *sl = slot_of(p);
+        const bool pin = p >= 0 && p < g.nz;
+        const size_t pb = pin ? (size_t)p * nxy : 0;
+#pragma unroll
+        for (int u = 0; u < kStageItems; ++u) {
+            if (goff[u] == -2) continue;
+            const bool isd = (dmask >> u) & 1u;
+            const bool ok = pin && goff[u] >= 0 && !(isd && first);
+            const float *base = isd ? dold : r;
+            cp_async16(sl + soff[u], ok ? base + pb + goff[u] : base, ok);
+        }
+        if (hgoff != -2) {
+            const bool ok = pin && hgoff >= 0 && !(hd && first);
+            const float *base = hd ? dold : r;
+            cp_async4(sl + hsoff, ok ? base + pb + hgoff : base, ok);
         }
     };
     double sdq = 0.0;
@@ -803,17 +832,31 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_pipe(SeqArgs a) {
     const int xh = hw ? i0 - 1 : (he ? i0 + kPipeX : 0);
     const int mxh = miss(xh, g.nx);
     const int row0 = j0 + wp * 2;  // this warp's two rows
-    // d of the lane's 4 cells of tile row ry (-1 .. 16) of plane p from the staged raw inputs
-    auto make4 = [&](const float *sl, int ry, int p, float (&out)[4]) {
-        const int row = j0 + ry;
-        if (row < 0 || row >= g.ny || p < 0 || p >= g.nz || !inx) {
+    // The four tile rows this warp forms d on (ri 0 .. 3 = rows row0 - 1 ..
+    // row0 + 2): inside the grid in y, y-class 3 miss(row), holding the
+    // pinned cell (row 0, x 0).
+    bool rin[4];
+    int rcls[4];
+    bool rpin[4];
+#pragma unroll
+    for (int ri = 0; ri < 4; ++ri) {
+        const int row = row0 - 1 + ri;
+        rin[ri] = row >= 0 && row < g.ny;
+        rcls[ri] = rin[ri] ? 3 * miss(row, g.ny) : 0;
+        rpin[ri] = row == 0 && ibc == 0;
+    }
+    // d of the lane's 4 cells of row ri of plane p from the staged raw
+    // inputs; cz = miss(p, nz), pin = p inside the grid
+    auto make4 = [&](const float *sl, int ri, int p, int cz, bool pin, float (&out)[4]) {
+        if (!pin || !rin[ri] || !inx) {
             out[0] = out[1] = out[2] = out[3] = 0.f;
             return;
         }
+        const int ry = wp * 2 - 1 + ri;
         const float4 rv = *reinterpret_cast<const float4 *>(sl + (ry + 1) * kPipeX + lane * 4);
         const float4 dv = *reinterpret_cast<const float4 *>(sl + kPipeArr + (ry + 1) * kPipeX + lane * 4);
         const float rr[4] = {rv.x, rv.y, rv.z, rv.w}, dd[4] = {dv.x, dv.y, dv.z, dv.w};
-        const int cyz = 3 * miss(row, g.ny) + miss(p, g.nz);
+        const int cyz = rcls[ri] + cz;
         const float mid = idg[cyz];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -823,25 +866,30 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_pipe(SeqArgs a) {
             const float z = rr[e] * id;
             out[e] = first ? z : float(z + beta * dd[e]);
         }
-        if (p == 0 && row == 0 && ibc == 0) out[0] = 0.f;  // pinned cell
+        if (p == 0 && rpin[ri]) out[0] = 0.f;  // pinned cell
     };
-    auto make_halo = [&](const float *sl, int y, int p) -> float {  // x-halo column cell of tile row y
-        const int row = j0 + y;
-        if (!(hw || he) || row >= g.ny || p < 0 || p >= g.nz) return 0.f;
-        if (p == 0 && row == 0 && xh == 0) return 0.f;
+    auto make_halo = [&](const float *sl, int m, int p, int cz, bool pin) -> float {  // x-halo cell of own row m
+        const int ri = m + 1, y = wp * 2 + m;
+        if (!(hw || he) || !rin[ri] || !pin) return 0.f;
+        if (p == 0 && row0 + m == 0 && xh == 0) return 0.f;
         const int side = he ? 1 : 0;
         const float rv = sl[kPipeRows * kPipeX + side * kPipeY + y];
         const float dv = sl[kPipeArr + kPipeRows * kPipeX + side * kPipeY + y];
-        const float z = rv * idg[9 * mxh + 3 * miss(row, g.ny) + miss(p, g.nz)];
+        const float z = rv * idg[9 * mxh + rcls[ri] + cz];
         return first ? z : float(z + beta * dv);
     };
     float below[2][4], cur[2][4];
     asm volatile("cp.async.wait_group 2;" ::: "memory");  // planes k0 - 1, k0 landed
     __syncthreads();
+    {
+        const int pb = k0 - 1;
+        const bool pinb = pb >= 0, pinc = k0 < g.nz;
+        const int czb = pinb ? miss(pb, g.nz) : 0, czc = miss(k0, g.nz);
 #pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        make4(slot_of(k0 - 1), wp * 2 + m, k0 - 1, below[m]);
-        make4(slot_of(k0), wp * 2 + m, k0, cur[m]);
+        for (int m = 0; m < 2; ++m) {
+            make4(slot_of(pb), m + 1, pb, czb, pinb, below[m]);
+            make4(slot_of(k0), m + 1, k0, czc, pinc, cur[m]);
+        }
     }
     for (int k = k0; k < k1; ++k) {
         if (k + 3 <= k1) stage(k + 3);
@@ -850,11 +898,13 @@ __global__ void __launch_bounds__(kBlock, 2) seq_dir_pipe(SeqArgs a) {
         __syncthreads();
         const float *slk = slot_of(k), *sla = slot_of(k + 1);
         float above[2][4], ys[4], yn[4];
-        make4(sla, wp * 2, k + 1, above[0]);
-        make4(sla, wp * 2 + 1, k + 1, above[1]);
-        make4(slk, wp * 2 - 1, k, ys);
-        make4(slk, wp * 2 + 2, k, yn);
-        const float hx0 = make_halo(slk, wp * 2, k), hx1 = make_halo(slk, wp * 2 + 1, k);
+        const bool pina = k + 1 < g.nz;
+        const int cza = pina ? miss(k + 1, g.nz) : 0, czk = miss(k, g.nz);
+        make4(sla, 1, k + 1, cza, pina, above[0]);
+        make4(sla, 2, k + 1, cza, pina, above[1]);
+        make4(slk, 0, k, czk, true, ys);
+        make4(slk, 3, k, czk, true, yn);
+        const float hx0 = make_halo(slk, 0, k, czk, true), hx1 = make_halo(slk, 1, k, czk, true);
         const float wzm = k > 0 ? wz : 0.f, wzp = k + 1 < g.nz ? wz : 0.f;
 #pragma unroll
         for (int m = 0; m < 2; ++m) {
