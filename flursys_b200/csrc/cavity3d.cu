@@ -17,7 +17,6 @@ namespace flursys {
 
 namespace {
 
-constexpr int kBlk = 256;     // diagnostics block
 constexpr int kRowBlk = 128;  // threads along x of the row-mapped kernels
 
 // Grid spacings and their reciprocals (the kernels multiply by these in
@@ -52,11 +51,17 @@ __device__ __forceinline__ double unb(const double *__restrict__ u, const G3 &g,
 __global__ void __launch_bounds__(kRowBlk) predict_u(const double *__restrict__ u, const double *__restrict__ v,
                                                      const double *__restrict__ w, double *__restrict__ us,
                                                      G3 g, double dt, double nu, double lid) {
+    // threads cover i < nx (whole blocks for nx a multiple of 128); the
+    // thread of i = 0 also writes the wall face i = nx
     const int i = blockIdx.x * kRowBlk + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     const long long sx = g.nx + 1;
-    if (i >= sx) return;
+    if (i >= g.nx) return;
     const long long id = i + sx * (j + (long long)g.ny * k);
-    if (i == 0 || i == g.nx) { us[id] = 0.0; return; }
+    if (i == 0) {
+        us[id] = 0.0;
+        us[id + g.nx] = 0.0;
+        return;
+    }
     const double c = __ldg(u + id);
     const double e = __ldg(u + id + 1), wst = __ldg(u + id - 1);
     const double nn = unb(u, g, i, j, k, 1, 0, c, lid), s = unb(u, g, i, j, k, -1, 0, c, lid);
@@ -167,17 +172,21 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
 // the (nx+1) x (ny+1) x (nz+1) index box with their threads along x, so a
 // thread never divides an index; one block maximum per block goes to the
 // result.
-__global__ void __launch_bounds__(kBlk) diagnostics(const double *__restrict__ u, const double *__restrict__ v,
+__global__ void __launch_bounds__(kRowBlk) diagnostics(const double *__restrict__ u, const double *__restrict__ v,
                                                     const double *__restrict__ w, const double *__restrict__ p,
                                                     G3 g, Diag3Dev *out) {
-    __shared__ double s_red[kBlk / 32];
+    __shared__ double s_red[kRowBlk / 32];
     const int rows = (g.ny + 1) * (g.nz + 1);
-    double mdiv = 0.0, mspeed = 0.0;
+    double mdiv = 0.0, mspeed2 = 0.0;  // the speed's maximum is taken squared; sqrt is monotone
     for (int row = blockIdx.x; row < rows; row += gridDim.x) {
         const int k = row / (g.ny + 1), j = row - k * (g.ny + 1);
-        for (int i = threadIdx.x; i <= g.nx; i += kBlk) {
-            const bool xin = i < g.nx, yin = j < g.ny, zin = k < g.nz;
-            if (xin && yin && zin) {
+        const bool yin = j < g.ny, zin = k < g.nz;
+        if (threadIdx.x == 0 && yin && zin) {  // the u face i = nx of this row
+            const long long iu = g.nx + (long long)(g.nx + 1) * (j + (long long)g.ny * k);
+            if (!isfinite(__ldg(u + iu))) atomicMin(&out->bad_index[1], (unsigned long long)iu);
+        }
+        for (int i = threadIdx.x; i < g.nx; i += kRowBlk) {
+            if (yin && zin) {
                 const long long id = i + (long long)g.nx * (j + (long long)g.ny * k);
                 const long long iu = i + (long long)(g.nx + 1) * (j + (long long)g.ny * k);
                 const long long iv = i + (long long)g.nx * (j + (long long)(g.ny + 1) * k);
@@ -187,25 +196,25 @@ __global__ void __launch_bounds__(kBlk) diagnostics(const double *__restrict__ u
                 const double div = (u1 - u0) * g.idx + (v1 - v0) * g.idy + (w1 - w0) * g.idz;
                 mdiv = fmax(mdiv, fabs(div));
                 const double a = 0.5 * (u0 + u1), b = 0.5 * (v0 + v1), c = 0.5 * (w0 + w1);
-                mspeed = fmax(mspeed, sqrt(a * a + b * b + c * c));
+                mspeed2 = fmax(mspeed2, a * a + b * b + c * c);
                 if (!isfinite(__ldg(p + id))) atomicMin(&out->bad_index[0], (unsigned long long)id);
             }
-            if (yin && zin) {  // u face (i, j, k), i <= nx
+            if (yin && zin) {  // u face (i, j, k), i < nx
                 const long long iu = i + (long long)(g.nx + 1) * (j + (long long)g.ny * k);
                 if (!isfinite(__ldg(u + iu))) atomicMin(&out->bad_index[1], (unsigned long long)iu);
             }
-            if (xin && zin) {  // v face, j <= ny
+            if (zin) {  // v face, j <= ny
                 const long long iv = i + (long long)g.nx * (j + (long long)(g.ny + 1) * k);
                 if (!isfinite(__ldg(v + iv))) atomicMin(&out->bad_index[2], (unsigned long long)iv);
             }
-            if (xin && yin) {  // w face, k <= nz
+            if (yin) {  // w face, k <= nz
                 const long long iw = i + (long long)g.nx * (j + (long long)g.ny * k);
                 if (!isfinite(__ldg(w + iw))) atomicMin(&out->bad_index[3], (unsigned long long)iw);
             }
         }
     }
-    const double bd = block_max<kBlk>(mdiv, s_red);
-    const double bs = block_max<kBlk>(mspeed, s_red);
+    const double bd = block_max<kRowBlk>(mdiv, s_red);
+    const double bs = sqrt(block_max<kRowBlk>(mspeed2, s_red));
     if (threadIdx.x == 0) {
         atomic_max_nonneg(&out->max_divergence, bd);
         atomic_max_nonneg(&out->max_speed, bs);
@@ -222,7 +231,7 @@ __global__ void diag_reset(Diag3Dev *out) {
 
 cudaError_t cavity3d_predict(const Cavity3dState &s, double dt, cudaStream_t st) {
     const G3 g = make_g3(s.nx, s.ny, s.nz, s.dx, s.dy, s.dz);
-    predict_u<<<row_grid(s.nx + 1, s.ny, s.nz), kRowBlk, 0, st>>>(s.u, s.v, s.w, s.us, g, dt, s.nu, s.lid);
+    predict_u<<<row_grid(s.nx, s.ny, s.nz), kRowBlk, 0, st>>>(s.u, s.v, s.w, s.us, g, dt, s.nu, s.lid);
     predict_v<<<row_grid(s.nx, s.ny + 1, s.nz), kRowBlk, 0, st>>>(s.u, s.v, s.w, s.vs, g, dt, s.nu);
     predict_w<<<row_grid(s.nx, s.ny, s.nz + 1), kRowBlk, 0, st>>>(s.u, s.v, s.w, s.ws, g, dt, s.nu);
     return cudaGetLastError();
@@ -244,8 +253,8 @@ cudaError_t cavity3d_diagnostics(const Cavity3dState &s, Diag3Dev *out, cudaStre
     const G3 g = make_g3(s.nx, s.ny, s.nz, s.dx, s.dy, s.dz);
     diag_reset<<<1, 1, 0, st>>>(out);
     const long long rows = (long long)(s.ny + 1) * (s.nz + 1);
-    const int blocks = (int)std::min<long long>(rows, (long long)s.sms * 8);
-    diagnostics<<<blocks, kBlk, 0, st>>>(s.u, s.v, s.w, s.p, g, out);
+    const int blocks = (int)std::min<long long>(rows, (long long)s.sms * 16);
+    diagnostics<<<blocks, kRowBlk, 0, st>>>(s.u, s.v, s.w, s.p, g, out);
     return cudaGetLastError();
 }
 
