@@ -38,15 +38,6 @@ G3 make_g3(int nx, int ny, int nz, double dx, double dy, double dz) {
 // (blockIdx.y = j, blockIdx.z = k), no index division.
 dim3 row_grid(long long sx, int sy, int sz) { return dim3((unsigned)((sx + kRowBlk - 1) / kRowBlk), sy, sz); }
 
-// u_neighbor (incompressible_3d.rs:365-393) for an interior u face.
-__device__ __forceinline__ double unb(const double *__restrict__ u, const G3 &g, int i, int j, int k,
-                                      int dj, int dk, double c, double lid) {
-    const int nj = j + dj, nk = k + dk;
-    if (nj >= 0 && nj < g.ny && nk >= 0 && nk < g.nz)
-        return __ldg(u + i + (long long)(g.nx + 1) * (nj + (long long)g.ny * nk));
-    return nj >= g.ny ? 2.0 * lid - c : -c;
-}
-
 // predict_momentum, u component (incompressible_3d.rs:181-210).
 __global__ void __launch_bounds__(kRowBlk) predict_u(const double *__restrict__ u, const double *__restrict__ v,
                                                      const double *__restrict__ w, double *__restrict__ us,
@@ -64,8 +55,13 @@ __global__ void __launch_bounds__(kRowBlk) predict_u(const double *__restrict__ 
     }
     const double c = __ldg(u + id);
     const double e = __ldg(u + id + 1), wst = __ldg(u + id - 1);
-    const double nn = unb(u, g, i, j, k, 1, 0, c, lid), s = unb(u, g, i, j, k, -1, 0, c, lid);
-    const double f = unb(u, g, i, j, k, 0, 1, c, lid), b = unb(u, g, i, j, k, 0, -1, c, lid);
+    // u_neighbor (incompressible_3d.rs:365-393): ghost 2 lid - c above the
+    // top wall, -c at the other walls
+    const long long suz = sx * g.ny;
+    const double nn = (j + 1 < g.ny) ? __ldg(u + id + sx) : 2.0 * lid - c;
+    const double s = (j > 0) ? __ldg(u + id - sx) : -c;
+    const double f = (k + 1 < g.nz) ? __ldg(u + id + suz) : -c;
+    const double b = (k > 0) ? __ldg(u + id - suz) : -c;
     const long long sv = g.nx, svz = (long long)g.nx * (g.ny + 1);
     const double vb = 0.25 * (__ldg(v + (i - 1) + sv * j + svz * k) + __ldg(v + i + sv * j + svz * k) +
                               __ldg(v + (i - 1) + sv * (j + 1) + svz * k) + __ldg(v + i + sv * (j + 1) + svz * k));
