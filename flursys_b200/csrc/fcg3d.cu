@@ -405,7 +405,9 @@ struct FcgWork {
     }
     double *partials = nullptr;
     FcgScalars *sc = nullptr, *h_sc = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // two event pairs around the network (an application can be queued
+    // ahead of the one being read) and the event of the scalar read-back
+    cudaEvent_t e0[2] = {nullptr, nullptr}, e1[2] = {nullptr, nullptr}, esc = nullptr;
     cudaError_t ensure(int nx_, int ny_, int nz_) {
         if (r && nx_ == nx && ny_ == ny && nz_ == nz) return cudaSuccess;
         release();
@@ -419,8 +421,11 @@ struct FcgWork {
         if (e == cudaSuccess) e = cudaMalloc(&partials, sizeof(double) * std::max<long long>(2 * np, kDotStride * kMaxPwBlocks));
         if (e == cudaSuccess) e = cudaMalloc(&sc, sizeof(FcgScalars));
         if (e == cudaSuccess) e = cudaMallocHost(&h_sc, sizeof(FcgScalars));
-        if (e == cudaSuccess) e = cudaEventCreate(&e0);
-        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        for (int k = 0; k < 2; ++k) {
+            if (e == cudaSuccess) e = cudaEventCreate(&e0[k]);
+            if (e == cudaSuccess) e = cudaEventCreate(&e1[k]);
+        }
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&esc, cudaEventDisableTiming);
         if (e == cudaSuccess) { nx = nx_; ny = ny_; nz = nz_; }
         return e;
     }
@@ -434,12 +439,16 @@ struct FcgWork {
         }
         ndirs = 0;
         if (h_sc) cudaFreeHost(h_sc);
-        if (e0) cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
+        for (int k = 0; k < 2; ++k) {
+            if (e0[k]) cudaEventDestroy(e0[k]);
+            if (e1[k]) cudaEventDestroy(e1[k]);
+            e0[k] = e1[k] = nullptr;
+        }
+        if (esc) cudaEventDestroy(esc);
+        esc = nullptr;
         r = z = t1 = t2 = nullptr;
         partials = nullptr;
         sc = h_sc = nullptr;
-        e0 = e1 = nullptr;
         nx = ny = nz = 0;
     }
 };
@@ -520,18 +529,19 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
         const double dg = (2 - mx) * g.wxd + (2 - my) * g.wyd + (2 - mz) * g.wzd;
         sw.winv[t] = dg > 0.0 ? float(omega / dg) : 0.f;
     }
-    auto precondition = [&]() -> cudaError_t {
+    // pair: the event pair timing this application of the network
+    auto precondition = [&](int pair) -> cudaError_t {
         cudaError_t m = cudaSuccess;
         if (!smooth) {
-            cudaEventRecord(f.e0, st);
+            cudaEventRecord(f.e0[pair], st);
             m = net_apply(net->w, net->ws, nx, ny, nz, h2, f.r, f.z, st);
-            cudaEventRecord(f.e1, st);
+            cudaEventRecord(f.e1[pair], st);
             return m;
         }
         fcg_presmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.t1, sw);  // t2 = z0, t1 = r - A z0
-        cudaEventRecord(f.e0, st);
+        cudaEventRecord(f.e0[pair], st);
         m = net_apply(net->w, net->ws, nx, ny, nz, h2, f.t1, f.z, st);   // z = N(r1)
-        cudaEventRecord(f.e1, st);
+        cudaEventRecord(f.e1[pair], st);
         if (m != cudaSuccess) return m;
         fcg_postsmooth_m<<<mgrid, sblock, 0, st>>>(g, f.r, f.t2, f.z, f.t1, sw);  // t1 = post-smoothed z0 + N(r1)
         std::swap(f.z, f.t1);                                                      // z = the preconditioned residual
@@ -564,10 +574,18 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     if (e != cudaSuccess) return set_cuda_error(err, e, "FCG direction storage");
     const char *trace_env = std::getenv("FLURSYS_FCG_TRACE");  // per-iteration scalars to stderr
     const bool trace = trace_env && trace_env[0] == '1';
+    // The host reads each iteration's scalars while the GPU already runs the
+    // next iteration's preconditioner M(r), which only reads r and writes the
+    // scratch vectors: it is kept when the iteration goes on unchanged and
+    // recomputed after a residual replacement (which rewrites r); a
+    // replacement due by the iteration count is not speculated on.
+    int pair = 0;            // event pair of the application this iteration uses
+    bool pre_ready = false;  // M(r) of this iteration was queued at the end of the previous one
     for (long long it = 0; !converged && !fallback; ++it) {
         if (it >= max_iters) { fallback = true; break; }
         // z = M(r); d = z - sum_j coef_j d_j over the last m directions
-        e = precondition();
+        e = pre_ready ? cudaSuccess : precondition(pair);
+        pre_ready = false;
         DirSet ds{};
         ds.count = (int)std::min<long long>(it, mdirs);
         for (int j = 0; j < ds.count; ++j) {
@@ -588,10 +606,14 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
             fcg_finalize<<<1, 1024, 0, st>>>(f.partials, npw, kFinRR, f.sc, 0);
             e = cudaGetLastError();
         }
-        if (e == cudaSuccess) e = sync_scalars();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(f.h_sc, f.sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(f.esc, st);
+        const bool speculate = e == cudaSuccess && (it + 1) % 50 != 0 && it + 1 < max_iters;
+        if (speculate) e = precondition(1 - pair);
+        if (e == cudaSuccess) e = cudaEventSynchronize(f.esc);
         if (e != cudaSuccess) return set_cuda_error(err, e, "FCG iteration");
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, f.e0, f.e1);
+        cudaEventElapsedTime(&ms, f.e0[pair], f.e1[pair]);
         net_ms += ms;
         its = it + 1;
         if (trace)
@@ -600,7 +622,9 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
         if (f.h_sc->breakdown) { fallback = true; break; }
         res = std::sqrt(f.h_sc->rr);
         if (!std::isfinite(res)) { fallback = true; break; }
+        bool replaced = false;
         if (res <= threshold || its % 50 == 0) {  // FP64 true residual replaces r
+            replaced = true;
             e = residual_neumann();
             if (e == cudaSuccess) e = sync_scalars();
             if (e != cudaSuccess) return set_cuda_error(err, e, "FCG residual replacement");
@@ -610,6 +634,10 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
         if (its % 25 == 0) {
             if (res > 0.5 * window_res) { fallback = true; break; }
             window_res = res;
+        }
+        if (speculate && !replaced) {  // no replacement rewrote r: keep the queued M(r)
+            pre_ready = true;
+            pair = 1 - pair;
         }
     }
     rep->fcg_iterations = its;
