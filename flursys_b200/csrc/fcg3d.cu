@@ -608,7 +608,9 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
         }
         if (e == cudaSuccess) e = cudaMemcpyAsync(f.h_sc, f.sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaEventRecord(f.esc, st);
-        const bool speculate = e == cudaSuccess && (it + 1) % 50 != 0 && it + 1 < max_iters;
+        // (not when the last residual read was within 3x of the threshold:
+        // the solve is about to stop and the queued application would be lost)
+        const bool speculate = e == cudaSuccess && (it + 1) % 50 != 0 && it + 1 < max_iters && res > 3.0 * threshold;
         if (speculate) e = precondition(1 - pair);
         if (e == cudaSuccess) e = cudaEventSynchronize(f.esc);
         if (e != cudaSuccess) return set_cuda_error(err, e, "FCG iteration");
