@@ -406,13 +406,13 @@ def main(argv=None) -> int:
     ap.add_argument("--traj64", type=int, default=25)
     ap.add_argument("--traj128", type=int, default=15)
     ap.add_argument("--steps", type=int, default=25, help="steps per trajectory (pairs per step: 1 + residual iters)")
-    ap.add_argument("--epochs", type=int, default=14)
+    ap.add_argument("--epochs", type=int, default=28)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--loss", choices=["residual", "energy"], default="residual")
     ap.add_argument("--residual-iters", default="8,32,128",
                     help="Jacobi-PCG iteration counts whose (residual, error) pairs join each step's pair")
-    ap.add_argument("--iterate-rounds", default="2,4,8,11",
+    ap.add_argument("--iterate-rounds", default="2,4,8,11,16,21",
                     help="epochs before which pairs from the FCG's own iterates with the current network are added")
     ap.add_argument("--summary", default=None, help="write a JSON summary here")
     args = ap.parse_args(argv)
