@@ -992,16 +992,13 @@ int grid_1d(long long n, int per = 256) { return (int)std::max<long long>(1, std
 // commits them to an mbarrier, and the four warps read the accumulator back
 // with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. voxel rows
 // 4w..4w+3) and store it as BF16. Two accumulator buffers alternate between
-// planes, and the loop is a software pipeline over a 5-plane input ring:
-// while the MMAs of plane z run, the CTA issues the copies of input plane
-// z + 3 (cp.async, zero-filled outside the grid), waits for those of plane
-// z + 2 issued one iteration earlier, queues the MMAs of plane z + 1 into the
-// other buffer, and only then waits for plane z and stores it, so the tensor
-// pipe has the next plane's work queued during every epilogue and the input
-// loads have a whole iteration to land.
+// planes, and the loop is a software pipeline: while the MMAs of plane z
+// run, the CTA stages input plane z + 2, queues the MMAs of plane z + 1
+// into the other buffer, and only then waits for plane z and stores it, so
+// the tensor pipe has the next plane's work queued during every epilogue.
 //
 // Operands are in the K-major no-swizzle core-matrix layout (8 rows x 16 B):
-//   input ring, 5 planes: [plane][k8][cell] with cell = cy*10 + cx of the
+//   input ring, 4 planes: [plane][k8][cell] with cell = cy*10 + cx of the
 //     10 x 18 halo tile, 16 B = 8 channels per entry. For tap (dy, dx) the
 //     A operand of the 128 voxels (row m = 8 y + x) starts at cell
 //     dy*10 + dx; 8-row groups (one voxel row) are 10 cells apart (SBO 160 B)
@@ -1021,8 +1018,7 @@ template <int CIN, int COUT>
 struct UmmaConv {
     static constexpr int kSlot = (CIN / 8) * kUCells * 16;       // bytes of one staged plane
     static constexpr int kWBytes = 27 * (CIN / 8) * COUT * 16;   // all taps' weights
-    static constexpr int kRing = 5;                               // staged input planes
-    static constexpr int kSmem = kRing * kSlot + kWBytes;
+    static constexpr int kSmem = 4 * kSlot + kWBytes;
     static constexpr int kTmemCols = 2 * COUT < 32 ? 32 : 2 * COUT;  // two accumulator buffers
 };
 
@@ -1094,7 +1090,7 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     const int z1 = min(z0 + kz, nz);
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(usmem);
     uint8_t *ring = usmem;
-    uint8_t *wts = usmem + G::kRing * G::kSlot;
+    uint8_t *wts = usmem + 4 * G::kSlot;
     // weights [tap][k8][co] from W[co][tap][ci]
     for (int idx = tid; idx < 27 * K8 * COUT; idx += kUThreads) {
         const int co = idx % COUT, rest = idx / COUT;
@@ -1105,24 +1101,8 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     // input plane p into its ring slot, channels fastest; every load of a
     // thread is issued before its first store
     constexpr int kItems = (kUCells * K8 + kUThreads - 1) / kUThreads;
-    auto slot_of = [&](int p) { return (p - z0 + 1) % G::kRing; };  // ring slot of input plane p >= z0 - 1
     auto stage = [&](int p) {
-        uint8_t *slot = ring + slot_of(p) * G::kSlot;
-        if (MODE == kPlain) {  // asynchronous copies, zero-filled outside the grid
-            const bool zin = p >= 0 && p < nz;
-#pragma unroll
-            for (int u = 0; u < kItems; ++u) {
-                const int idx = tid + u * kUThreads;
-                if (idx < kUCells * K8) {
-                    const int k8 = idx % K8, cell = idx / K8;
-                    const int x = x0 - 1 + cell % kUHX, y = y0 - 1 + cell / kUHX;
-                    const bool ok = zin && x >= 0 && y >= 0 && x < nx && y < ny;
-                    const uint16_t *g = ok ? src.in + (((long long)p * ny + y) * nx + x) * CIN + k8 * 8 : src.in;
-                    cp_async_zfill<16>(slot + (k8 * kUCells + cell) * 16, g, ok);
-                }
-            }
-            return;
-        }
+        uint8_t *slot = ring + ((p + 4) & 3) * G::kSlot;
         uint4 v[kItems];
 #pragma unroll
         for (int u = 0; u < kItems; ++u) {
@@ -1143,14 +1123,9 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
             }
         }
     };
-    // planes z0 - 1 .. z0 + 1, then z0 + 2 in a group of its own
     stage(z0 - 1);
     stage(z0);
     if (z0 + 1 <= z1) stage(z0 + 1);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    if (z0 + 2 <= z1) stage(z0 + 2);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 1;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 0) {
         const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
@@ -1179,10 +1154,10 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     auto issue = [&](int z, int b) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t dbuf = tmem + (uint32_t)(b * COUT);
-        const uint64_t wdesc = umma_desc(sbase + G::kRing * G::kSlot, COUT * 16, 128);
+        const uint64_t wdesc = umma_desc(sbase + 4 * G::kSlot, COUT * 16, 128);
 #pragma unroll
         for (int dz = 0; dz < 3; ++dz) {
-            const uint64_t adesc = umma_desc(sbase + (uint32_t)(slot_of(z + dz - 1) * G::kSlot), kUCells * 16, kUHX * 16);
+            const uint64_t adesc = umma_desc(sbase + (uint32_t)(((z + dz - 1 + 4) & 3) * G::kSlot), kUCells * 16, kUHX * 16);
 #pragma unroll
             for (int t9 = 0; t9 < 9; ++t9) {
 #pragma unroll
@@ -1204,13 +1179,10 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     int failed_z = -1;
     for (int z = z0; z < z1; ++z) {
         const int b = (z - z0) & 1;
-        // Plane z + 3 goes to the slot of plane z - 2, whose last reader (the
+        // Plane z + 2 goes to the slot of plane z - 2, whose last reader (the
         // MMAs of plane z - 1) finished before the previous epilogue; the
-        // MMAs of plane z (planes z - 1 .. z + 1) run meanwhile, and the
-        // copies of plane z + 2, issued one iteration earlier, are awaited.
-        if (z + 3 <= z1) stage(z + 3);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        // MMAs of plane z (planes z - 1 .. z + 1) run meanwhile.
+        if (z + 2 <= z1) stage(z + 2);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         // The MMAs of plane z + 1 (into the other buffer, free since the
