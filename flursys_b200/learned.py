@@ -415,6 +415,8 @@ def main(argv=None) -> int:
     ap.add_argument("--iterate-rounds", default="2,4,8,11,16,21",
                     help="epochs before which pairs from the FCG's own iterates with the current network are added")
     ap.add_argument("--summary", default=None, help="write a JSON summary here")
+    ap.add_argument("--init", default=None,
+                    help="start from these weights (a .flnt file) instead of a fresh initialisation")
     args = ap.parse_args(argv)
     t0 = time.time()
     plan = [(64, args.traj64, args.steps), (128, args.traj128, args.steps)]
@@ -422,7 +424,7 @@ def main(argv=None) -> int:
     ks = tuple(int(k) for k in args.residual_iters.split(",") if k)
     pairs = generate_pairs(plan, args.seed, residual_iters=ks, log=lambda s: print(s, flush=True))
     gen_s = time.time() - t0
-    params = init_params(args.seed)
+    params = read_weights(args.init) if args.init else init_params(args.seed)
     kind = _abi.FCG_LOSS_RESIDUAL if args.loss == "residual" else _abi.FCG_LOSS_ENERGY
     rounds = tuple(int(k) for k in args.iterate_rounds.split(",") if k)
     res = train(pairs, params, args.epochs, lr=args.lr, batch=args.batch, seed=args.seed, loss_kind=kind,
@@ -431,7 +433,8 @@ def main(argv=None) -> int:
     summary = {"pairs": len(pairs), "plan": plan, "residual_iters": ks, "loss": args.loss,
                "generate_s": gen_s, "train_s": res["train_s"],
                "adam_steps": res["adam_steps"], "loss_history": res["loss_history"], "out": args.out,
-               "seed": args.seed}
+               "seed": args.seed, "epochs": args.epochs, "lr": args.lr, "iterate_rounds": list(rounds),
+               "init": args.init}
     print(json.dumps(summary), flush=True)
     if args.summary:
         with open(args.summary, "w") as f:
