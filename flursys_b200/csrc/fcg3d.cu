@@ -24,9 +24,10 @@
 // local receptive field cannot. The first step is the network's initial guess,
 // scaled by the A-optimal alpha. Precision as in the mixed PCG: r, z, d, q
 // and the stencil in FP32, x and every dot in FP64, the FP32 residual replaced
-// by the FP64 true residual b - A x every 50 iterations and before the stop
-// test is accepted, so ||b - A x||_2 <= atol + rtol ||b - A x0||_2 holds for
-// the FP64 solution exactly as for the plain PCG.
+// by the FP64 true residual b - A x every 50 iterations, whenever it has
+// fallen 1000-fold since the last replacement, and before the stop test is
+// accepted, so ||b - A x||_2 <= atol + rtol ||b - A x0||_2 holds for the FP64
+// solution exactly as for the plain PCG.
 //
 // Fallback: when the residual has not halved over 25 iterations, a search
 // direction breaks down, or the FCG iteration cap is reached, the plain
@@ -565,6 +566,12 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     long long its = 0;
     bool converged = r0 <= threshold, fallback = false;
     double window_res = res;
+    // residual at the last replacement (or the start): the FP32 recurrence
+    // is replaced by the FP64 true residual once it has fallen 1000-fold
+    // below it, so the rounding the recurrence accumulated while the
+    // residual was large never exceeds ~1e-4 of the current residual
+    // (reliable updates, after van der Vorst and Ye)
+    double rep_ref = res;
     // stored directions (1..8): 6 by default (measured at 256^3 on B200:
     // m = 6 and 8 take the same ~197 iterations, 6 moves 2 x 2 fewer vectors
     // per iteration; m = 4 needs ~250)
@@ -625,12 +632,13 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
         res = std::sqrt(f.h_sc->rr);
         if (!std::isfinite(res)) { fallback = true; break; }
         bool replaced = false;
-        if (res <= threshold || its % 50 == 0) {  // FP64 true residual replaces r
+        if (res <= threshold || its % 50 == 0 || res < 1.0e-3 * rep_ref) {  // FP64 true residual replaces r
             replaced = true;
             e = residual_neumann();
             if (e == cudaSuccess) e = sync_scalars();
             if (e != cudaSuccess) return set_cuda_error(err, e, "FCG residual replacement");
             res = std::sqrt(f.h_sc->rr);
+            rep_ref = res;
             if (res <= threshold) { converged = true; break; }
         }
         if (its % 25 == 0) {
