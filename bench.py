@@ -466,6 +466,9 @@ def run_ours(args):
         if args.big_size and not args.no_big:
             line["pcg_big"] = big_solve(args.big_size, precision, local, args.repeats)
             line["fcg_big"] = fcg_solve(args.big_size, precision, local, line["pcg_big"], args.repeats)
+            # the learned FCG on the headline workload, against the timed PCG steps above
+            pcg_here = {"pressure_solve_ms_median": statistics.median(solve_ms), "pressure_iterations": its}
+            line["fcg_headline"] = fcg_solve(n, precision, local, pcg_here, args.repeats)
         if not args.no_extra:
             line["batch2d"], errors["batch2d_subset_mixed"] = batch2d_run(local)
             line["cavity2d_128"] = cavity2d_run(local)
