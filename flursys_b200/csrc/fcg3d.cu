@@ -523,7 +523,10 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     // damped-Jacobi post-smoothing (smooth = 0: the network alone).
     const char *smooth_env = std::getenv("FLURSYS_FCG_SMOOTH");
     const bool smooth = !(smooth_env && smooth_env[0] == '0');
-    const double omega = 0.8;
+    // damped-Jacobi weight of the smoothers (FLURSYS_FCG_OMEGA, 0 < omega < 2)
+    const char *omega_env = std::getenv("FLURSYS_FCG_OMEGA");
+    const double omega_set = omega_env ? std::atof(omega_env) : 0.8;
+    const double omega = omega_set > 0.0 && omega_set < 2.0 ? omega_set : 0.8;
     SmoothW sw{};
     for (int t = 0; t < 27; ++t) {
         const int mx = t / 9, my = (t / 3) % 3, mz = t % 3;
