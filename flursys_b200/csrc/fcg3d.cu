@@ -10,8 +10,7 @@
 // the pin's global offset. Directions are kept mean-free.
 //
 // FCG(m) (Notay, "Flexible conjugate gradients", SIAM J. Sci. Comput. 22,
-// 2000: truncated A-orthogonalisation against the last m directions, m = 6
-// by default, up to 8):
+// 2000: truncated A-orthogonalisation against the last m directions, m = 8):
 //   z = M(r);  d = z - sum_j (z.q_j)/(d_j.q_j) d_j
 //   q = A d;   alpha = (d.r)/(d.q);  x += alpha d;  r -= alpha q
 // With one stored direction (m = 1) a preconditioner that is not symmetric
@@ -56,7 +55,7 @@ constexpr int kBX = 32, kBY = 8;
 constexpr int kPw = 256;           // pointwise block
 constexpr int kMaxPwBlocks = 1184;
 constexpr int kMaxM = 8;           // stored directions of FCG(m), at most
-constexpr int kDefaultM = 6;       // and by default
+constexpr int kDefaultM = 8;       // and by default
 constexpr int kDotStride = kMaxM + 2;  // partials per block of the direction dots
 
 struct FcgScalars {
@@ -575,9 +574,9 @@ int32_t fcg_solve(FlursysFcgNet *net, int nx, int ny, int nz, double dx, double 
     // residual was large never exceeds ~1e-4 of the current residual
     // (reliable updates, after van der Vorst and Ye)
     double rep_ref = res;
-    // stored directions (1..8): 6 by default (measured at 256^3 on B200:
-    // m = 6 and 8 take the same ~197 iterations, 6 moves 2 x 2 fewer vectors
-    // per iteration; m = 4 needs ~250)
+    // stored directions (1..8): 8 by default (measured at 256^3 on B200 with
+    // the shipped network: 67-70 iterations and 121.6 ms per warm-started
+    // solve for m = 8, 69-74 and 124.9 ms for m = 6, 76-84 for m = 4)
     const char *m_env = std::getenv("FLURSYS_FCG_M");
     const int mdirs = m_env ? std::max(1, std::min(kMaxM, std::atoi(m_env))) : kDefaultM;
     e = f.ensure_dirs(mdirs);
