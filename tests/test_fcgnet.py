@@ -205,3 +205,25 @@ def test_fcg_cavity_steps_match_f64_oracle(oracle):
         assert r.pressure_true_relative_residual <= 1e-8 * 1.01
     for fid in (_abi.FIELD_U, _abi.FIELD_V, _abi.FIELD_W):
         assert rel_l2(gpu.download(fid), ref.get(fid)) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [64, 128])
+def test_fcg_steps_from_rest_converge_without_fallback(oracle, n):
+    # the first steps from rest start from residuals 1e8 above the stop
+    # threshold: the FP32 recurrence must be replaced by the FP64 residual as
+    # it falls (reliable updates), or it stalls at its rounding floor and the
+    # step ends in the Jacobi-PCG fallback
+    from flursys_b200 import _abi
+    from flursys_b200.solver import _Handle
+    w = _weights_or_skip()
+    from .test_gpu_cavity3d import cfg3d
+    cfg = cfg3d(oracle, n, n, n, rtol=1e-8, precision=_abi.PRECISION_MIXED)
+    cfg.pressure_solver = _abi.PRESSURE_FCG
+    cfg.fcg_weights_path = os.fsencode(w)
+    gpu = _Handle(cfg)
+    for _ in range(4):
+        r = gpu.step(1)
+        assert r.pressure_status == _abi.LINEAR_CONVERGED
+        assert r.fcg_fallback == 0
+        assert r.pressure_true_relative_residual <= 1e-8 * 1.01
