@@ -27,7 +27,6 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
-#include <cstring>
 
 #include "common.cuh"
 #include "fcgnet.cuh"
@@ -44,26 +43,6 @@ constexpr int kPad = 8;                       // BF16 padding of a staged row
 enum StageMode { kPlain = 0, kPool = 1, kUpAdd = 2 };
 
 __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float(uint32_t(b) << 16); }
-
-// Two FP32 lanes in one 64-bit register (low lane first) and their
-// lane-wise fused multiply-add (fma.rn.f32x2, sm_100a).
-__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(__float_as_uint(lo)), "r"(__float_as_uint(hi)));
-    return r;
-}
-__device__ __forceinline__ void unpack_f32x2(unsigned long long v, float &lo, float &hi) {
-    uint32_t a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=r"(a), "=r"(b) : "l"(v));
-    lo = __uint_as_float(a);
-    hi = __uint_as_float(b);
-}
-__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
-                                                        unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
 
 // Asynchronous global-to-shared copies of N = 4, 8 or 16 bytes; a copy with
 // `valid` false writes zeros (source size 0, the source address unread).
@@ -840,10 +819,10 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
     const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
     const int X = X0 + tx, Y = Y0 + ty;
     if (X >= cx || Y >= cy) return;
-    // skip path: acc[f], f = fx + 2 fy + 4 fz. The two fine cells of a pair
-    // (fx = 0, 1) share every weight, so they accumulate in one two-lane FMA
-    // (fma.rn.f32x2: each lane rounds as fmaf, in the same order).
-    unsigned long long acc2[4] = {0ull, 0ull, 0ull, 0ull};  // pair (fx = 0, 1) of acc[2 fy + 4 fz]
+    // skip path: acc[f], f = fx + 2 fy + 4 fz
+    float acc[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) acc[f] = 0.f;
 #pragma unroll
     for (int pz = 0; pz < 6; ++pz) {
 #pragma unroll
@@ -851,9 +830,6 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
             const float2 *row = reinterpret_cast<const float2 *>(&win[pz][2 * ty + py][2 * tx]);
             const float2 a = row[0], b = row[1], c = row[2];
             const float v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
-            unsigned long long vp[5];  // (v[i], v[i + 1])
-#pragma unroll
-            for (int i = 0; i < 5; ++i) vp[i] = pack_f32x2(v[i], v[i + 1]);
 #pragma unroll
             for (int fz = 0; fz < 2; ++fz) {
                 const int dz = pz - 2 - fz;
@@ -863,16 +839,15 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
                     const int dy = py - 2 - fy;
                     if (dy < -2 || dy > 2) continue;
 #pragma unroll
-                    for (int dx = -2; dx <= 2; ++dx)
-                        acc2[fy + 2 * fz] =
-                            fma_f32x2(P.k2[((dz + 2) * 5 + dy + 2) * 5 + dx + 2], vp[dx + 2], acc2[fy + 2 * fz]);
+                    for (int fx = 0; fx < 2; ++fx)
+#pragma unroll
+                        for (int dx = -2; dx <= 2; ++dx)
+                            acc[fx + 2 * fy + 4 * fz] =
+                                fmaf(P.k[((dz + 2) * 5 + dy + 2) * 5 + dx + 2], v[fx + dx + 2], acc[fx + 2 * fy + 4 * fz]);
                 }
             }
         }
     }
-    float acc[8];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) unpack_f32x2(acc2[q], acc[2 * q], acc[2 * q + 1]);
     // up path: coarse neighbour (X + ox, Y + oy, Z + oz) feeds child f when
     // o - (f == 0 ? -1 : 0) is 0 or 1 on every axis (that bit picks c8)
     float up[8];
@@ -1501,11 +1476,6 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
         if (e != cudaSuccess) return e;
         for (int c = 0; c < 16; ++c)
             for (int o = 0; o < 64; ++o) w.in_params.k2[o * 16 + c] = k2[c * 64 + o];
-        for (int t = 0; t < 125; ++t) {
-            uint32_t b;
-            std::memcpy(&b, &P.k[t], sizeof b);
-            P.k2[t] = ((unsigned long long)b << 32) | b;
-        }
         w.host_params_valid = true;
     }
     {

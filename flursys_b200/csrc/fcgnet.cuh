@@ -59,7 +59,6 @@ struct NetWorkspace {
 struct NetOutParams {
     float k[125];         // (dz * 5 + dy) * 5 + dx, offsets -2..2
     float wp[8 * 8 * 16]; // [fine parity][coarse cell][channel]
-    unsigned long long k2[125];  // k as packed pairs {k, k} for the two-lane FMAs
 };
 
 // Composite input stencil (pool o c1, 4x4x4 of stride 2, 16 outputs), by value.
