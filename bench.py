@@ -17,20 +17,24 @@ Arms:
                      host threads, bounded sample of the same workload; its
                      configuration is built by the oracle alone.
 Extra keys on the same JSON object (rank 0): the 256^3 plain-PCG solve and
-the learned-FCG solve at the same stop rule (pcg_big, fcg_big), the batched
+the learned-FCG solve at the same stop rule (pcg_big, fcg_big), the learned
+FCG on the 128^3 workload beside the timed PCG steps (fcg_headline), the batched
 2D cavities (batch2d), the 2D 128^2 cavity (cavity2d_128), the steady
 SIMPLE channel (simple_channel), and `error_vs_oracle`: the error of each
 workload's fields against the FP64 oracle run on the same inputs.
 Multi-GPU (torchrun): replicas only — every rank advances its own cavity; no
 collective is on the data path.
 
-Single sub-measurements for profilers (one JSON line each, no oracle):
+Single sub-measurements for profilers (one JSON line each, no oracle except
+--case errors3d):
   --case pcg       the 3D pressure solve's per-phase split (--size, --steps, --iters)
   --case velocity  the 3D step's velocity kernels: steps with a 1-iteration solve
   --case fcgnet    network applications on a random residual (--size, --reps)
   --case fcg       3D cavity steps with the learned FCG (--size, --steps)
   --case batch2d   batched 2D cavity steps (--instances, --steps)
   --case simple    SIMPLE channel outer iterations (--nx, --ny, --outer)
+  --case errors3d  mixed PCG and learned FCG steps from rest against the FP64
+                   oracle's steps (all host threads) at --size, --steps
 """
 from __future__ import annotations
 
@@ -823,7 +827,20 @@ def case_simple(args) -> dict:
             "solve_ms": r.solve_ms, "pressure_pcg_iterations": int(r.pressure.iterations)}
 
 
-CASES = {"pcg": case_pcg, "velocity": case_velocity, "fcgnet": case_fcgnet, "fcg": case_fcg,
+def case_errors3d(args) -> dict:
+    """The mixed PCG and the learned FCG against the FP64 oracle on the
+    n^3 cavity, `steps` steps from rest (the oracle on all host threads)."""
+    import torch
+    t0 = time.perf_counter()
+    steps, secs, its, ref = cpu_reference_run(args.size, args.steps, 1e9, os.cpu_count() or 1)
+    out = {"case": "errors3d", "size": args.size, "steps": steps, "oracle_pressure_iterations": its,
+           "oracle_seconds": secs}
+    out.update(cavity3d_errors(args.size, steps, ref, torch.device("cuda", 0)))
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+CASES = {"errors3d": case_errors3d, "pcg": case_pcg, "velocity": case_velocity, "fcgnet": case_fcgnet, "fcg": case_fcg,
          "batch2d": case_batch2d, "simple": case_simple}
 
 
