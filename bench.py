@@ -830,12 +830,11 @@ def case_simple(args) -> dict:
 def case_errors3d(args) -> dict:
     """The mixed PCG and the learned FCG against the FP64 oracle on the
     n^3 cavity, `steps` steps from rest (the oracle on all host threads)."""
-    import torch
     t0 = time.perf_counter()
     steps, secs, its, ref = cpu_reference_run(args.size, args.steps, 1e9, os.cpu_count() or 1)
     out = {"case": "errors3d", "size": args.size, "steps": steps, "oracle_pressure_iterations": its,
            "oracle_seconds": secs}
-    out.update(cavity3d_errors(args.size, steps, ref, torch.device("cuda", 0)))
+    out.update(cavity3d_errors(args.size, steps, ref, 0))
     out["seconds"] = time.perf_counter() - t0
     return out
 
