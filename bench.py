@@ -682,8 +682,20 @@ def cavity2d_run(device, n=128, steps=1000):
     rep = h.step(steps)
     secs = time.perf_counter() - t0
     h.close()
+    # compulsory FP64 bytes per cell and step: predictor 4, RHS 3, correction
+    # 5 values, and 11 per PCG iteration (the last step's count stands for all)
+    its = int(rep.pressure_iterations)
+    bytes_step = n * n * 8.0 * (12 + 11 * its)
+    peak = FALLBACK_HBM_GBS
+    try:
+        peak = float(json.load(open(PEAKS_FILE))["hbm_gbs"])
+    except Exception:
+        pass
+    hbm = bytes_step * steps / secs / 1e9
     return {"cells": n * n, "steps": steps, "seconds": secs, "cell_steps_per_s": n * n * steps / secs,
-            "last_pressure_iterations": int(rep.pressure_iterations), "last_dt": rep.time_step}
+            "last_pressure_iterations": its, "last_dt": rep.time_step,
+            "hbm_gbs_equivalent": hbm, "hbm_frac": hbm / peak,
+            "bound": "latency: the whole state (~1.3 MB) stays on the chip"}
 
 
 def roofline(n_cells, its, solve_ms, precision, resident=False):
