@@ -862,10 +862,11 @@ bool pcg3d_res_plan(Pcg3dResPlan &plan, const Pcg3dArgs &args, int device) {
     // one reduction per iteration for the L2 stop rule (FLURSYS_PCG_RESIDENT=2
     // keeps the two-reduction form)
     plan.single = args.stop_rule == FLURSYS_STOP_REL_L2 && !(env && std::strcmp(env, "2") == 0);
-    // column sums of the dot products in FP32 (default) or every product in
-    // FP64 (FLURSYS_PCG_RES_DOTS=64)
+    // every product of the dot products in FP64 (default: the CG inner
+    // products are FP64 throughout) or each column's products summed in FP32
+    // first (FLURSYS_PCG_RES_DOTS=32)
     const char *denv = std::getenv("FLURSYS_PCG_RES_DOTS");
-    plan.col32 = !(denv && std::atoi(denv) == 64);
+    plan.col32 = denv && std::atoi(denv) == 32;
     plan.block = kResBlock;
     plan.kernel = !plan.single ? (const void *)pcg3d_res2_kernel
                   : plan.col32 ? (const void *)pcg3d_res1_kernel<kResBlock, true>

@@ -40,7 +40,7 @@ struct Pcg3dResPlan {
     bool single = false;             // single-reduction form (L2 stop rule)
     const void *kernel = nullptr;    // the launched kernel
     int block = 512;                 // its threads per block
-    bool col32 = true;               // dot products: FP32 column sums, FP64 across columns
+    bool col32 = false;              // dot products: every product in FP64, or FP32 column sums
     int grid = 0;
     size_t smem = 0;
     double *partials = nullptr;
