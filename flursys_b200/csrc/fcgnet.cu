@@ -694,6 +694,40 @@ __global__ void pack_fused(const float *master, long long off_first, long long o
     }
 }
 
+// The up path of the fused output layer as a GEMM on the tensor cores:
+// up[cell][par] = sum over the 27 coarse offsets o and 16 channels ci of
+// b2[cell + o][ci] * Wo[o][ci][par], with Wo[o][ci][par] = Wp[par][c8][ci]
+// when coarse neighbour o feeds fine child par (c8 its bit pattern) and 0
+// otherwise. B operands of mma.m16n8k16 (K = ci, N = par) in fragment order,
+// each weight split into BF16 hi + lo (hi + lo = the FP32 weight to ~2^-17):
+// upfrag[((o * 2 + split) * 32 + lane) * 2 + reg], reg 0 holding
+// k = 2 (lane & 3) + {0, 1} and reg 1 k + 8, of column n = lane >> 2, the
+// lower k in the low half.
+constexpr int kUpFragWords = 27 * 2 * 32 * 2;
+
+__device__ __forceinline__ float up_weight(const float *wp, int o, int n, int k) {
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
+    const int bx = ox + ((n & 1) ? 0 : 1), by = oy + ((n & 2) ? 0 : 1), bz = oz + ((n & 4) ? 0 : 1);
+    if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) return 0.f;
+    return wp[(n * 8 + (bx | (by << 1) | (bz << 2))) * 16 + k];
+}
+
+__global__ void pack_upfrag(const float *fz, uint32_t *upfrag) {
+    const float *wp = fz + kFusedWp;
+    for (int i = threadIdx.x; i < kUpFragWords; i += blockDim.x) {
+        const int reg = i & 1, lane = (i >> 1) & 31, split = (i >> 6) & 1, o = i >> 7;
+        const int n = lane >> 2, k = 2 * (lane & 3) + 8 * reg;
+        uint32_t word = 0;
+        for (int e = 0; e < 2; ++e) {
+            const float w = up_weight(wp, o, n, k + e);
+            const uint16_t hi = f2bf(w);
+            const uint16_t v = split ? f2bf(w - bf2f(hi)) : hi;
+            word |= uint32_t(v) << (16 * e);
+        }
+        upfrag[i] = word;
+    }
+}
+
 // x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz): one thread per
 // coarse cell, its 4 x 4 x 4 window of r read from a shared tile of one
 // coarse layer (float2, conflict-free), the 1024 weights a by-value
@@ -756,14 +790,18 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 
 // z = (sum over 8 coarse cells of Wp * b2 + scale * K125[class] * r) * h2 / scale,
 // in two launches. net_out_interior applies the interior-class stencil to
-// every cell: one thread per coarse cell computes its 2 x 2 x 2 fine cells,
-// reading their 6 x 6 x 6 window of r once (float2, conflict-free) from a
-// shared tile of one coarse layer and the 27 coarse neighbours of b2 once
-// from the block's staged BF16 neighbourhood (zeros outside the grid);
-// all taps are unrolled, so the weights (a by-value parameter) are
-// constant-bank operands. net_out_boundary then adds, on the cells of the
-// six faces, h2 * (K125[class] - K125[interior]) * r, the taps of c7 that
-// leave the domain.
+// every cell: one thread per coarse cell computes its 2 x 2 x 2 fine cells
+// from their 6 x 6 x 6 window of r, read once (float2, conflict-free) from a
+// shared tile of one coarse layer, all 125 taps unrolled with the weights a
+// by-value parameter (constant-bank operands). The up path runs on the
+// tensor cores: each warp (one row of 32 coarse cells) takes the GEMM
+// [32 cells x (27 offsets x 16 channels)] x [.. x 8 children] as 27 x 2
+// mma.m16n8k16 per weight split, A by ldmatrix from the block's staged BF16
+// b2 neighbourhood (zeros outside the grid; 8 consecutive cells are 128
+// contiguous bytes, conflict-free), B from upfrag, and hands each cell its
+// 8 sums through shared memory. net_out_boundary then adds, on the cells of
+// the six faces, h2 * (K125[class] - K125[interior]) * r, the taps of c7
+// that leave the domain.
 constexpr int kOutCX = 32, kOutCY = 8;                       // coarse cells per block
 constexpr int kOutWX = 2 * kOutCX + 4, kOutWY = 2 * kOutCY + 4, kOutWZ = 6;  // fine window
 constexpr int kFusedInterior = 13;                            // class 1 + 3 * 1 + 9 * 1
@@ -772,6 +810,7 @@ constexpr int kOutBwin = 3 * kOutBY * 2 * kOutBX;             // its 16-byte uni
 constexpr int kOutBwinBytes = kOutBwin * 16;
 __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float *__restrict__ r,
                                                                     const uint16_t *__restrict__ b2,
+                                                                    const uint32_t *__restrict__ upfrag,
                                                                     const double *scale_ptr, double h2, float *out,
                                                                     int nx, int ny, int nz,
                                                                     const __grid_constant__ NetOutParams P) {
@@ -816,8 +855,54 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
         cp_async_wait_all();
     }
     __syncthreads();
-    const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;
+    const int tx = threadIdx.x % kOutCX, ty = threadIdx.x / kOutCX;  // warp ty, lane tx
     const int X = X0 + tx, Y = Y0 + ty;
+    // up path: coarse neighbour (X + ox, Y + oy, Z + oz) feeds child f when
+    // o - (f == 0 ? -1 : 0) is 0 or 1 on every axis (that bit picks c8).
+    // Every warp runs it (the MMAs are warp-wide; the staged neighbourhood
+    // covers cells past the grid's edge as zeros).
+    float up[8];
+    {
+        const int lane = tx;
+        float cf[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) cf[mt][i] = 0.f;
+        // ldmatrix rows: lane l addresses cell (l & 7) + 8 ((l >> 3) & 1) of
+        // the 16-cell tile, channel half l >> 4
+        const int arow = (lane & 7) + 8 * ((lane >> 3) & 1), ahalf = lane >> 4;
+        const uint2 *bf = reinterpret_cast<const uint2 *>(upfrag) + lane;
+#pragma unroll 3
+        for (int o = 0; o < 27; ++o) {
+            const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
+            const uint2 bh = __ldg(bf + (o * 2) * 32), bl = __ldg(bf + (o * 2 + 1) * 32);
+            const uint4 *rowp = bwin + (((oz + 1) * kOutBY + ty + 1 + oy) * 2 + ahalf) * kOutBX + arow + 1 + ox;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                uint32_t a0, a1, a2, a3;
+                ldsm_x4(a0, a1, a2, a3, rowp + 16 * mt);
+                mma_bf16(cf[mt], a0, a1, a2, a3, bh.x, bh.y);
+                mma_bf16(cf[mt], a0, a1, a2, a3, bl.x, bl.y);
+            }
+        }
+        // accumulator (row g = lane >> 2 and g + 8 of tile mt, columns
+        // 2 (lane & 3) + {0, 1}) to the cell's thread: bwin is free once
+        // every warp has read it
+        __syncthreads();
+        float *ex = reinterpret_cast<float *>(bwin) + ty * 32 * 8;
+        const int g = lane >> 2, c2 = 2 * (lane & 3);
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            *reinterpret_cast<float2 *>(ex + (16 * mt + g) * 8 + c2) = make_float2(cf[mt][0], cf[mt][1]);
+            *reinterpret_cast<float2 *>(ex + (16 * mt + g + 8) * 8 + c2) = make_float2(cf[mt][2], cf[mt][3]);
+        }
+        __syncwarp();
+        const float4 u0 = reinterpret_cast<const float4 *>(ex + lane * 8)[0];
+        const float4 u1 = reinterpret_cast<const float4 *>(ex + lane * 8)[1];
+        up[0] = u0.x; up[1] = u0.y; up[2] = u0.z; up[3] = u0.w;
+        up[4] = u1.x; up[5] = u1.y; up[6] = u1.z; up[7] = u1.w;
+    }
     if (X >= cx || Y >= cy) return;
     // skip path: acc[f], f = fx + 2 fy + 4 fz
     float acc[8];
@@ -848,44 +933,6 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
             }
         }
     }
-    // up path: coarse neighbour (X + ox, Y + oy, Z + oz) feeds child f when
-    // o - (f == 0 ? -1 : 0) is 0 or 1 on every axis (that bit picks c8)
-    float up[8];
-#pragma unroll
-    for (int f = 0; f < 8; ++f) up[f] = 0.f;
-#pragma unroll
-    for (int oz = -1; oz <= 1; ++oz)
-#pragma unroll
-        for (int oy = -1; oy <= 1; ++oy)
-#pragma unroll
-            for (int ox = -1; ox <= 1; ++ox) {
-                // neighbours outside the grid are staged as zeros (they add nothing)
-                const uint4 *src = bwin + ((oz + 1) * kOutBY + ty + 1 + oy) * 2 * kOutBX + tx + 1 + ox;
-                const uint4 qa = src[0], qb = src[kOutBX];
-                // BF16 pairs unpacked word by word (one integer op per value)
-                const uint32_t wv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
-                float bv[16];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    bv[2 * j] = __uint_as_float(wv[j] << 16);
-                    bv[2 * j + 1] = __uint_as_float(wv[j] & 0xffff0000u);
-                }
-#pragma unroll
-                for (int fz = 0; fz < 2; ++fz)
-#pragma unroll
-                    for (int fy = 0; fy < 2; ++fy)
-#pragma unroll
-                        for (int fx = 0; fx < 2; ++fx) {
-                            const int bx = ox + (fx == 0 ? 1 : 0), by = oy + (fy == 0 ? 1 : 0), bz = oz + (fz == 0 ? 1 : 0);
-                            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-                            const int par = fx | (fy << 1) | (fz << 2), c8 = bx | (by << 1) | (bz << 2);
-                            const float *w = P.wp + (par * 8 + c8) * 16;
-                            float t = up[par];
-#pragma unroll
-                            for (int j = 0; j < 16; ++j) t = fmaf(w[j], bv[j], t);
-                            up[par] = t;
-                        }
-            }
     const double s = scale_ptr[0];
     const double fac = s > 0.0 ? h2 / s : 0.0;
 #pragma unroll
@@ -1433,6 +1480,7 @@ cudaError_t NetWeights::allocate() {
     if (e == cudaSuccess) e = cudaMalloc(&bwd, n * 2);
     if (e == cudaSuccess) e = cudaMalloc(&fwd_f32, 1296 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&fused, kFusedCount * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&upfrag, kUpFragWords * sizeof(uint32_t));
     return e;
 }
 
@@ -1441,14 +1489,17 @@ void NetWeights::release() {
     if (bwd) cudaFree(bwd);
     if (fwd_f32) cudaFree(fwd_f32);
     if (fused) cudaFree(fused);
+    if (upfrag) cudaFree(upfrag);
     fwd = bwd = nullptr;
     fwd_f32 = fused = nullptr;
+    upfrag = nullptr;
 }
 
 cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st) {
     const long long n = net_param_count();
     pack_kernel<<<grid_1d(n), 256, 0, st>>>(master, w.fwd, w.bwd, w.fwd_f32, n);
     pack_fused<<<1, 256, 0, st>>>(master, net_param_offset(0), net_param_offset(kNetLayers - 1), w.fused);
+    pack_upfrag<<<1, 256, 0, st>>>(w.fused, w.upfrag);
     w.host_params_valid = false;
     return cudaGetLastError();
 }
@@ -1471,7 +1522,6 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
         e = cudaMemcpyAsync(k2, w.fused + kFusedK2, sizeof k2, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(P.k, w.fused + kFusedK125 + kFusedInterior * 125, sizeof P.k, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(P.wp, w.fused + kFusedWp, sizeof P.wp, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return e;
         for (int c = 0; c < 16; ++c)
@@ -1510,8 +1560,8 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
             if (e != cudaSuccess) return e;
             configured = true;
         }
-        net_out_interior<<<grid, kOutCX * kOutCY, kOutBwinBytes, st>>>(r, ws.b2, ws.scalars, h2, z, nx, ny, nz,
-                                                                       w.out_params);
+        net_out_interior<<<grid, kOutCX * kOutCY, kOutBwinBytes, st>>>(r, ws.b2, w.upfrag, ws.scalars, h2, z, nx,
+                                                                       ny, nz, w.out_params);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {

@@ -54,11 +54,10 @@ struct NetWorkspace {
 
 // BF16 copies of the parameters: forward layout and the transposed, flipped
 // layout that turns the data gradient into a forward convolution.
-// Interior composite 5x5x5 stencil and up-path weights of the fused output
-// layer, passed to its kernel by value (constant-bank operands).
+// Interior composite 5x5x5 stencil of the fused output layer, passed to its
+// kernel by value (constant-bank operands).
 struct NetOutParams {
     float k[125];         // (dz * 5 + dy) * 5 + dx, offsets -2..2
-    float wp[8 * 8 * 16]; // [fine parity][coarse cell][channel]
 };
 
 // Composite input stencil (pool o c1, 4x4x4 of stride 2, 16 outputs), by value.
@@ -71,6 +70,7 @@ struct NetWeights {
     uint16_t *bwd = nullptr;   // W'[ci][26 - tap][co]
     float *fwd_f32 = nullptr;  // FP32 copies of c1, c7 (CUDA-core layers) and their transposes
     float *fused = nullptr;    // FP32 composite stencils of the fused full-resolution layers
+    uint32_t *upfrag = nullptr;  // the output layer's up-path weights as tensor-core B fragments
     // host copies of the full-resolution layers' weights, refreshed from `fused` on the
     // first application after a repack
     mutable NetOutParams out_params{};
