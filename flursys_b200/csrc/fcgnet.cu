@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "fcgnet.cuh"
+#include "tma.cuh"
 
 namespace flursys {
 
@@ -1273,6 +1274,221 @@ __global__ void __launch_bounds__(kUThreads) conv_umma(Src src, const uint16_t *
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(G::kTmemCols));
 }
 
+// ---------------------------------------------------------------------------
+// conv_umma_tma<CIN, COUT, NS>: the tcgen05 convolution of plain inputs with
+// TMA staging and warp-specialised roles, 160 threads. Warps 0-3 are the
+// epilogue (warp w reads TMEM lanes 32w..32w+31, voxel rows 4w..4w+3); lane 0
+// of warp 4 loads and issues. Input planes arrive by cp.async.bulk.tensor,
+// one 8-channel slice per copy (the box 8 channels x 10 x 18 cells lands as
+// one K-major core-matrix slice; halo cells outside the tensor are
+// zero-filled by the copy engine), into a ring of NS plane slots. Every
+// hand-off is an mbarrier:
+//   full[s]   the plane in slot s has landed (transaction bytes)
+//   done[b]   the MMAs of a plane into accumulator buffer b have completed
+//   empty[b]  the four epilogue warps have read accumulator buffer b
+// The issuer queues the MMAs of plane z once planes z-1..z+1 have landed
+// and buffer b is empty, then, once the MMAs of plane z-1 are done, refills
+// the slot of plane z-2 (their last reader) with plane z-2+NS, so each copy
+// has NS-3 planes of MMAs to land behind. No block-wide barrier runs inside
+// the march. Every wait is bounded: on a timeout the epilogue writes NaN
+// for its voxels of that plane (the solver then sees a non-finite residual
+// and falls back), and the issuer waits (bounded) for its copies and MMAs in
+// flight before the tensor memory is freed.
+// ---------------------------------------------------------------------------
+constexpr int kUSlice = (kUCells * 16 + 127) / 128 * 128;  // one 8-channel slice, 128-byte aligned
+constexpr int kUTmaThreads = 160;
+
+template <int CIN, int COUT>
+struct UmmaTma {
+    static constexpr int kSlot = (CIN / 8) * kUSlice;
+    static constexpr int kWBytes = 27 * (CIN / 8) * COUT * 16;
+    static constexpr int smem(int ns) { return ns * kSlot + kWBytes; }
+    static constexpr int kTmemCols = 2 * COUT < 32 ? 32 : 2 * COUT;
+};
+
+// Waits for phase `parity` of an mbarrier for at most about a second of
+// device time (%globaltimer, read every 1024 polls); false when it ran out.
+__device__ __forceinline__ bool mbar_wait_timed(uint32_t mbar, uint32_t parity) {
+    unsigned long long t0 = 0;
+    for (unsigned spin = 1;; ++spin) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((spin & 1023u) == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > 1000000000ull) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive_cta(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// The copies of input plane p (K8 slices of 8 channels) into its ring slot,
+// completion on that slot's full barrier.
+template <int K8, int NS, int SLOT>
+__device__ __forceinline__ void tma_plane(uint8_t *ring, uint64_t *full, const CUtensorMap *map, int p, int z0, int x0,
+                                          int y0) {
+    const int s = (p - z0 + 1) % NS;
+    mbar_expect_tx(&full[s], K8 * 8 * kUCells * 2);
+#pragma unroll
+    for (int k8 = 0; k8 < K8; ++k8) tma_load_4d(ring + s * SLOT + k8 * kUSlice, map, 8 * k8, x0 - 1, y0 - 1, p, &full[s]);
+}
+
+template <int CIN, int COUT, int NS>
+__global__ void __launch_bounds__(kUTmaThreads) conv_umma_tma(const uint16_t *__restrict__ W, uint16_t *out, int nx,
+                                                              int ny, int nz, int kz,
+                                                              const __grid_constant__ CUtensorMap tmap) {
+    using G = UmmaTma<CIN, COUT>;
+    extern __shared__ __align__(1024) uint8_t usmem[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_full[NS], s_done[2], s_empty[2];
+    constexpr int K8 = CIN / 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kUX, y0 = blockIdx.y * kUY, z0 = blockIdx.z * kz;
+    const int z1 = min(z0 + kz, nz);
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(usmem);
+    uint8_t *ring = usmem;
+    uint8_t *wts = usmem + NS * G::kSlot;
+    const bool issuer = tid == 4 * 32;
+    // planes z0 - 1 .. z1 pass through the ring in order
+    auto slot_of = [&](int p) { return (p - z0 + 1) % NS; };
+    auto full_parity = [&](int p) { return (uint32_t)(((p - z0 + 1) / NS) & 1); };
+    auto bar = [](const uint64_t &b) { return (uint32_t)__cvta_generic_to_shared(&b); };
+    int loaded = z0 - 2;  // issuer: last plane whose copies were issued
+    if (issuer) {
+        for (int s = 0; s < NS; ++s) mbar_init(&s_full[s], 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&s_done[b], 1);
+            mbar_init(&s_empty[b], 4);
+        }
+        // the first planes' copies overlap the weight staging below
+        for (int p = z0 - 1; p <= min(z1, z0 - 2 + NS); ++p) {
+            tma_plane<K8, NS, G::kSlot>(ring, s_full, &tmap, p, z0, x0, y0);
+            loaded = p;
+        }
+    }
+    // weights [tap][k8][co] from W[co][tap][ci]
+    for (int idx = tid; idx < 27 * K8 * COUT; idx += kUTmaThreads) {
+        const int co = idx % COUT, rest = idx / COUT;
+        const int k8 = rest % K8, t27 = rest / K8;
+        const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + t27) * CIN + k8 * 8);
+        *reinterpret_cast<uint4 *>(wts + ((t27 * K8 + k8) * COUT + co) * 16) = q;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst),
+                     "n"(G::kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    if (issuer) {
+        constexpr uint32_t kIdesc =
+            (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((128u >> 4) << 24);
+        bool ok = true;
+        int waited = z0 - 2;  // last plane whose arrival was seen
+        int issued = z0 - 1;  // last plane whose MMAs were committed
+        int confirmed = z0 - 1;  // last plane whose MMAs were seen complete
+        for (int z = z0; z < z1 && ok; ++z) {
+            const int b = (z - z0) & 1;
+            if (z - z0 >= 2) ok = mbar_wait_timed(bar(s_empty[b]), (uint32_t)(((z - z0 - 2) >> 1) & 1));
+            for (int p = waited + 1; p <= z + 1 && ok; ++p) {  // planes z - 1 .. z + 1 landed
+                ok = mbar_wait_timed(bar(s_full[slot_of(p)]), full_parity(p));
+                if (ok) waited = p;
+            }
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dbuf = tmem + (uint32_t)(b * COUT);
+            // the weights' descriptor is formed per plane from an opaque copy
+            // of its address, so the compiler keeps the 27 x CIN/16 weight
+            // descriptors as immediate offsets instead of hoisting them into
+            // registers
+            uint32_t waddr;
+            asm volatile("mov.u32 %0, %1;" : "=r"(waddr) : "r"(sbase + (uint32_t)(NS * G::kSlot)));
+            const uint64_t wdesc = umma_desc(waddr, COUT * 16, 128);
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz) {
+                const uint64_t adesc = umma_desc(sbase + (uint32_t)(slot_of(z + dz - 1) * G::kSlot), kUSlice, kUHX * 16);
+#pragma unroll
+                for (int t9 = 0; t9 < 9; ++t9) {
+#pragma unroll
+                    for (int kc = 0; kc < CIN / 16; ++kc) {
+                        const int dy = t9 / 3, dx = t9 % 3, tap = dz * 9 + t9;
+                        const uint64_t a = adesc + (uint64_t)((((dy * kUHX + dx) * 16) + 2 * kc * kUSlice) >> 4);
+                        const uint64_t w = wdesc + (uint64_t)((((tap * K8 + 2 * kc) * COUT) * 16) >> 4);
+                        umma_f16(dbuf, a, w, kIdesc, (dz | t9 | kc) ? 1u : 0u);
+                    }
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             bar(s_done[b]))
+                         : "memory");
+            issued = z;
+            if (z > z0) {
+                // the MMAs of plane z - 1 were the last readers of plane z - 2
+                ok = mbar_wait_timed(bar(s_done[(z - 1 - z0) & 1]), (uint32_t)(((z - 1 - z0) >> 1) & 1));
+                if (ok) confirmed = z - 1;
+                if (ok && z - 2 + NS <= z1) {
+                    tma_plane<K8, NS, G::kSlot>(ring, s_full, &tmap, z - 2 + NS, z0, x0, y0);
+                    loaded = z - 2 + NS;
+                }
+            }
+        }
+        if (!ok) {
+            // drain what is in flight (bounded): copies not yet seen, MMAs not yet confirmed
+            for (int p = waited + 1; p <= loaded; ++p)
+                (void)mbar_wait_timed(bar(s_full[slot_of(p)]), full_parity(p));
+            for (int z = confirmed + 1; z <= issued; ++z)
+                (void)mbar_wait_timed(bar(s_done[(z - z0) & 1]), (uint32_t)(((z - z0) >> 1) & 1));
+        }
+    } else if (warp < 4) {
+        const int m = warp * 32 + lane;  // this thread's voxel row of the accumulator
+        const int vx = x0 + (m % kUX), vy = y0 + m / kUX;
+        for (int z = z0; z < z1; ++z) {
+            const int b = (z - z0) & 1;
+            const bool arrived =
+                __all_sync(0xffffffffu, mbar_wait_timed(bar(s_done[b]), (uint32_t)(((z - z0) >> 1) & 1)));
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float acc[COUT];
+            if (arrived) {
+                tmem_ld<COUT>(tmem + (uint32_t)(b * COUT) + ((uint32_t)(warp * 32) << 16), acc);
+            } else {
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) acc[c] = __int_as_float(0x7fc00000);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (arrived && lane == 0) mbar_arrive_cta(bar(s_empty[b]));
+            if (vx < nx && vy < ny) {
+                uint16_t *o = out + (((long long)z * ny + vy) * nx + vx) * COUT;
+#pragma unroll
+                for (int c = 0; c < COUT; c += 8) {
+                    uint4 q;
+                    uint16_t *h = reinterpret_cast<uint16_t *>(&q);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) h[e] = f2bf(acc[c + e]);
+                    *reinterpret_cast<uint4 *>(o + c) = q;
+                }
+            }
+            if (!arrived) break;  // a lost accumulator: stop
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(G::kTmemCols));
+}
+
 // Planes per block of conv_tc_z: the largest of 8, 4, 2 that still gives
 // about two blocks per SM, else 1.
 int conv_planes(int nx, int ny, int nz) {
@@ -1321,41 +1537,39 @@ bool umma_enabled() {
     return !(env && env[0] == '0');
 }
 
-template <int CIN, int COUT, int MODE>
-cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
-    using G = UmmaConv<CIN, COUT>;
-    if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
-    static int slots = 0, per_sm = 0;  // resident CTAs per device and per SM (per instantiation)
-    if (!slots) {
-        // the largest shared-memory carveout, so that as many CTAs as fit
-        // by shared and tensor memory share an SM
-        cudaError_t e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             G::kSmem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(conv_umma<CIN, COUT, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     (int)cudaSharedmemCarveoutMaxShared);
-        int dev = 0, sms = 0, smem_sm = 0;
-        if (e == cudaSuccess) e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        if (e != cudaSuccess) return e;
-        const int by_smem = smem_sm / (G::kSmem + 2048);  // + static and reserved shared memory per CTA
-        per_sm = std::max(1, std::min(by_smem, 512 / G::kTmemCols));
-        slots = std::max(1, sms * per_sm);
-    }
-    // Planes per CTA. Where several CTAs share an SM: the longest march that
-    // still leaves about four CTAs per resident slot over the launch
-    // (measured on B200: longer marches with fewer CTAs ran up to 2x slower).
-    // Where one CTA fills an SM (the weights of all taps take most of the
-    // shared memory): the longest march whose grid fills its last wave to
-    // 85% or more, so the weights are loaded once per many planes.
+// Resident CTAs per SM and per device of a tcgen05 convolution kernel with
+// `smem` bytes of dynamic shared memory, its carveout set to the maximum so
+// that as many CTAs as fit by shared and tensor memory share an SM.
+cudaError_t umma_occupancy(const void *fn, int smem, int tmem_cols, int &per_sm, int &slots) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    int dev = 0, sms = 0, smem_sm = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e != cudaSuccess) return e;
+    const int by_smem = smem_sm / (smem + 2048);  // + static and reserved shared memory per CTA
+    per_sm = std::max(1, std::min(by_smem, 512 / tmem_cols));
+    slots = std::max(1, sms * per_sm);
+    return cudaSuccess;
+}
+
+// Planes per CTA. Where several CTAs share an SM: the longest march that
+// still leaves about four CTAs per resident slot over the launch (measured
+// on B200: longer marches with fewer CTAs ran up to 2x slower). Where one
+// CTA fills an SM (the weights of all taps take most of the shared
+// memory): the longest march whose grid fills its last wave to 85% or
+// more, so the weights are loaded once per many planes.
+int umma_planes(int nx, int ny, int nz, int per_sm, int slots) {
     const long long cols = (long long)((nx + kUX - 1) / kUX) * ((ny + kUY - 1) / kUY);
     int kz = 1;
     if (per_sm > 1) {
         while (kz < nz && cols * ((nz + 2 * kz - 1) / (2 * kz)) >= 4LL * (slots / per_sm)) kz *= 2;
+        return kz;
     }
-    double best = per_sm > 1 ? 2.0 : -1.0;
-    for (int t = 1; t <= nz && per_sm == 1; t *= 2) {
+    double best = -1.0;
+    for (int t = 1; t <= nz; t *= 2) {
         const long long ctas = cols * ((nz + t - 1) / t);
         const long long waves = (ctas + slots - 1) / slots;
         const double fill = double(ctas) / double(waves * slots);
@@ -1364,6 +1578,66 @@ cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int 
             best = std::max(best, fill);
         }
     }
+    return kz;
+}
+
+// Input staging of the tcgen05 convolutions of plain tensors: TMA copies
+// (conv_umma_tma, the default) unless FLURSYS_FCG_TMA=0, which selects the
+// register-staged conv_umma. Plane slots of the TMA ring: 5 where that
+// keeps as many CTAs per SM as 4, else 4 (FLURSYS_FCG_TMA_SLOTS=4 or 5
+// forces one).
+bool tma_conv_enabled() {
+    const char *env = std::getenv("FLURSYS_FCG_TMA");
+    return !(env && env[0] == '0');
+}
+int tma_conv_slots_forced() {
+    const char *env = std::getenv("FLURSYS_FCG_TMA_SLOTS");
+    const int v = env ? std::atoi(env) : 0;
+    return v == 4 || v == 5 ? v : 0;
+}
+
+template <int CIN, int COUT, int NS>
+cudaError_t launch_conv_tma(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, int per_sm,
+                            int slots, cudaStream_t st) {
+    CUtensorMap map;
+    if (!tma_map_bf16_cxyz(&map, s.in, CIN, nx, ny, nz, 8, kUHX, kUHY)) return cudaErrorInvalidValue;
+    const int kz = umma_planes(nx, ny, nz, per_sm, slots);
+    dim3 grid((nx + kUX - 1) / kUX, (ny + kUY - 1) / kUY, (nz + kz - 1) / kz);
+    conv_umma_tma<CIN, COUT, NS><<<grid, kUTmaThreads, UmmaTma<CIN, COUT>::smem(NS), st>>>(W, out, nx, ny, nz, kz, map);
+    return cudaGetLastError();
+}
+
+template <int CIN, int COUT, int MODE>
+cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, cudaStream_t st) {
+    using G = UmmaConv<CIN, COUT>;
+    using T = UmmaTma<CIN, COUT>;
+    if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
+    if constexpr (MODE == kPlain && T::smem(4) <= 220 * 1024) {
+        if (tma_conv_enabled()) {
+        // per instantiation: resident CTAs of the 4- and 5-slot rings, and the choice
+        static int ns = 0, per4 = 0, slots4 = 0, per5 = 0, slots5 = 0;
+        if (!ns) {
+            cudaError_t e = umma_occupancy((const void *)conv_umma_tma<CIN, COUT, 4>, T::smem(4), T::kTmemCols, per4, slots4);
+            if (e != cudaSuccess) return e;
+            ns = 4;
+            if (T::smem(5) <= 220 * 1024) {
+                e = umma_occupancy((const void *)conv_umma_tma<CIN, COUT, 5>, T::smem(5), T::kTmemCols, per5, slots5);
+                if (e != cudaSuccess) return e;
+                if (per5 == per4) ns = 5;
+            }
+            const int forced = tma_conv_slots_forced();
+            if (forced == 4 || (forced == 5 && per5 > 0)) ns = forced;
+        }
+        if (ns == 5) return launch_conv_tma<CIN, COUT, 5>(s, W, out, nx, ny, nz, per5, slots5, st);
+        return launch_conv_tma<CIN, COUT, 4>(s, W, out, nx, ny, nz, per4, slots4, st);
+        }
+    }
+    static int slots = 0, per_sm = 0;  // resident CTAs per device and per SM (per instantiation)
+    if (!slots) {
+        cudaError_t e = umma_occupancy((const void *)conv_umma<CIN, COUT, MODE>, G::kSmem, G::kTmemCols, per_sm, slots);
+        if (e != cudaSuccess) return e;
+    }
+    const int kz = umma_planes(nx, ny, nz, per_sm, slots);
     dim3 grid((nx + kUX - 1) / kUX, (ny + kUY - 1) / kUY, (nz + kz - 1) / kz);
     conv_umma<CIN, COUT, MODE><<<grid, kUThreads, G::kSmem, st>>>(s, W, out, nx, ny, nz, kz);
     return cudaGetLastError();

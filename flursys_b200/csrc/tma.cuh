@@ -46,6 +46,23 @@ inline bool tma_map_f32_3d(CUtensorMap *map, const float *base, int nx, int ny, 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tiled map of a dense BF16 activation tensor [nz][ny][nx][c] (channels
+// fastest), box bc channels x bx x by x 1 plane, zero fill outside the
+// tensor. Needs c % 8 == 0 and a 16-byte aligned base. Returns false when
+// the driver refuses.
+inline bool tma_map_bf16_cxyz(CUtensorMap *map, const void *base, int c, int nx, int ny, int nz, unsigned bc,
+                              unsigned bx, unsigned by) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tma_encode_fn();
+    if (!fn || c % 8 != 0 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * nx * 2, (cuuint64_t)c * nx * ny * 2};
+    const cuuint32_t box[4] = {bc, bx, by, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // -------------------------------------------------------------- device side
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
@@ -92,6 +109,18 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
         "[%5];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// 4D tile load (c, x, y, z) of a tma_map_bf16_cxyz map, completion on `bar`.
+// c * 2 bytes must be a multiple of 16; x, y, z may be negative or beyond
+// the tensor (zero fill). The destination is 128-byte aligned.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c, int x, int y, int z,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
 }
 

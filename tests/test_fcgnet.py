@@ -97,6 +97,27 @@ def test_net_apply_matches_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 40, 32)])
+def test_tma_staged_convolutions_equal_register_staged(dims, monkeypatch):
+    """The tcgen05 convolutions give the same bits whether their input planes
+    arrive by TMA copies (halo zero-filled by the copy engine) or by
+    register-staged loads with bounds checks."""
+    from flursys_b200.learned import DEFAULT_WEIGHTS, FcgNet
+    net = FcgNet(path=DEFAULT_WEIGHTS)
+    n = int(np.prod(dims))
+    rt = torch.tensor(np.random.default_rng(3).standard_normal(n), dtype=torch.float32, device="cuda")
+    out = {}
+    for tma in ("0", "1"):
+        monkeypatch.setenv("FLURSYS_FCG_TMA", tma)
+        zt = torch.empty_like(rt)
+        net.apply(rt, zt, dims, 1.0 / dims[0] ** 2)
+        torch.cuda.synchronize()
+        out[tma] = zt.cpu().numpy()
+    assert np.isfinite(out["1"]).all()
+    assert np.array_equal(out["0"], out["1"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["energy", "residual"])
 def test_net_gradients_match_oracle(kind):
     from flursys_b200 import _abi
