@@ -729,15 +729,55 @@ __global__ void pack_upfrag(const float *fz, uint32_t *upfrag) {
     }
 }
 
-// x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz): one thread per
-// coarse cell, its 4 x 4 x 4 window of r read from a shared tile of one
-// coarse layer (float2, conflict-free), the 1024 weights a by-value
-// parameter (constant-bank operands of the unrolled FMAs).
+// The input layer as a GEMM on the tensor cores: x2[cell][c] = sum over the
+// 64 taps o of r[window of cell][o] * K2[c][o], K = 64 taps in four chunks
+// of 16 (one oz plane each: k = 4 oy + ox), N = 16 channels in two tiles of
+// 8. B operands of mma.m16n8k16 per lane, each weight split into BF16
+// hi + lo: infrag[lane * 32 + ((kc * 2 + nt) * 2 + split) * 2 + reg], reg 0
+// holding taps 16 kc + 2 (lane & 3) + {0, 1} and reg 1 those + 8, of channel
+// 8 nt + (lane >> 2), the lower tap in the low half.
+constexpr int kInFragWords = 32 * 32;
+
+__global__ void pack_infrag(const float *fz, uint32_t *infrag) {
+    const float *k2 = fz + kFusedK2;  // [16 channels][64 taps]
+    for (int i = threadIdx.x; i < kInFragWords; i += blockDim.x) {
+        const int lane = i >> 5, w = i & 31;
+        const int reg = w & 1, split = (w >> 1) & 1, nt = (w >> 2) & 1, kc = w >> 3;
+        const int c = 8 * nt + (lane >> 2), o = 16 * kc + 2 * (lane & 3) + 8 * reg;
+        uint32_t word = 0;
+        for (int e = 0; e < 2; ++e) {
+            const float v = k2[c * 64 + o + e];
+            const uint16_t hi = f2bf(v);
+            const uint16_t u = split ? f2bf(v - bf2f(hi)) : hi;
+            word |= uint32_t(u) << (16 * e);
+        }
+        infrag[i] = word;
+    }
+}
+
+// Two FP32 values as BF16 pairs hi and lo = bf16(v - hi), the lower element
+// in the low half.
+__device__ __forceinline__ void split_bf16x2(float2 v, uint32_t &hi, uint32_t &lo) {
+    const uint16_t h0 = f2bf(v.x), h1 = f2bf(v.y);
+    hi = uint32_t(h0) | (uint32_t(h1) << 16);
+    lo = uint32_t(f2bf(v.x - bf2f(h0))) | (uint32_t(f2bf(v.y - bf2f(h1))) << 16);
+}
+
+// x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz): a block owns
+// 32 x 8 coarse cells of one coarse layer and stages their 4 x 4 x 4
+// windows of r as one shared tile (cp.async, zeros outside the grid); each
+// warp (one row of 32 cells) forms the GEMM [32 cells x 64 taps] x
+// [64 taps x 16 channels] as 4 tap chunks x 2 cell tiles x 2 channel tiles
+// of mma.m16n8k16, each with the window values and the weights split into
+// BF16 hi + lo and the products hi*hi + hi*lo + lo*hi accumulated in FP32
+// (the dropped lo*lo term is ~2^-16 of a product, below the BF16 rounding
+// of the output). A operands come from float2 pairs of the tile (taps
+// ox = 0, 1 and 2, 3 are adjacent fine cells).
 constexpr int kInCX = 32, kInCY = 8;                                        // coarse cells per block
 constexpr int kInWX = 2 * kInCX + 2, kInWY = 2 * kInCY + 2, kInWZ = 4;      // fine window
 __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__restrict__ r, const double *scale_ptr,
-                                                              uint16_t *x2, int cx, int cy, int cz,
-                                                              const __grid_constant__ NetInParams P) {
+                                                              const uint32_t *__restrict__ infrag, uint16_t *x2,
+                                                              int cx, int cy, int cz) {
     __shared__ __align__(16) float win[kInWZ][kInWY][kInWX];
     const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
     const int X0 = blockIdx.x * kInCX, Y0 = blockIdx.y * kInCY, Z = blockIdx.z;
@@ -760,33 +800,64 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
         cp_async_wait_all();
     }
     __syncthreads();
-    const int tx = threadIdx.x % kInCX, ty = threadIdx.x / kInCX;
-    const int X = X0 + tx, Y = Y0 + ty;
-    if (X >= cx || Y >= cy) return;
-    float acc[16];
+    const int lane = threadIdx.x & 31, ty = threadIdx.x >> 5;  // warp ty: coarse row Y0 + ty
+    const int Y = Y0 + ty;
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t bfr[32];
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(infrag) + lane * 8;
 #pragma unroll
-    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
-#pragma unroll
-    for (int oz = 0; oz < 4; ++oz)
-#pragma unroll
-        for (int oy = 0; oy < 4; ++oy) {
-            // window columns 2 tx .. 2 tx + 3 (two float2)
-            const float *row = &win[oz][2 * ty + oy][2 * tx];
-            const float2 a = reinterpret_cast<const float2 *>(row)[0], b = reinterpret_cast<const float2 *>(row)[1];
-            const float v[4] = {a.x, a.y, b.x, b.y};
-#pragma unroll
-            for (int ox = 0; ox < 4; ++ox)
-#pragma unroll
-                for (int c = 0; c < 16; ++c) acc[c] = fmaf(P.k2[((oz * 4 + oy) * 4 + ox) * 16 + c], v[ox], acc[c]);
+        for (int i = 0; i < 8; ++i) {
+            const uint4 q = __ldg(src + i);
+            bfr[4 * i] = q.x; bfr[4 * i + 1] = q.y; bfr[4 * i + 2] = q.z; bfr[4 * i + 3] = q.w;
         }
-    const float scale = float(scale_ptr[0]);
-    uint4 q[2];
-    uint16_t *h = reinterpret_cast<uint16_t *>(q);
+    }
+    float cf[2][2][4];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) h[c] = f2bf(acc[c] * scale);
-    uint4 *o4 = reinterpret_cast<uint4 *>(x2 + (((long long)Z * cy + Y) * cx + X) * 16);
-    o4[0] = q[0];
-    o4[1] = q[1];
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) cf[mt][nt][i] = 0.f;
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {  // tap plane oz = kc
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            // rows g and g + 8 of the tile: cells 16 mt + g (+ 8); taps
+            // k = 2 t + {0, 1} (oy = t >> 1, ox = 2 (t & 1) + {0, 1}) and k + 8 (oy + 2)
+            const float *w0 = &win[kc][2 * ty + (t >> 1)][2 * (16 * mt + g) + 2 * (t & 1)];
+            const float2 v0 = *reinterpret_cast<const float2 *>(w0);
+            const float2 v1 = *reinterpret_cast<const float2 *>(w0 + 16);
+            const float2 v2 = *reinterpret_cast<const float2 *>(w0 + 2 * kInWX);
+            const float2 v3 = *reinterpret_cast<const float2 *>(w0 + 2 * kInWX + 16);
+            uint32_t ah[4], al[4];
+            split_bf16x2(v0, ah[0], al[0]);
+            split_bf16x2(v1, ah[1], al[1]);
+            split_bf16x2(v2, ah[2], al[2]);
+            split_bf16x2(v3, ah[3], al[3]);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                const uint32_t *bh = bfr + ((kc * 2 + nt) * 2) * 2, *bl = bh + 2;
+                mma_bf16(cf[mt][nt], ah[0], ah[1], ah[2], ah[3], bh[0], bh[1]);
+                mma_bf16(cf[mt][nt], ah[0], ah[1], ah[2], ah[3], bl[0], bl[1]);
+                mma_bf16(cf[mt][nt], al[0], al[1], al[2], al[3], bh[0], bh[1]);
+            }
+        }
+    }
+    if (Y >= cy) return;
+    const float scale = float(scale_ptr[0]);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // accumulator rows g (h = 0) and g + 8
+            const int X = X0 + 16 * mt + g + 8 * h;
+            if (X >= cx) continue;
+            uint32_t *o = reinterpret_cast<uint32_t *>(x2 + (((long long)Z * cy + Y) * cx + X) * 16);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+                o[4 * nt + t] = uint32_t(f2bf(cf[mt][nt][2 * h] * scale)) |
+                                (uint32_t(f2bf(cf[mt][nt][2 * h + 1] * scale)) << 16);
+        }
 }
 
 // z = (sum over 8 coarse cells of Wp * b2 + scale * K125[class] * r) * h2 / scale,
@@ -1755,6 +1826,7 @@ cudaError_t NetWeights::allocate() {
     if (e == cudaSuccess) e = cudaMalloc(&fwd_f32, 1296 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&fused, kFusedCount * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&upfrag, kUpFragWords * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&infrag, kInFragWords * sizeof(uint32_t));
     return e;
 }
 
@@ -1764,9 +1836,10 @@ void NetWeights::release() {
     if (fwd_f32) cudaFree(fwd_f32);
     if (fused) cudaFree(fused);
     if (upfrag) cudaFree(upfrag);
+    if (infrag) cudaFree(infrag);
     fwd = bwd = nullptr;
     fwd_f32 = fused = nullptr;
-    upfrag = nullptr;
+    upfrag = infrag = nullptr;
 }
 
 cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st) {
@@ -1774,6 +1847,7 @@ cudaError_t net_pack_weights(const float *master, NetWeights &w, cudaStream_t st
     pack_kernel<<<grid_1d(n), 256, 0, st>>>(master, w.fwd, w.bwd, w.fwd_f32, n);
     pack_fused<<<1, 256, 0, st>>>(master, net_param_offset(0), net_param_offset(kNetLayers - 1), w.fused);
     pack_upfrag<<<1, 256, 0, st>>>(w.fused, w.upfrag);
+    pack_infrag<<<1, 256, 0, st>>>(w.fused, w.infrag);
     w.host_params_valid = false;
     return cudaGetLastError();
 }
@@ -1790,21 +1864,16 @@ cudaError_t net_apply(const NetWeights &w, NetWorkspace &ws, int nx, int ny, int
     const int n2x = nx / 2, n2y = ny / 2, n2z = nz / 2, n3x = nx / 4, n3y = ny / 4, n3z = nz / 4;
     const int n4x = nx / 8, n4y = ny / 8, n4z = nz / 8;
     if (!w.host_params_valid) {
-        // first application after a repack: bring the full-resolution layers' weights to the host
+        // first application after a repack: bring the output layer's interior stencil to the host
         NetOutParams &P = w.out_params;
-        float k2[16 * 64];  // [channel][tap] as packed
-        e = cudaMemcpyAsync(k2, w.fused + kFusedK2, sizeof k2, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(P.k, w.fused + kFusedK125 + kFusedInterior * 125, sizeof P.k, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(P.k, w.fused + kFusedK125 + kFusedInterior * 125, sizeof P.k, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return e;
-        for (int c = 0; c < 16; ++c)
-            for (int o = 0; o < 64; ++o) w.in_params.k2[o * 16 + c] = k2[c * 64 + o];
         w.host_params_valid = true;
     }
     {
         dim3 grid((n2x + kInCX - 1) / kInCX, (n2y + kInCY - 1) / kInCY, n2z);
-        net_in_fused<<<grid, kInCX * kInCY, 0, st>>>(r, ws.scalars, ws.x2, n2x, n2y, n2z, w.in_params);
+        net_in_fused<<<grid, kInCX * kInCY, 0, st>>>(r, ws.scalars, w.infrag, ws.x2, n2x, n2y, n2z);
     }
     e = cudaGetLastError();
     const uint16_t *W = w.fwd;

@@ -60,21 +60,16 @@ struct NetOutParams {
     float k[125];         // (dz * 5 + dy) * 5 + dx, offsets -2..2
 };
 
-// Composite input stencil (pool o c1, 4x4x4 of stride 2, 16 outputs), by value.
-struct NetInParams {
-    float k2[64 * 16];    // [tap (oz * 4 + oy) * 4 + ox, offsets -1..2][channel]
-};
-
 struct NetWeights {
     uint16_t *fwd = nullptr;   // W[co][tap][ci]
     uint16_t *bwd = nullptr;   // W'[ci][26 - tap][co]
     float *fwd_f32 = nullptr;  // FP32 copies of c1, c7 (CUDA-core layers) and their transposes
     float *fused = nullptr;    // FP32 composite stencils of the fused full-resolution layers
     uint32_t *upfrag = nullptr;  // the output layer's up-path weights as tensor-core B fragments
-    // host copies of the full-resolution layers' weights, refreshed from `fused` on the
+    uint32_t *infrag = nullptr;  // the input layer's composite stencil as tensor-core B fragments
+    // host copy of the output layer's interior stencil, refreshed from `fused` on the
     // first application after a repack
     mutable NetOutParams out_params{};
-    mutable NetInParams in_params{};
     mutable bool host_params_valid = false;
     cudaError_t allocate();
     void release();
