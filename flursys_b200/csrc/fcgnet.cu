@@ -765,37 +765,36 @@ __device__ __forceinline__ void split_bf16x2(float2 v, uint32_t &hi, uint32_t &l
 
 // x2 = bf16(scale * K2 * r) on the level-2 grid (cx, cy, cz): a block owns
 // 32 x 8 coarse cells of one coarse layer and stages their 4 x 4 x 4
-// windows of r as one shared tile (cp.async, zeros outside the grid); each
+// windows of r as one shared tile (16-byte cp.async copies of whole rows
+// from the 16-byte aligned fine column 2 X0 - 4, zeros outside the grid;
+// 4-byte copies of the exact window left the load/store unit the
+// bottleneck); each
 // warp (one row of 32 cells) forms the GEMM [32 cells x 64 taps] x
 // [64 taps x 16 channels] as 4 tap chunks x 2 cell tiles x 2 channel tiles
 // of mma.m16n8k16, each with the window values and the weights split into
 // BF16 hi + lo and the products hi*hi + hi*lo + lo*hi accumulated in FP32
 // (the dropped lo*lo term is ~2^-16 of a product, below the BF16 rounding
-// of the output). A operands come from float2 pairs of the tile (taps
-// ox = 0, 1 and 2, 3 are adjacent fine cells).
+// of the output). A operands are pairs of adjacent fine cells of the tile
+// (taps ox = 0, 1 and 2, 3).
 constexpr int kInCX = 32, kInCY = 8;                                        // coarse cells per block
-constexpr int kInWX = 2 * kInCX + 2, kInWY = 2 * kInCY + 2, kInWZ = 4;      // fine window
+constexpr int kInWX = 2 * kInCX + 8, kInWY = 2 * kInCY + 2, kInWZ = 4;      // fine window, x from 2 X0 - 4
 __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__restrict__ r, const double *scale_ptr,
                                                               const uint32_t *__restrict__ infrag, uint16_t *x2,
                                                               int cx, int cy, int cz) {
     __shared__ __align__(16) float win[kInWZ][kInWY][kInWX];
     const int nx = 2 * cx, ny = 2 * cy, nz = 2 * cz;
     const int X0 = blockIdx.x * kInCX, Y0 = blockIdx.y * kInCY, Z = blockIdx.z;
-    const int x0 = 2 * X0 - 1, y0 = 2 * Y0 - 1, z0 = 2 * Z - 1;
-    {  // one window row per warp at a time, lanes along x; every copy is in
-       // flight before the block waits
-        const int lane = threadIdx.x & 31;
-        for (int row = threadIdx.x >> 5; row < kInWZ * kInWY; row += blockDim.x >> 5) {
+    const int x0 = 2 * X0 - 4, y0 = 2 * Y0 - 1, z0 = 2 * Z - 1;
+    {  // 16-byte chunks (x0 and nx are multiples of 4, so a chunk is inside or
+       // outside the grid as a whole); every copy is in flight before the block waits
+        constexpr int kChunks = kInWX / 4, kAll = kInWZ * kInWY * kChunks;
+        for (int i = threadIdx.x; i < kAll; i += blockDim.x) {
+            const int row = i / kChunks, ch = i - row * kChunks;
             const int wz = row / kInWY, wy = row - wz * kInWY;
-            const int y = y0 + wy, z = z0 + wz;
-            const bool yz = y >= 0 && z >= 0 && y < ny && z < nz;
-            const float *src = r + ((long long)(yz ? z : 0) * ny + (yz ? y : 0)) * nx;
-#pragma unroll
-            for (int wx = lane; wx < kInWX; wx += 32) {
-                const int x = x0 + wx;
-                const bool ok = yz && x >= 0 && x < nx;
-                cp_async_zfill<4>(&win[wz][wy][wx], ok ? src + x : r, ok);
-            }
+            const int y = y0 + wy, z = z0 + wz, x = x0 + 4 * ch;
+            const bool ok = y >= 0 && z >= 0 && y < ny && z < nz && x >= 0 && x < nx;
+            const float *src = ok ? r + ((long long)z * ny + y) * nx + x : r;
+            cp_async_zfill<16>(&win[wz][wy][4 * ch], src, ok);
         }
         cp_async_wait_all();
     }
@@ -824,12 +823,13 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
             // rows g and g + 8 of the tile: cells 16 mt + g (+ 8); taps
-            // k = 2 t + {0, 1} (oy = t >> 1, ox = 2 (t & 1) + {0, 1}) and k + 8 (oy + 2)
-            const float *w0 = &win[kc][2 * ty + (t >> 1)][2 * (16 * mt + g) + 2 * (t & 1)];
-            const float2 v0 = *reinterpret_cast<const float2 *>(w0);
-            const float2 v1 = *reinterpret_cast<const float2 *>(w0 + 16);
-            const float2 v2 = *reinterpret_cast<const float2 *>(w0 + 2 * kInWX);
-            const float2 v3 = *reinterpret_cast<const float2 *>(w0 + 2 * kInWX + 16);
+            // k = 2 t + {0, 1} (oy = t >> 1, ox = 2 (t & 1) + {0, 1}) and k + 8
+            // (oy + 2); tap ox of cell i sits at window column 2 i + ox + 3
+            const float *w0 = &win[kc][2 * ty + (t >> 1)][2 * (16 * mt + g) + 2 * (t & 1) + 3];
+            const float2 v0 = make_float2(w0[0], w0[1]);
+            const float2 v1 = make_float2(w0[16], w0[17]);
+            const float2 v2 = make_float2(w0[2 * kInWX], w0[2 * kInWX + 1]);
+            const float2 v3 = make_float2(w0[2 * kInWX + 16], w0[2 * kInWX + 17]);
             uint32_t ah[4], al[4];
             split_bf16x2(v0, ah[0], al[0]);
             split_bf16x2(v1, ah[1], al[1]);
@@ -875,7 +875,7 @@ __global__ void __launch_bounds__(kInCX * kInCY) net_in_fused(const float *__res
 // the six faces, h2 * (K125[class] - K125[interior]) * r, the taps of c7
 // that leave the domain.
 constexpr int kOutCX = 32, kOutCY = 8;                       // coarse cells per block
-constexpr int kOutWX = 2 * kOutCX + 4, kOutWY = 2 * kOutCY + 4, kOutWZ = 6;  // fine window
+constexpr int kOutWX = 2 * kOutCX + 8, kOutWY = 2 * kOutCY + 4, kOutWZ = 6;  // fine window, x from 2 X0 - 4
 constexpr int kFusedInterior = 13;                            // class 1 + 3 * 1 + 9 * 1
 constexpr int kOutBX = kOutCX + 2, kOutBY = kOutCY + 2;       // coarse neighbourhood of a block
 constexpr int kOutBwin = 3 * kOutBY * 2 * kOutBX;             // its 16-byte units (two per coarse cell)
@@ -892,24 +892,20 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
     extern __shared__ __align__(16) uint4 bwin[];
     const int cx = nx >> 1, cy = ny >> 1, cz = nz >> 1;
     const int X0 = blockIdx.x * kOutCX, Y0 = blockIdx.y * kOutCY, Z = blockIdx.z;
-    const int x0 = 2 * X0 - 2, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
-    {  // one window row per warp at a time: r as float2 along x (x0 and nx are
-       // even, so a pair is inside or outside the grid as a whole), then the
-       // b2 neighbourhood row by row; every copy is in flight before the
-       // block waits
+    const int x0 = 2 * X0 - 4, y0 = 2 * Y0 - 2, z0 = 2 * Z - 2;
+    {  // r in 16-byte chunks from the 16-byte aligned column x0 (x0 and nx are
+       // multiples of 4, so a chunk is inside or outside the grid as a
+       // whole), then the b2 neighbourhood row by row; every copy is in
+       // flight before the block waits
         const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-        for (int row = threadIdx.x >> 5; row < kOutWZ * kOutWY; row += nw) {
+        constexpr int kChunks = kOutWX / 4, kAll = kOutWZ * kOutWY * kChunks;
+        for (int i = threadIdx.x; i < kAll; i += blockDim.x) {
+            const int row = i / kChunks, ch = i - row * kChunks;
             const int wz = row / kOutWY, wy = row - wz * kOutWY;
-            const int y = y0 + wy, z = z0 + wz;
-            const bool yz = y >= 0 && z >= 0 && y < ny && z < nz;
-            const float2 *src = reinterpret_cast<const float2 *>(r + ((long long)(yz ? z : 0) * ny + (yz ? y : 0)) * nx);
-            float2 *dst = reinterpret_cast<float2 *>(&win[wz][wy][0]);
-#pragma unroll
-            for (int e = lane; e < kOutWX / 2; e += 32) {
-                const int x = x0 + 2 * e;
-                const bool ok = yz && x >= 0 && x < nx;
-                cp_async_zfill<8>(dst + e, ok ? src + (x >> 1) : src, ok);
-            }
+            const int y = y0 + wy, z = z0 + wz, x = x0 + 4 * ch;
+            const bool ok = y >= 0 && z >= 0 && y < ny && z < nz && x >= 0 && x < nx;
+            const float *src = ok ? r + ((long long)z * ny + y) * nx + x : r;
+            cp_async_zfill<16>(&win[wz][wy][4 * ch], src, ok);
         }
         for (int row = threadIdx.x >> 5; row < 3 * kOutBY * 2; row += nw) {
             const int h = row & 1, byz = row >> 1;
@@ -984,7 +980,7 @@ __global__ void __launch_bounds__(kOutCX * kOutCY) net_out_interior(const float 
     for (int pz = 0; pz < 6; ++pz) {
 #pragma unroll
         for (int py = 0; py < 6; ++py) {
-            const float2 *row = reinterpret_cast<const float2 *>(&win[pz][2 * ty + py][2 * tx]);
+            const float2 *row = reinterpret_cast<const float2 *>(&win[pz][2 * ty + py][2 * tx + 2]);
             const float2 a = row[0], b = row[1], c = row[2];
             const float v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
 #pragma unroll
