@@ -1556,6 +1556,193 @@ __global__ void __launch_bounds__(kUTmaThreads) conv_umma_tma(const uint16_t *__
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(G::kTmemCols));
 }
 
+// The 9 x CIN/16 MMAs of one staged input plane (slot at shared address
+// `abase`) against the stacked weights starting at row `wrow` of each
+// (t9, k8) block (`wbase` = block 0 + wrow * 16 bytes; blocks 3 COUT rows
+// apart), into the accumulator at `dtmem`; `first` clears it with the
+// first MMA.
+template <int K8, int COUT>
+__device__ __forceinline__ void umma_plane(uint32_t abase, uint32_t wbase, uint32_t idesc, uint32_t dtmem, bool first) {
+    const uint64_t adesc = umma_desc(abase, kUSlice, kUHX * 16);
+    const uint64_t wdesc = umma_desc(wbase, 3 * COUT * 16, 128);
+#pragma unroll
+    for (int t9 = 0; t9 < 9; ++t9) {
+#pragma unroll
+        for (int kc = 0; kc < K8 / 2; ++kc) {
+            const int dy = t9 / 3, dx = t9 % 3;
+            const uint64_t a = adesc + (uint64_t)((((dy * kUHX + dx) * 16) + 2 * kc * kUSlice) >> 4);
+            const uint64_t w = wdesc + (uint64_t)((((t9 * K8 + 2 * kc) * 3 * COUT) * 16) >> 4);
+            umma_f16(dtmem, a, w, idesc, (first && t9 == 0 && kc == 0) ? 0u : 1u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// conv_umma_pair<CIN, COUT, NS>: conv_umma_tma computing output planes in
+// pairs (z, z + 1). An input plane p feeds outputs p - 1, p, p + 1 through
+// the weights of taps dz = 2, 1, 0, so the weights are stored per (t9, k8)
+// as one stacked block of 3 x COUT rows [W(dz=2); W(dz=1); W(dz=0)] and one
+// MMA of N = 2 COUT takes an input plane into both outputs of the pair:
+//   plane z      rows W1;W0 -> outputs z, z+1   (N = 2 COUT, first: clears)
+//   plane z + 1  rows W2;W1 -> outputs z, z+1   (N = 2 COUT)
+//   plane z - 1  rows W0    -> output z         (N = COUT)
+//   plane z + 2  rows W2    -> output z + 1     (N = COUT)
+// so each 128-voxel A tile is read from shared memory 36 instead of 54
+// times per output plane for CIN = 32 (the A reads bound these MMAs of
+// small N). Accumulators: two buffers of 2 COUT columns. Ring of NS = 6
+// plane slots: once the MMAs of pair z - 2 are done, planes z - 3 and z - 2
+// are refilled with z + 3 and z + 4, which the next pair needs. Roles,
+// barriers and the bounded waits are those of conv_umma_tma; planes per
+// CTA are even.
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct UmmaPair {
+    static constexpr int kNS = 6;
+    static constexpr int kSlot = (CIN / 8) * kUSlice;
+    static constexpr int kWBytes = 27 * (CIN / 8) * COUT * 16;
+    static constexpr int kSmem = kNS * kSlot + kWBytes;
+    static constexpr int kTmemCols = 4 * COUT < 32 ? 32 : 4 * COUT;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kUTmaThreads) conv_umma_pair(const uint16_t *__restrict__ W, uint16_t *out, int nx,
+                                                               int ny, int nz, int kz,
+                                                               const __grid_constant__ CUtensorMap tmap) {
+    using G = UmmaPair<CIN, COUT>;
+    constexpr int NS = G::kNS;
+    extern __shared__ __align__(1024) uint8_t usmem[];
+    __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_full[NS], s_done[2], s_empty[2];
+    constexpr int K8 = CIN / 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kUX, y0 = blockIdx.y * kUY, z0 = blockIdx.z * kz;
+    const int z1 = min(z0 + kz, nz);  // z1 - z0 is even
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(usmem);
+    uint8_t *ring = usmem;
+    uint8_t *wts = usmem + NS * G::kSlot;
+    const bool issuer = tid == 4 * 32;
+    auto slot_of = [&](int p) { return (p - z0 + 1) % NS; };
+    auto full_parity = [&](int p) { return (uint32_t)(((p - z0 + 1) / NS) & 1); };
+    auto bar = [](const uint64_t &b) { return (uint32_t)__cvta_generic_to_shared(&b); };
+    int loaded = z0 - 2;
+    if (issuer) {
+        for (int s = 0; s < NS; ++s) mbar_init(&s_full[s], 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&s_done[b], 1);
+            mbar_init(&s_empty[b], 4);
+        }
+        for (int p = z0 - 1; p <= min(z1, z0 - 2 + NS); ++p) {
+            tma_plane<K8, NS, G::kSlot>(ring, s_full, &tmap, p, z0, x0, y0);
+            loaded = p;
+        }
+    }
+    // weights [t9][k8][(2 - dz) * COUT + co] from W[co][dz * 9 + t9][ci]
+    for (int idx = tid; idx < 27 * K8 * COUT; idx += kUTmaThreads) {
+        const int co = idx % COUT, rest = idx / COUT;
+        const int k8 = rest % K8, t27 = rest / K8;
+        const int dz = t27 / 9, t9 = t27 % 9;
+        const uint4 q = *reinterpret_cast<const uint4 *>(W + ((long long)co * 27 + t27) * CIN + k8 * 8);
+        *reinterpret_cast<uint4 *>(wts + ((t9 * K8 + k8) * 3 * COUT + (2 - dz) * COUT + co) * 16) = q;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst),
+                     "n"(G::kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    if (issuer) {
+        constexpr uint32_t kIdesc1 =
+            (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((128u >> 4) << 24);
+        constexpr uint32_t kIdesc2 =
+            (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)((2 * COUT) >> 3) << 17) | ((128u >> 4) << 24);
+        const int npairs = (z1 - z0) >> 1;
+        bool ok = true;
+        int waited = z0 - 2;  // last plane whose arrival was seen
+        int issued = -1;      // last pair whose MMAs were committed
+        int confirmed = -1;   // last pair whose MMAs were seen complete
+        for (int j = 0; j < npairs && ok; ++j) {
+            const int z = z0 + 2 * j, b = j & 1;
+            if (j >= 2) ok = mbar_wait_timed(bar(s_empty[b]), (uint32_t)(((j - 2) >> 1) & 1));
+            for (int p = waited + 1; p <= z + 2 && ok; ++p) {  // planes z - 1 .. z + 2 landed
+                ok = mbar_wait_timed(bar(s_full[slot_of(p)]), full_parity(p));
+                if (ok) waited = p;
+            }
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dbuf = tmem + (uint32_t)(b * 2 * COUT);
+            uint32_t waddr;  // opaque copy: the weight offsets stay immediates
+            asm volatile("mov.u32 %0, %1;" : "=r"(waddr) : "r"(sbase + (uint32_t)(NS * G::kSlot)));
+            const uint32_t rb = sbase;
+            umma_plane<K8, COUT>(rb + slot_of(z) * G::kSlot, waddr + COUT * 16, kIdesc2, dbuf, true);
+            umma_plane<K8, COUT>(rb + slot_of(z + 1) * G::kSlot, waddr, kIdesc2, dbuf, false);
+            umma_plane<K8, COUT>(rb + slot_of(z - 1) * G::kSlot, waddr + 2 * COUT * 16, kIdesc1, dbuf, false);
+            umma_plane<K8, COUT>(rb + slot_of(z + 2) * G::kSlot, waddr, kIdesc1, dbuf + COUT, false);
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             bar(s_done[b]))
+                         : "memory");
+            issued = j;
+            if (j >= 1) {
+                // the MMAs of pair j - 1 were the last readers of planes z - 3 and z - 2
+                ok = mbar_wait_timed(bar(s_done[(j - 1) & 1]), (uint32_t)(((j - 1) >> 1) & 1));
+                if (ok) confirmed = j - 1;
+                for (int p = z - 3 + NS; ok && p <= z - 2 + NS && p <= z1; ++p) {
+                    tma_plane<K8, NS, G::kSlot>(ring, s_full, &tmap, p, z0, x0, y0);
+                    loaded = p;
+                }
+            }
+        }
+        if (!ok) {
+            for (int p = waited + 1; p <= loaded; ++p) (void)mbar_wait_timed(bar(s_full[slot_of(p)]), full_parity(p));
+            for (int j = confirmed + 1; j <= issued; ++j)
+                (void)mbar_wait_timed(bar(s_done[j & 1]), (uint32_t)((j >> 1) & 1));
+        }
+    } else if (warp < 4) {
+        const int m = warp * 32 + lane;
+        const int vx = x0 + (m % kUX), vy = y0 + m / kUX;
+        const int npairs = (z1 - z0) >> 1;
+        for (int j = 0; j < npairs; ++j) {
+            const int z = z0 + 2 * j, b = j & 1;
+            const bool arrived = __all_sync(0xffffffffu, mbar_wait_timed(bar(s_done[b]), (uint32_t)((j >> 1) & 1)));
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {  // output planes z and z + 1
+                float acc[COUT];
+                if (arrived) {
+                    tmem_ld<COUT>(tmem + (uint32_t)(b * 2 * COUT + h * COUT) + ((uint32_t)(warp * 32) << 16), acc);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) acc[c] = __int_as_float(0x7fc00000);
+                }
+                if (h == 1) {
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (arrived && lane == 0) mbar_arrive_cta(bar(s_empty[b]));
+                }
+                if (vx < nx && vy < ny) {
+                    uint16_t *o = out + (((long long)(z + h) * ny + vy) * nx + vx) * COUT;
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 8) {
+                        uint4 q;
+                        uint16_t *hh = reinterpret_cast<uint16_t *>(&q);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) hh[e] = f2bf(acc[c + e]);
+                        *reinterpret_cast<uint4 *>(o + c) = q;
+                    }
+                }
+            }
+            if (!arrived) break;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(G::kTmemCols));
+}
+
 // Planes per block of conv_tc_z: the largest of 8, 4, 2 that still gives
 // about two blocks per SM, else 1.
 int conv_planes(int nx, int ny, int nz) {
@@ -1663,6 +1850,23 @@ int tma_conv_slots_forced() {
     return v == 4 || v == 5 ? v : 0;
 }
 
+// Output planes in pairs (conv_umma_pair) where its six-slot ring fits and
+// the planes per CTA come out even, unless FLURSYS_FCG_PAIR=0.
+bool pair_conv_enabled() {
+    const char *env = std::getenv("FLURSYS_FCG_PAIR");
+    return !(env && env[0] == '0');
+}
+
+template <int CIN, int COUT>
+cudaError_t launch_conv_pair(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, int kz,
+                             cudaStream_t st) {
+    CUtensorMap map;
+    if (!tma_map_bf16_cxyz(&map, s.in, CIN, nx, ny, nz, 8, kUHX, kUHY)) return cudaErrorInvalidValue;
+    dim3 grid((nx + kUX - 1) / kUX, (ny + kUY - 1) / kUY, (nz + kz - 1) / kz);
+    conv_umma_pair<CIN, COUT><<<grid, kUTmaThreads, UmmaPair<CIN, COUT>::kSmem, st>>>(W, out, nx, ny, nz, kz, map);
+    return cudaGetLastError();
+}
+
 template <int CIN, int COUT, int NS>
 cudaError_t launch_conv_tma(const Src &s, const uint16_t *W, uint16_t *out, int nx, int ny, int nz, int per_sm,
                             int slots, cudaStream_t st) {
@@ -1680,6 +1884,19 @@ cudaError_t launch_conv_fwd(const Src &s, const uint16_t *W, uint16_t *out, int 
     using T = UmmaTma<CIN, COUT>;
     if (!umma_enabled() || G::kSmem > 220 * 1024) return launch_conv<CIN, COUT, MODE>(s, W, out, nx, ny, nz, st);
     if constexpr (MODE == kPlain && T::smem(4) <= 220 * 1024) {
+        if constexpr (UmmaPair<CIN, COUT>::kSmem <= 220 * 1024) {
+            if (tma_conv_enabled() && pair_conv_enabled() && nz % 2 == 0) {
+                using P = UmmaPair<CIN, COUT>;
+                static int pper = 0, pslots = 0;  // per instantiation
+                if (!pslots) {
+                    cudaError_t e = umma_occupancy((const void *)conv_umma_pair<CIN, COUT>, P::kSmem, P::kTmemCols,
+                                                   pper, pslots);
+                    if (e != cudaSuccess) return e;
+                }
+                const int kz = umma_planes(nx, ny, nz, pper, pslots);
+                if (kz % 2 == 0) return launch_conv_pair<CIN, COUT>(s, W, out, nx, ny, nz, kz, st);
+            }
+        }
         if (tma_conv_enabled()) {
         // per instantiation: resident CTAs of the 4- and 5-slot rings, and the choice
         static int ns = 0, per4 = 0, slots4 = 0, per5 = 0, slots5 = 0;

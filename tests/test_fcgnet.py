@@ -102,19 +102,38 @@ def test_tma_staged_convolutions_equal_register_staged(dims, monkeypatch):
     """The tcgen05 convolutions give the same bits whether their input planes
     arrive by TMA copies (halo zero-filled by the copy engine) or by
     register-staged loads with bounds checks."""
+    monkeypatch.setenv("FLURSYS_FCG_PAIR", "0")
+    out = {}
+    for tma in ("0", "1"):
+        monkeypatch.setenv("FLURSYS_FCG_TMA", tma)
+        out[tma] = _apply_default_net(dims)
+    assert np.isfinite(out["1"]).all()
+    assert np.array_equal(out["0"], out["1"])
+
+
+def _apply_default_net(dims):
     from flursys_b200.learned import DEFAULT_WEIGHTS, FcgNet
     net = FcgNet(path=DEFAULT_WEIGHTS)
     n = int(np.prod(dims))
     rt = torch.tensor(np.random.default_rng(3).standard_normal(n), dtype=torch.float32, device="cuda")
+    zt = torch.empty_like(rt)
+    net.apply(rt, zt, dims, 1.0 / dims[0] ** 2)
+    torch.cuda.synchronize()
+    return zt.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(64, 64, 64), (48, 40, 32)])
+def test_paired_plane_convolutions_match_single_plane(dims, monkeypatch):
+    """Output planes computed in pairs (one MMA of N = 2 Cout per input plane)
+    agree with the one-plane kernel up to the FP32 summation order inside the
+    tensor cores, i.e. BF16 roundings of the activations."""
     out = {}
-    for tma in ("0", "1"):
-        monkeypatch.setenv("FLURSYS_FCG_TMA", tma)
-        zt = torch.empty_like(rt)
-        net.apply(rt, zt, dims, 1.0 / dims[0] ** 2)
-        torch.cuda.synchronize()
-        out[tma] = zt.cpu().numpy()
+    for pair in ("0", "1"):
+        monkeypatch.setenv("FLURSYS_FCG_PAIR", pair)
+        out[pair] = _apply_default_net(dims)
     assert np.isfinite(out["1"]).all()
-    assert np.array_equal(out["0"], out["1"])
+    assert rel_l2(out["1"], out["0"]) < 1e-2
 
 
 @pytest.mark.gpu
