@@ -12,6 +12,11 @@
 //       UPADD adds the nearest-neighbour upsampled coarser tensor to a skip
 //       tensor — with the same FP32 sums and BF16 rounding as the separate
 //       pool / up_add kernels, so fused and unfused paths agree bit for bit.
+//   conv_umma / conv_umma_tma / conv_umma_pair  the convolutions of
+//       inference on the 5th-generation tensor cores (tcgen05.mma, FP32
+//       accumulators in tensor memory): register-staged input planes, TMA
+//       copies with warp-specialised issue and epilogue, and output planes
+//       in pairs (see below)
 //   conv_first  1 -> 16 channels (FP32 input, CUDA cores; training)
 //   conv_last   16 -> 1 channel (FP32 output, CUDA cores, staged tile; training)
 //   net_in_fused / net_out_interior + net_out_boundary  the full-resolution layers of inference,
